@@ -1,0 +1,276 @@
+/*
+ * megastation_b200.h -- C ABI of the B200-native (sm_100a) MegaStation
+ * per-slot baseband hot path.
+ *
+ * Plain C: pointers, sizes and status codes; no C++ or torch types.  Every
+ * device pointer is caller-owned device memory; every `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).  Operators
+ * own only their scratch and tables, sized at create time; no entry point
+ * allocates device memory on the hot path.  No function throws; each
+ * returns an mb_status.
+ *
+ * Layouts follow the reference's Matrix convention (dims[0] fastest,
+ * src/operators/matrix/matrix.h:95-117), written here slowest-first:
+ *   IQ samples       [sym][M][N]   complex (c32, or int16/int8/fp16 pairs)
+ *   uplink FFT out   [sym][M][S]   c32          (baseband/buffers.cc:87-88)
+ *   CSI / detector W [G][M][K]     c32          (buffers.cc:77-78)
+ *   precoder P       [G][K][M]     c32          (buffers.cc:79-80)
+ *   LLR              [sym][K][cb_stride*cb_blocks] fp16 (buffers.cc:96-99,
+ *                    tight stride: cb_stride >= zeros + cb_size)
+ *   user symbols     [sym][K][S]   c32          (buffers.cc:135-136)
+ *   precoded         [sym][M][N]   c32          (buffers.cc:140-141)
+ * with M antennas, K users, N FFT size, S data subcarriers, sg subcarrier
+ * group size and G = ceil(S / sg) groups.
+ *
+ * Threading (as in the reference, scheduler/gpu_engine.cc:77-430): a handle
+ * is used by one host thread / one stream at a time; distinct handles are
+ * independent.  mb_tables_init is idempotent and thread-safe.
+ */
+#ifndef MEGASTATION_B200_H_
+#define MEGASTATION_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MB_OK = 0,
+  MB_BAD_SHAPE = 1,    /* sizes inconsistent or outside supported range */
+  MB_BAD_ARG = 2,      /* NULL pointer, bad enum, misaligned buffer */
+  MB_NOT_PD = 3,       /* a Gram matrix was not positive definite */
+  MB_CUDA_ERROR = 4,   /* a CUDA runtime call failed */
+  MB_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+  MB_NO_MEMORY = 6,    /* create-time allocation failed */
+  MB_UNSUPPORTED = 7   /* valid request this build does not implement */
+} mb_status;
+
+typedef enum {
+  MB_IQ_C32 = 0, /* complex float32 */
+  MB_IQ_I16 = 1, /* int16 I/Q pairs, value / 32768 (fft_utils.h:19-22) */
+  MB_IQ_I8 = 2,  /* int8 I/Q pairs, value / 128 (QuanT = char, types.h:26) */
+  MB_IQ_F16 = 3  /* fp16 I/Q pairs */
+} mb_iq_dtype;
+
+typedef struct {
+  float re, im;
+} mb_c32;
+
+const char *mb_status_str(mb_status s);
+/* Version string of this library build. */
+const char *mb_version(void);
+
+/* ------------------------------------------------------------- tables --- */
+/* Per-device constant tables (QAM maps, 127-bit scrambler sequence, FFT
+ * twiddles).  Replaces Modulation::init / Scrambler::init / PilotSign::init
+ * (modulation/modulation.cu:78-113, scrambler/scrambler.cu:22-38,
+ * fft/fft_op.cu:176-192); idempotent and thread-safe.  Called implicitly by
+ * every create function for the current device. */
+mb_status mb_tables_init(int device);
+
+/* Host-side pilot sequence p/|p|^2 of length S (fft/fft_op.cu:176-192 over
+ * utils.h:54-95).  out: S host complex values. */
+mb_status mb_pilot_sign(uint64_t S, mb_c32 *out);
+/* Host-side per-user DM-RS table [K][S] (modulation/modulation.cu:82-86). */
+mb_status mb_dmrs_table(uint64_t S, uint64_t K, mb_c32 *out);
+/* LDPC code-block sizing of config/config.cc:84-135 (TS 38.212 lifting
+ * sizes; BG1 22 / BG2 10 information columns, 2 punctured columns). */
+mb_status mb_ldpc_sizes(uint64_t S, uint32_t Qm, double code_rate,
+                        uint32_t base_graph, uint64_t pilot_spacing,
+                        int downlink, uint64_t *encoded_bits,
+                        uint64_t *punctured_bits, uint64_t *decoded_bits);
+
+/* ---------------------------------------------------------------- FFT --- */
+/* Replaces UplinkFFT / PilotFFT / DownlinkIFFT (fft/fft_op.h:50-120).  One
+ * handle per (start, N, S, M, K, sg) shape, like the reference objects
+ * constructed per frame (baseband/process.cc:66-87).  N is a power of two
+ * in [16, 8192]; S <= N; start + S <= N is not required (indices wrap mod N
+ * as in fft_callback.cuh:52-53). */
+typedef struct {
+  uint32_t ofdm_start; /* first data subcarrier, (N - S) / 2 (config.cc:31) */
+  uint32_t ofdm_ca;    /* N, FFT size */
+  uint32_t ofdm_num;   /* S, data subcarriers */
+  uint32_t bs_num;     /* M, antennas */
+  uint32_t ue_num;     /* K, users (pilot FFT only) */
+  uint32_t sc_group;   /* sg, subcarrier group (pilot FFT only) */
+} mb_fft_desc;
+
+typedef struct mb_fft mb_fft;
+mb_status mb_fft_create(const mb_fft_desc *desc, mb_fft **out);
+mb_status mb_fft_destroy(mb_fft *fft);
+
+/* UplinkFFT::operator() (fft/fft_op.cu:135-143): for n_sym symbols, the
+ * unnormalised forward FFT of each antenna row with the shift gather
+ * out[b][i] = X[b][(i + start + N/2) % N], i < S.  iq: [n_sym][M][N],
+ * out: [n_sym][M][S]. */
+mb_status mb_fft_uplink(mb_fft *fft, const void *iq, int iq_dtype,
+                        uint32_t n_sym, mb_c32 *out, void *stream);
+
+/* PilotFFT::operator()(in, out, ue_start) (fft/fft_op.cu:145-165): symbol p
+ * of n_sym carries the comb pilots of users ue_start + p*sg + (i % sg); the
+ * LS estimate conj(X)*p/|p|^2 of subcarrier i is stored at
+ * csi[i/sg][b][u] (fft_callback.cuh:76-108).  csi: [G][M][K]. */
+mb_status mb_fft_pilot(mb_fft *fft, const void *iq, int iq_dtype,
+                       uint32_t n_sym, uint32_t ue_start, mb_c32 *csi,
+                       void *stream);
+
+/* DownlinkIFFT::operator() (fft/fft_op.cu:167-174, ifft_callback.cuh:21-59):
+ * unnormalised inverse FFT of each [M][N] row, then for int16/int8 outputs
+ * q = saturate(rint(x * (max+1) / N)); for MB_IQ_F16 / MB_IQ_C32 outputs
+ * x / N.  in: [n_sym][M][N] c32, out: [n_sym][M][N] pairs of out_dtype. */
+mb_status mb_ifft_downlink(mb_fft *fft, const mb_c32 *in, uint32_t n_sym,
+                           void *out, int out_dtype, void *stream);
+
+/* ------------------------------------------------------- zero forcing --- */
+/* Replaces Beamform (beamform/beamform.h:27-84). */
+typedef enum {
+  /* FP32 Gram + FP32 Cholesky + triangular solves: the reference's math
+   * (cuBLAS Cgemm + cuSOLVER potrf/potrs, beamform.cu:74-122) */
+  MB_ZF_FP32 = 0,
+  /* BF16 Gram on tensor cores (FP32 accumulate), FP32 inverse refined by
+   * Newton-Schulz, FP64 Cholesky for groups above cond_threshold */
+  MB_ZF_MIXED = 1,
+  /* FP64 Cholesky for every group */
+  MB_ZF_FP64 = 2
+} mb_zf_precision;
+
+typedef struct {
+  uint32_t precision;     /* mb_zf_precision */
+  uint32_t ns_iters;      /* Newton-Schulz refinements (MIXED), e.g. 2 */
+  float cond_threshold;   /* FP64 fallback above this estimate, e.g. 1e4 */
+  uint32_t reserved;
+} mb_zf_opts;
+
+typedef struct mb_zf mb_zf;
+/* Beamform(num_bs, num_ue, max_batch) (beamform.cu:19-31). */
+mb_status mb_zf_create(uint32_t num_bs, uint32_t num_ue, uint32_t max_groups,
+                       mb_zf **out);
+mb_status mb_zf_destroy(mb_zf *zf);
+
+/* Beamform::beamform_uplink (beamform.cu:74-122, 144-152): for each group g,
+ * C = csi[g] viewed as K x M column-major, W = (C C^H)^{-1} C overwrites
+ * csi[g].  S and sc_group locate a short last group (S % sg != 0), whose
+ * users without a pilot subcarrier take group G-2's estimate.
+ * group_status (device, nullable): per group 0 = ok, 1 = not positive
+ * definite (W zeroed), 2 = solved on the FP64 fallback.  When not NULL,
+ * group_cond (device) receives the condition estimate per group. */
+mb_status mb_zf_uplink(mb_zf *zf, mb_c32 *csi, uint32_t groups, uint32_t S,
+                       uint32_t sc_group, const mb_zf_opts *opts,
+                       int32_t *group_status, float *group_cond,
+                       void *stream);
+
+/* Beamform::beamform_downlink (beamform.cu:154-168, beam_utils.cuh:40-80):
+ * P[g][u][b] = W[g][b][u] / max_{b,u} |W[g][b][u]|. */
+mb_status mb_zf_precoder(const mb_c32 *W, mb_c32 *P, uint32_t num_bs,
+                         uint32_t num_ue, uint32_t groups, void *stream);
+
+/* ----------------------------------------------------- equalize + demod -- */
+typedef struct mb_scrambler mb_scrambler;
+typedef enum {
+  /* 127-periodic x^7+x^4+1 LFSR from state 0x5D, shared by all users
+   * (scrambler/scrambler.cu:22-31): the reference's sequence */
+  MB_SCR_LFSR127 = 0,
+  /* TS 38.211 5.2.1 Gold sequence per user, c_init(u) = c_init + u */
+  MB_SCR_GOLD = 1
+} mb_scrambler_mode;
+mb_status mb_scrambler_create(int mode, uint32_t c_init, uint32_t num_ue,
+                              uint64_t num_bits, mb_scrambler **out);
+mb_status mb_scrambler_destroy(mb_scrambler *scr);
+
+/* Equalize::equalize (sgemv/equalize.h:70-73, equalize.cu:53-67) batched
+ * over n_sym symbols: x[u][s] = sum_b W[g(s)][b][u] y[b][s], g(s) = s / sg,
+ * then the soft demapper (modulation/demodulation.h:30-67) in FP16.  The Qm
+ * LLRs of subcarrier s start at (t/cb_size)*cb_stride + zeros +
+ * t % cb_size, t = s*Qm, and are dropped when t/cb_size >= cb_blocks
+ * (equalize_kernel.cuh:272-287).  Slots outside the written positions are
+ * left untouched.
+ * hard (nullable): descrambled hard decisions (llr < 0) of stream bits
+ * t < min(S*Qm, cb_size*cb_blocks), packed MSB-first per (symbol, user)
+ * row of ceil(n/8) bytes; requires sg*Qm % 8 == 0.  scr NULL means no
+ * descrambling.  x (nullable): the equalized symbols [n_sym][K][S].
+ * y: [n_sym][M][S], llr: [n_sym][K][cb_stride*cb_blocks]. */
+mb_status mb_equalize(const mb_c32 *W, const mb_c32 *y, uint32_t K,
+                      uint32_t M, uint32_t S, uint32_t sg, uint32_t n_sym,
+                      uint32_t Qm, uint64_t cb_size, uint64_t cb_stride,
+                      uint64_t zeros, uint32_t cb_blocks, uint16_t *llr,
+                      uint8_t *hard, const mb_scrambler *scr, mb_c32 *x,
+                      void *stream);
+
+/* ------------------------------------------------------------ precode --- */
+/* Precode::precode (sgemv/precode.h:59-61, precode_kernel.cuh:255-262)
+ * batched over n_sym symbols: out[b][(s + start + N/2) % N] =
+ * sum_u P[g(s)][u][b] s[u][s]; unlike the reference every guard bin of the
+ * N-row is written as zero.  s: [n_sym][K][S], out: [n_sym][M][N]. */
+mb_status mb_precode(const mb_c32 *P, const mb_c32 *s, uint32_t M,
+                     uint32_t K, uint32_t S, uint32_t sg, uint32_t N,
+                     uint32_t start, uint32_t n_sym, mb_c32 *out,
+                     void *stream);
+
+/* -------------------------------------------------- modulate / scramble -- */
+/* Modulation::modulate (modulation/modulation.cu:115-128,
+ * modulation_kernel.cuh:37-68): bits of user u (in_bytes per user, LSB
+ * first) to Gray QAM; with pilot_spacing > 0 every pilot_spacing-th
+ * subcarrier carries pilot_table[u][c] (device, [K][S]).  out: [K][S]. */
+mb_status mb_modulate(const uint8_t *in, mb_c32 *out, uint64_t in_bytes,
+                      uint64_t num_carriers, uint64_t num_ues, uint32_t Qm,
+                      uint32_t pilot_spacing, const mb_c32 *pilot_table,
+                      void *stream);
+
+/* Scrambler::scrambler (scrambler/scrambler.cu:40-50,
+ * scrambler_kernel.cuh:36-56): out[j] = in[j] ^ (8 sequence bits, first in
+ * the MSB); in == out allowed.  [batch][num_bytes]. */
+mb_status mb_scramble(uint8_t *out, const uint8_t *in, uint64_t num_bytes,
+                      uint64_t batch, void *stream);
+
+
+/* --------------------------------------------------------- slot runner --- */
+/* Single-GPU stage sequencer replacing BandProcess::process
+ * (baseband/process.cc:134-225) and the multi-GPU scheduler
+ * (scheduler/gpu_engine.cc:253-409): per slot, the pilot FFT of all P pilot
+ * symbols (one launch), the ZF detector (+ downlink precoder) over all
+ * groups, then uplink FFT + equalize/demod/descramble in batches of
+ * sym_batch symbols, on one stream with a side stream that overlaps the
+ * first uplink FFT batch with the ZF solve.  All buffers are allocated at
+ * create; a slot call allocates nothing. */
+typedef struct {
+  uint32_t M, K, N, S, sg, Qm;  /* antennas, users, FFT, data subcarriers */
+  uint32_t P, U, D;             /* pilot, uplink, downlink symbols */
+  int32_t iq_dtype;             /* mb_iq_dtype of the uplink samples */
+  uint64_t cb_size, cb_stride, zeros; /* uplink LLR layout, one code block */
+  uint32_t zf_precision;        /* mb_zf_precision */
+  uint32_t ns_iters;
+  float cond_threshold;
+  uint32_t scrambler_mode;      /* mb_scrambler_mode; descrambles hard bits */
+  uint32_t c_init;
+  int32_t out_dtype;            /* downlink IFFT output mb_iq_dtype */
+  uint32_t sym_batch;           /* uplink symbols per FFT/equalize batch */
+  uint32_t use_graph;           /* replay the uplink slot as a CUDA graph */
+} mb_cell_desc;
+
+typedef struct mb_slot mb_slot;
+mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out);
+mb_status mb_slot_destroy(mb_slot *slot);
+
+/* One uplink slot: iq [P+U][M][N] (device) -> llr [U][K][cb_stride] fp16,
+ * hard [U][K][ceil(min(S*Qm, cb_size)/8)] (nullable).  group_status
+ * (device, nullable) [G] as in mb_zf_uplink. */
+mb_status mb_slot_uplink(mb_slot *slot, const void *iq, uint16_t *llr,
+                         uint8_t *hard, int32_t *group_status, void *stream);
+
+/* Downlink of the same slot: precode the D symbol vectors [D][K][S] with
+ * the precoder of the last uplink ZF, then IFFT to out [D][M][N] pairs of
+ * out_dtype. */
+mb_status mb_slot_downlink(mb_slot *slot, const mb_c32 *symbols, void *out,
+                           void *stream);
+
+/* Device views of the slot's internal buffers (for inspection and tests):
+ * CSI/W [G][M][K], precoder [G][K][M]. */
+mb_status mb_slot_buffers(mb_slot *slot, mb_c32 **csi, mb_c32 **precoder);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MEGASTATION_B200_H_ */

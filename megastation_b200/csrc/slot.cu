@@ -1,0 +1,232 @@
+// slot.cu -- single-GPU slot runner: the stage sequence of
+// BandProcess::process (baseband/process.cc:134-225) for one cell, with the
+// buffers of BandBuffers::init (baseband/buffers.cc:40-156) allocated once
+// at create.  The reference issues one operator per symbol on a stream per
+// symbol and synchronises the host after the pilots (process.cc:167-173);
+// here a whole slot is issued without host synchronisation: pilot FFT for
+// all pilot symbols in one launch, ZF over all groups in one launch, and the
+// uplink symbols in batches (FFT then fused equalize), with the first batch's
+// FFT forked onto a side stream so it overlaps the ZF solve.  Optionally the
+// whole uplink slot is captured once into a CUDA graph and replayed.
+#include <algorithm>
+
+#include "common.cuh"
+#include "sgemv.cuh"
+#include "slot.cuh"
+#include "zf.cuh"
+
+using namespace mb;
+
+struct mb_slot {
+  mb_cell_desc c;
+  uint32_t G;
+  uint64_t n_valid, hrow;
+  mb_fft *fft;
+  mb_scrambler *scr;
+  float2 *csi;        // [G][M][K]: CSI, then W in place
+  float2 *precoder;   // [G][K][M]
+  float2 *y;          // [sym_batch][M][S] uplink FFT output
+  void *y_lp;         // low-precision copy of y for the mixed path
+  float2 *precoded;   // [D][M][N]
+  cudaStream_t side;
+  cudaEvent_t ev_fork, ev_join;
+  // graph cache
+  cudaGraphExec_t graph;
+  const void *g_iq;
+  uint16_t *g_llr;
+  uint8_t *g_hard;
+  int32_t *g_status;
+  cudaStream_t g_stream;
+};
+
+static size_t iq_elem_bytes(int dt) {
+  return dt == MB_IQ_C32 ? 8 : dt == MB_IQ_I8 ? 2 : 4;
+}
+
+extern "C" mb_status mb_slot_destroy(mb_slot *s) {
+  if (!s) return MB_BAD_ARG;
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  if (s->fft) mb_fft_destroy(s->fft);
+  if (s->scr) mb_scrambler_destroy(s->scr);
+  cudaFree(s->csi);
+  cudaFree(s->precoder);
+  cudaFree(s->y);
+  cudaFree(s->y_lp);
+  cudaFree(s->precoded);
+  if (s->side) cudaStreamDestroy(s->side);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
+  delete s;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
+  if (!cell || !out) return MB_BAD_ARG;
+  *out = nullptr;
+  const mb_cell_desc &c = *cell;
+  if (c.M == 0 || c.K == 0 || c.K > c.M || c.K > 64 || c.sg == 0 || c.S == 0 ||
+      c.S > c.N || !is_pow2(c.N))
+    return MB_BAD_SHAPE;
+  if ((uint64_t)c.P * c.sg < c.K) return MB_BAD_SHAPE;  // config.cc:75-82
+  if (c.Qm != 2 && c.Qm != 4 && c.Qm != 6 && c.Qm != 8) return MB_BAD_ARG;
+  if (c.U && (c.cb_size == 0 || c.cb_stride < c.zeros + c.cb_size)) return MB_BAD_SHAPE;
+  mb_slot *s = new mb_slot();
+  s->c = c;
+  if (s->c.sym_batch == 0) s->c.sym_batch = 4;
+  s->c.sym_batch = std::min(s->c.sym_batch, std::max<uint32_t>(c.U, 1));
+  s->G = (c.S + c.sg - 1) / c.sg;
+  s->n_valid = std::min<uint64_t>((uint64_t)c.S * c.Qm, c.cb_size);
+  s->hrow = (s->n_valid + 7) / 8;
+  mb_fft_desc fd{(c.N - c.S) / 2, c.N, c.S, c.M, c.K, c.sg};
+  mb_status st = mb_fft_create(&fd, &s->fft);
+  if (st == MB_OK && c.U)
+    st = mb_scrambler_create((int)c.scrambler_mode, c.c_init, c.K, s->n_valid, &s->scr);
+  auto alloc = [&](void **p, size_t bytes) {
+    if (st != MB_OK || bytes == 0) return;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) st = record_error(e);
+  };
+  const size_t gmk = (size_t)s->G * c.M * c.K;
+  alloc((void **)&s->csi, sizeof(float2) * gmk);
+  alloc((void **)&s->precoder, sizeof(float2) * gmk);
+  alloc((void **)&s->y, sizeof(float2) * (size_t)s->c.sym_batch * c.M * c.S);
+  alloc((void **)&s->precoded, sizeof(float2) * (size_t)c.D * c.M * c.N);
+  if (st == MB_OK && c.zf_precision == MB_ZF_MIXED)
+    alloc(&s->y_lp, sizeof(uint32_t) * (size_t)s->c.sym_batch * c.M * c.S);
+  if (st == MB_OK) {
+    cudaError_t e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) st = record_error(e);
+  }
+  if (st == MB_OK && s->csi) {
+    // a short last group reads pilots of users it has no comb position for;
+    // start from zeros so those entries are defined before the tail fill
+    cudaError_t e = cudaMemset(s->csi, 0, sizeof(float2) * gmk);
+    if (e != cudaSuccess) st = record_error(e);
+  }
+  if (st != MB_OK) {
+    mb_slot_destroy(s);
+    return st;
+  }
+  *out = s;
+  return MB_OK;
+}
+
+static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
+                              uint8_t *hard, int32_t *status,
+                              cudaStream_t st) {
+  const mb_cell_desc &c = s->c;
+  const size_t sym_bytes = iq_elem_bytes(c.iq_dtype) * c.M * c.N;
+  const char *iq_b = reinterpret_cast<const char *>(iq);
+  mb_status r;
+  // fork: the first uplink FFT batch only needs the samples
+  const uint32_t nb0 = std::min(c.sym_batch, c.U);
+  if (c.U) {
+    MB_CUDA_TRY(cudaEventRecord(s->ev_fork, st));
+    MB_CUDA_TRY(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
+    r = mb_fft_uplink(s->fft, iq_b + (size_t)c.P * sym_bytes, c.iq_dtype, nb0,
+                      reinterpret_cast<mb_c32 *>(s->y), s->side);
+    if (r != MB_OK) return r;
+    MB_CUDA_TRY(cudaEventRecord(s->ev_join, s->side));
+  }
+  // pilots -> CSI -> W (+ precoder)
+  r = mb_fft_pilot(s->fft, iq, c.iq_dtype, c.P, 0, reinterpret_cast<mb_c32 *>(s->csi), st);
+  if (r != MB_OK) return r;
+  r = zf_fill_tail(s->csi, s->G, c.S, c.sg, c.M, c.K, st);
+  if (r != MB_OK) return r;
+  float2 *prec = c.D ? s->precoder : nullptr;
+  if (c.zf_precision == MB_ZF_MIXED) {
+    mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, 0};
+    r = zf_mixed(s->csi, prec, s->G, c.M, c.K, &o, status, nullptr, st);
+  } else {
+    r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, st);
+  }
+  if (r != MB_OK) return r;
+  if (!c.U) return MB_OK;
+  MB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
+  const uint64_t llr_sym = (uint64_t)c.K * c.cb_stride;
+  const uint64_t hard_sym = (uint64_t)c.K * s->hrow;
+  for (uint32_t l0 = 0; l0 < c.U; l0 += c.sym_batch) {
+    const uint32_t nb = std::min(c.sym_batch, c.U - l0);
+    if (l0) {
+      r = mb_fft_uplink(s->fft, iq_b + (size_t)(c.P + l0) * sym_bytes, c.iq_dtype, nb,
+                        reinterpret_cast<mb_c32 *>(s->y), st);
+      if (r != MB_OK) return r;
+    }
+    r = slot_equalize(s->c, s->csi, s->y, s->y_lp, nb, llr + l0 * llr_sym,
+                      hard ? hard + l0 * hard_sym : nullptr, s->scr, st);
+    if (r != MB_OK) return r;
+  }
+  return MB_OK;
+}
+
+mb_status mb::slot_equalize(const mb_cell_desc &c, const float2 *W,
+                            const float2 *y, void *y_lp, uint32_t nb,
+                            uint16_t *llr, uint8_t *hard,
+                            const mb_scrambler *scr, cudaStream_t st) {
+  (void)y_lp;
+  return mb_equalize(reinterpret_cast<const mb_c32 *>(W),
+                     reinterpret_cast<const mb_c32 *>(y), c.K, c.M, c.S, c.sg,
+                     nb, c.Qm, c.cb_size, c.cb_stride, c.zeros, 1, llr, hard,
+                     scr, nullptr, st);
+}
+
+extern "C" mb_status mb_slot_uplink(mb_slot *s, const void *iq, uint16_t *llr,
+                                    uint8_t *hard, int32_t *status,
+                                    void *stream) {
+  if (!s || !iq || (s->c.U && !llr)) return MB_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  if (!s->c.use_graph) return issue_uplink(s, iq, llr, hard, status, st);
+  if (!st) return MB_BAD_ARG;  // the legacy stream cannot be captured
+  if (!s->graph || s->g_iq != iq || s->g_llr != llr || s->g_hard != hard ||
+      s->g_status != status || s->g_stream != st) {
+    if (s->graph) {
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+    MB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    mb_status r = issue_uplink(s, iq, llr, hard, status, st);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (r != MB_OK) {
+      if (g) cudaGraphDestroy(g);
+      return r;
+    }
+    if (e != cudaSuccess) return record_error(e);
+    e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      s->graph = nullptr;
+      return record_error(e);
+    }
+    s->g_iq = iq;
+    s->g_llr = llr;
+    s->g_hard = hard;
+    s->g_status = status;
+    s->g_stream = st;
+  }
+  MB_CUDA_TRY(cudaGraphLaunch(s->graph, st));
+  return MB_OK;
+}
+
+extern "C" mb_status mb_slot_downlink(mb_slot *s, const mb_c32 *symbols,
+                                      void *out, void *stream) {
+  if (!s || !symbols || !out) return MB_BAD_ARG;
+  const mb_cell_desc &c = s->c;
+  if (!c.D) return MB_BAD_SHAPE;
+  cudaStream_t st = as_stream(stream);
+  mb_status r = mb_precode(reinterpret_cast<const mb_c32 *>(s->precoder), symbols,
+                           c.M, c.K, c.S, c.sg, c.N, (c.N - c.S) / 2, c.D,
+                           reinterpret_cast<mb_c32 *>(s->precoded), st);
+  if (r != MB_OK) return r;
+  return mb_ifft_downlink(s->fft, reinterpret_cast<const mb_c32 *>(s->precoded), c.D,
+                          out, c.out_dtype, st);
+}
+
+extern "C" mb_status mb_slot_buffers(mb_slot *s, mb_c32 **csi, mb_c32 **precoder) {
+  if (!s) return MB_BAD_ARG;
+  if (csi) *csi = reinterpret_cast<mb_c32 *>(s->csi);
+  if (precoder) *precoder = reinterpret_cast<mb_c32 *>(s->precoder);
+  return MB_OK;
+}

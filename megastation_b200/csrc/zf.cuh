@@ -1,0 +1,22 @@
+// zf.cuh -- internal launchers of the zero-forcing kernels.
+#pragma once
+#include "common.cuh"
+
+namespace mb {
+
+// copies users without a pilot in a short last group from group G-2
+mb_status zf_fill_tail(float2 *csi, uint32_t groups, uint32_t S, uint32_t sg,
+                       uint32_t M, uint32_t K, cudaStream_t st);
+// Cholesky ZF in FP32 or FP64, W in place; optional fused precoder
+mb_status zf_chol(float2 *csi, float2 *precoder, uint32_t groups, uint32_t M,
+                  uint32_t K, bool dbl, int32_t *status, float *cond,
+                  cudaStream_t st);
+// mixed precision ZF (zf_mixed.cu)
+mb_status zf_mixed(float2 *csi, float2 *precoder, uint32_t groups, uint32_t M,
+                   uint32_t K, const mb_zf_opts *opts, int32_t *status,
+                   float *cond, cudaStream_t st);
+mb_status precoder_launch(const float2 *W, float2 *P, uint32_t M, uint32_t K,
+                          uint32_t groups, cudaStream_t st);
+size_t zf_chol_smem(uint32_t M, uint32_t K, bool dbl);
+
+}  // namespace mb

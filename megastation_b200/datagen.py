@@ -1,0 +1,220 @@
+"""Seeded synthetic slot generator (the project's own; numpy, host side).
+
+No public dataset is involved: the reference generates its vectors with a
+MATLAB script (matlab/data_generator.m), and the workloads here are seeded
+synthetic slots with the shapes and statistics of the configurations this
+build is measured on.  A slot holds P comb-pilot symbols followed by U
+uplink data symbols, each an [M][N] array of time-domain antenna samples.
+
+Pilots follow the reference's comb layout (fft_callback.cuh:76-108): on pilot
+symbol p, subcarrier i carries user p*sg + (i % sg) with the value
+p_raw[i], where p_raw / |p_raw|^2 is the receiver's pilot table
+(fft_op.cu:176-192).  Data bits are scrambled, mapped with the Gray tables
+that the reference's soft demapper inverts (modulation/demodulation.h:30-67;
+for 256-QAM the reference's table is inverted on every bit relative to its
+demapper, so the generator flips the index to stay consistent), and placed
+on subcarrier s as stream bits s*Qm .. s*Qm+Qm-1.
+
+Channels: "iid_group" draws CN(0,1) per (group of sg subcarriers, antenna,
+user); "tdl" draws an n_taps exponential power-delay-profile channel with
+exponential antenna correlation rho (Kronecker, receive side), normalised
+to unit average power per link.  AWGN is added per subcarrier at the stated
+per-user SNR.
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import ops
+
+
+@dataclass
+class CellConfig:
+    M: int = 64            # antennas
+    K: int = 16            # users
+    N: int = 2048          # FFT size
+    S: int = 1200          # data subcarriers
+    sg: int = 16           # subcarrier group
+    Qm: int = 4            # bits per QAM symbol
+    U: int = 13            # uplink data symbols per slot
+    snr_db: float = 20.0
+    channel: str = "iid_group"   # or "tdl"
+    n_taps: int = 8
+    tap_decay: float = 2.0       # PDP e^{-l / tap_decay}, in samples
+    rho: float = 0.0             # antenna correlation
+    iq_dtype: str = "c64"        # c64 | int16 | int8 | f16
+    scrambler: str = "lfsr127"   # lfsr127 | gold
+    c_init: int = 0x1234
+    code_rate: float = 1.0 / 3.0
+    seed: int = 0
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def P(self):
+        return (self.K + self.sg - 1) // self.sg  # config.cc:75-82, main.cc:67
+
+    @property
+    def G(self):
+        return (self.S + self.sg - 1) // self.sg
+
+    @property
+    def start(self):
+        return (self.N - self.S) // 2  # config.cc:31
+
+    @property
+    def symbols(self):
+        return self.P + self.U
+
+    def ldpc(self):
+        """(cb_size, zeros, cb_stride): encoded bits, punctured bits and the
+        tight row stride of the LLR layout for one code block per symbol."""
+        e, p, _ = ops.ldpc_sizes(self.S, self.Qm, self.code_rate)
+        return e, p, e + p
+
+
+def mod_table(Qm):
+    """Reference Gray tables (modulation.cu:22-72)."""
+    if Qm == 2:
+        s = np.float32(1 / np.sqrt(2))
+        v = np.array([-s, s], np.float32)
+        idx = np.arange(4)
+        return (v[idx // 2] + 1j * v[idx % 2]).astype(np.complex64)
+    if Qm == 4:
+        s = np.float32(1 / np.sqrt(10))
+        v = np.array([1, 3, -1, -3], np.float32) * s
+        i = np.arange(16)
+        im = (((i >> 2) & 1) << 1) + (i & 1)
+        re = (((i >> 3) & 1) << 1) + ((i >> 1) & 1)
+        return (v[re] + 1j * v[im]).astype(np.complex64)
+    if Qm == 6:
+        s = np.float32(1 / np.sqrt(42))
+        v = np.array([3, 1, 5, 7, -3, -1, -5, -7], np.float32) * s
+        i = np.arange(64)
+        im = (((i >> 4) & 1) << 2) + (((i >> 2) & 1) << 1) + (i & 1)
+        re = (((i >> 5) & 1) << 2) + (((i >> 3) & 1) << 1) + ((i >> 1) & 1)
+        return (v[re] + 1j * v[im]).astype(np.complex64)
+    s = np.float32(1 / np.sqrt(170))
+    v = np.array([-15, -13, -9, -11, -1, -3, -7, -5, 15, 13, 9, 11, 1, 3, 7, 5], np.float32) * s
+    i = np.arange(256)
+    im = ((i & 0x40) >> 3) + ((i & 0x10) >> 2) + ((i & 0x4) >> 1) + (i & 0x1)
+    re = ((i & 0x80) >> 4) + ((i & 0x20) >> 3) + ((i & 0x8) >> 2) + ((i & 0x2) >> 1)
+    return (v[re] + 1j * v[im]).astype(np.complex64)
+
+
+def lfsr127():
+    """scrambler.cu:22-31."""
+    s, out = 0x5D, np.zeros(127, np.uint8)
+    for i in range(127):
+        fb = (s ^ (s >> 3)) & 1
+        out[i] = fb
+        s = (s >> 1) | (fb << 6)
+    return out
+
+
+def gold(c_init, n):
+    """TS 38.211 5.2.1 Gold sequence c(0..n-1)."""
+    Nc = 1600
+    x1 = np.zeros(n + Nc + 31, np.uint8)
+    x2 = np.zeros(n + Nc + 31, np.uint8)
+    x1[0] = 1
+    x2[:31] = [(c_init >> i) & 1 for i in range(31)]
+    for k in range(n + Nc):
+        x1[k + 31] = x1[k + 3] ^ x1[k]
+        x2[k + 31] = x2[k + 3] ^ x2[k + 2] ^ x2[k + 1] ^ x2[k]
+    return x1[Nc:Nc + n] ^ x2[Nc:Nc + n]
+
+
+def scrambling_bits(cfg, n_bits):
+    """[K][n_bits] descrambling sequence per user, as the receiver uses it."""
+    if cfg.scrambler == "gold":
+        return np.stack([gold(cfg.c_init + u, n_bits) for u in range(cfg.K)])
+    seq = lfsr127()
+    return np.tile(seq[np.arange(n_bits) % 127], (cfg.K, 1))
+
+
+def _channel(cfg, rng):
+    """Frequency response H[s][b][u] (complex64) on the S data subcarriers."""
+    M, K, S, sg = cfg.M, cfg.K, cfg.S, cfg.sg
+    if cfg.channel == "iid_group":
+        G = cfg.G
+        h = (rng.standard_normal((G, M, K)) + 1j * rng.standard_normal((G, M, K))) / np.sqrt(2)
+        return h[np.arange(S) // sg].astype(np.complex64)
+    # tdl: taps[l][b][u] with exponential PDP and receive correlation
+    L = cfg.n_taps
+    pdp = np.exp(-np.arange(L) / cfg.tap_decay)
+    pdp /= pdp.sum()
+    w = (rng.standard_normal((L, M, K)) + 1j * rng.standard_normal((L, M, K))) / np.sqrt(2)
+    if cfg.rho:
+        idx = np.arange(M)
+        R = cfg.rho ** np.abs(idx[:, None] - idx[None, :])
+        Rh = np.linalg.cholesky(R)
+        w = np.einsum("ab,lbk->lak", Rh, w)
+    taps = w * np.sqrt(pdp)[:, None, None]
+    bins = (np.arange(S) + cfg.start + cfg.N // 2) % cfg.N
+    # the data bins' physical frequency offset relative to DC
+    f = ((bins + cfg.N // 2) % cfg.N) - cfg.N // 2
+    ph = np.exp(-2j * np.pi * np.outer(f, np.arange(L)) / cfg.N)  # [S][L]
+    H = np.tensordot(ph, taps, axes=(1, 0))  # [S][M][K]
+    return H.astype(np.complex64)
+
+
+def _to_time(cfg, Y, gain):
+    """Y [sym][M][S] frequency samples -> [sym][M][N] time samples (numpy
+    inverse FFT, so the receiver's unnormalised forward FFT returns Y*gain)."""
+    n_sym = Y.shape[0]
+    row = np.zeros((n_sym, cfg.M, cfg.N), np.complex64)
+    bins = (np.arange(cfg.S) + cfg.start + cfg.N // 2) % cfg.N
+    row[:, :, bins] = Y * gain
+    x = np.fft.ifft(row, axis=-1).astype(np.complex64)
+    if cfg.iq_dtype == "c64":
+        return x
+    iq = np.stack([x.real, x.imag], axis=-1)
+    if cfg.iq_dtype == "f16":
+        return iq.astype(np.float16)
+    qmax = 32767 if cfg.iq_dtype == "int16" else 127
+    q = np.clip(np.rint(iq * (qmax + 1)), -qmax - 1, qmax)
+    return q.astype(np.int16 if cfg.iq_dtype == "int16" else np.int8)
+
+
+def make_slot(cfg):
+    """Returns a dict: iq [P+U][M][N](...), H [S][M][K], bits [U][K][S*Qm]
+    (transmitted coded bits, before scrambling), x [U][K][S] (transmitted
+    QAM symbols), noise_var, pilot_raw [S], seq [K][S*Qm]."""
+    rng = np.random.default_rng(np.random.Philox(cfg.seed))
+    M, K, S, sg, Qm, U, P = cfg.M, cfg.K, cfg.S, cfg.sg, cfg.Qm, cfg.U, cfg.P
+    H = _channel(cfg, rng)
+    ps = ops.pilot_sign(S).numpy()
+    pilot_raw = (ps / (np.abs(ps) ** 2)).astype(np.complex64)  # p = ps / |ps|^2
+    nbits = S * Qm
+    bits = rng.integers(0, 2, (U, K, nbits), dtype=np.uint8)
+    seq = scrambling_bits(cfg, nbits)
+    tx = bits ^ seq[None]
+    weights = 1 << np.arange(Qm - 1, -1, -1)
+    idx = (tx.reshape(U, K, S, Qm) * weights).sum(-1)
+    if Qm == 8:
+        idx = idx ^ 0xFF
+    X = mod_table(Qm)[idx]  # [U][K][S]
+    noise_var = 10.0 ** (-cfg.snr_db / 10.0)
+
+    Yp = np.zeros((P, M, S), np.complex64)
+    s_idx = np.arange(S)
+    for p in range(P):
+        users = p * sg + (s_idx % sg)
+        ok = users < K
+        # H[s][:, users[s]] * pilot[s]
+        hs = H[s_idx[ok], :, users[ok]]  # [n_ok][M]
+        Yp[p][:, s_idx[ok]] = (hs * pilot_raw[s_idx[ok], None]).T
+    Yu = np.matmul(H[None], X.transpose(0, 2, 1)[..., None])[..., 0]  # [U][S][M]
+    Yu = Yu.transpose(0, 2, 1)
+    Y = np.concatenate([Yp, Yu]).astype(np.complex64)
+    nz = (rng.standard_normal(Y.shape) + 1j * rng.standard_normal(Y.shape)) * np.sqrt(noise_var / 2)
+    Y = (Y + nz).astype(np.complex64)
+    # the unnormalised FFT of numpy's ifft returns Y; int formats get a gain
+    # that puts the time-domain RMS near a quarter of full scale
+    gain = 1.0
+    if cfg.iq_dtype in ("int16", "int8"):
+        rms = np.sqrt(np.mean(np.abs(Y) ** 2) * S) / cfg.N
+        gain = 0.25 / max(rms, 1e-12)
+    iq = _to_time(cfg, Y, gain)
+    return dict(iq=iq, H=H, bits=bits, x=X, noise_var=noise_var, pilot_raw=pilot_raw,
+                seq=seq, gain=gain, Y=Y)

@@ -1,0 +1,75 @@
+"""Per-slot stage runner over the C ABI (mb_slot_*): the single-GPU
+replacement of BandProcess::process (baseband/process.cc:134-225)."""
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import LIB, check
+from .ops import _dev, _stream
+
+_PREC = {"fp32": _lib.MB_ZF_FP32, "mixed": _lib.MB_ZF_MIXED, "fp64": _lib.MB_ZF_FP64}
+_IQ = {"c64": _lib.MB_IQ_C32, "int16": _lib.MB_IQ_I16, "int8": _lib.MB_IQ_I8, "f16": _lib.MB_IQ_F16}
+_SCR = {"lfsr127": _lib.MB_SCR_LFSR127, "gold": _lib.MB_SCR_GOLD}
+
+
+class UplinkSlot:
+    """Runs one uplink slot of a cell: pilot FFT -> ZF -> (FFT -> equalize)
+    per batch of uplink symbols.  cfg is a datagen.CellConfig (or anything
+    with the same fields)."""
+
+    def __init__(self, cfg, precision="fp32", sym_batch=4, use_graph=False, D=0, out_dtype="f16",
+                 ns_iters=2, cond_threshold=1e4):
+        cb, zeros, stride = cfg.ldpc()
+        self.cfg = cfg
+        self.cb_size, self.zeros, self.cb_stride = cb, zeros, stride
+        self.n_valid = min(cfg.S * cfg.Qm, cb)
+        self.hrow = (self.n_valid + 7) // 8
+        d = _lib.MbCellDesc(cfg.M, cfg.K, cfg.N, cfg.S, cfg.sg, cfg.Qm, cfg.P, cfg.U, D,
+                            _IQ[cfg.iq_dtype], cb, stride, zeros, _PREC[precision], ns_iters,
+                            cond_threshold, _SCR[cfg.scrambler], cfg.c_init, _IQ[out_dtype],
+                            sym_batch, int(use_graph))
+        h = ctypes.c_void_p()
+        check(LIB.mb_slot_create(ctypes.byref(d), ctypes.byref(h)), "mb_slot_create")
+        self._h = h
+        self.D = D
+        self.llr = torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda")
+        self.hard = torch.zeros(cfg.U, cfg.K, self.hrow, dtype=torch.uint8, device="cuda")
+        self.status = torch.zeros(cfg.G, dtype=torch.int32, device="cuda")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            LIB.mb_slot_destroy(h)
+            self._h = None
+
+    def __call__(self, iq, llr=None, hard=None, stream=None):
+        llr = self.llr if llr is None else llr
+        hard = self.hard if hard is None else hard
+        check(LIB.mb_slot_uplink(self._h, _dev(iq, "iq"), _dev(llr, "llr"), _dev(hard, "hard"),
+                                 _dev(self.status, "status"), _stream(stream)), "mb_slot_uplink")
+        return llr, hard
+
+    def downlink(self, symbols, out, stream=None):
+        check(LIB.mb_slot_downlink(self._h, _dev(symbols, "symbols"), _dev(out, "out"), _stream(stream)),
+              "mb_slot_downlink")
+        return out
+
+    def buffers(self):
+        """(W [G, M, K], precoder [G, K, M]) as torch views of the slot's buffers."""
+        c, p = ctypes.c_void_p(), ctypes.c_void_p()
+        check(LIB.mb_slot_buffers(self._h, ctypes.byref(c), ctypes.byref(p)), "mb_slot_buffers")
+        cfg = self.cfg
+        n = cfg.G * cfg.M * cfg.K
+        W = _wrap(c.value, n).view(cfg.G, cfg.M, cfg.K)
+        P = _wrap(p.value, n).view(cfg.G, cfg.K, cfg.M)
+        return W, P
+
+
+def _wrap(ptr, n):
+    """A complex64 torch view of n elements of library-owned device memory."""
+    class _Holder:
+        pass
+    h = _Holder()
+    h.__cuda_array_interface__ = {"shape": (n,), "typestr": "<c8", "data": (ptr, False), "version": 3}
+    return torch.as_tensor(h, device="cuda")
