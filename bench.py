@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the per-slot uplink hot path on B200.
+
+Workload (one "step" = one uplink slot of one cell): 256 antennas x 32 users,
+4096-point FFT with 3276 data subcarriers, 14 OFDM symbols (2 comb-pilot
+symbols + 12 data symbols), 64-QAM at 25 dB SNR over an 8-tap exponential
+power-delay-profile channel with antenna correlation 0.5; complex float32
+time-domain samples in.  Per slot: pilot FFT + LS estimate, per-group ZF
+(Gram, inverse, detector), uplink FFT, equalize + FP16 LLR demod + descrambled
+hard bits.  Inputs are seeded synthetic slots (megastation_b200.datagen).
+
+Lines printed (rank 0): one JSON object.  Multi-GPU (torchrun): replicas, one
+independent slot stream per GPU (the path has no exchange step).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=12, snr_db=25.0, channel="tdl",
+                n_taps=8, tap_decay=2.0, rho=0.5, iq_dtype="c64", seed=2024)
+METRIC = "slots/s"
+UNIT = "slots/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
+    ap.add_argument("--sym-batch", type=int, default=4)
+    ap.add_argument("--rotate", type=int, default=4, help="distinct input slots cycled (L2 flush)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def algorithmic_bytes(cfg, b_in=8):
+    """Compulsory bytes of one uplink slot: samples in, FP16 LLRs and packed
+    hard bits out (intermediates excluded)."""
+    cb, zeros, stride = cfg.ldpc()
+    n_valid = min(cfg.S * cfg.Qm, cb)
+    return (cfg.P + cfg.U) * cfg.M * cfg.N * b_in + cfg.U * cfg.K * n_valid * 2 + \
+        cfg.U * cfg.K * ((n_valid + 7) // 8)
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def cpu_baseline(cfg, slot_np, seconds):
+    """Host C++/OpenMP restatement of the same slot (oracle), all host threads."""
+    from oracle import oracle as orc
+    cb, zeros, stride = cfg.ldpc()
+    ps = orc.pilot_sign(cfg.S)
+    seq = slot_np["seq"][0]
+    threads = os.cpu_count() or 1
+    n, t0 = 0, time.perf_counter()
+    while True:
+        orc.slot_uplink_cpu(slot_np["iq"], cfg.P, cfg.U, cfg.K, cfg.N, cfg.S, cfg.sg, cfg.Qm, cb, stride,
+                            zeros, ps, seq, threads=threads)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 200:
+            break
+    return {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} full slots of the bench workload (FP32, OpenMP, {threads} threads) in {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    from megastation_b200 import datagen
+    if rank != 0:
+        return
+    cfg = datagen.CellConfig(**WORKLOAD)
+    d = datagen.make_slot(cfg)
+    from oracle import oracle as orc
+    cb, zeros, stride = cfg.ldpc()
+    ps = orc.pilot_sign(cfg.S)
+    threads = os.cpu_count() or 1
+    # bounded sample per step: one full slot per step
+    for _ in range(max(0, min(args.warmup, 1))):
+        orc.slot_uplink_cpu(d["iq"], cfg.P, cfg.U, cfg.K, cfg.N, cfg.S, cfg.sg, cfg.Qm, cb, stride, zeros, ps,
+                            d["seq"][0], threads=threads)
+    steps = max(1, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        orc.slot_uplink_cpu(d["iq"], cfg.P, cfg.U, cfg.K, cfg.N, cfg.S, cfg.sg, cfg.Qm, cb, stride, zeros, ps,
+                            d["seq"][0], threads=threads)
+    el = time.perf_counter() - t0
+    v = steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * el / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": workload_config(cfg, args),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{steps} full slots, FP32 host C++/OpenMP restatement of the "
+                                       f"reference operators ({threads} threads)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(cfg, args):
+    return {"workload": "uplink slot 256x32, N=4096, S=3276, 2 pilot + 12 data symbols, 64-QAM, "
+                        "8-tap exp-PDP rho=0.5, 25 dB, c64 samples",
+            "M": cfg.M, "K": cfg.K, "N": cfg.N, "S": cfg.S, "sg": cfg.sg, "Qm": cfg.Qm, "P": cfg.P,
+            "U": cfg.U, "precision": args.precision, "sym_batch": args.sym_batch,
+            "l2": f"inputs {cfg.symbols * cfg.M * cfg.N * 8 / 1e6:.0f} MB per slot, {args.rotate} "
+                  "slots rotated (larger than the 126 MB L2)",
+            "seed": cfg.seed}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    import megastation_b200 as mb
+    from megastation_b200 import datagen, slot
+    cfg = datagen.CellConfig(**WORKLOAD)
+    d = datagen.make_slot(cfg)
+    cb, zeros, stride = cfg.ldpc()
+    n_valid = min(cfg.S * cfg.Qm, cb)
+    hrow = (n_valid + 7) // 8
+
+    R = max(2, args.rotate)
+    iq_host = torch.from_numpy(d["iq"]).pin_memory()
+    iq_dev = [iq_host.cuda() for _ in range(R)]
+    stream = torch.cuda.Stream()
+    run = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=True)
+    llr = [torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda") for _ in range(2)]
+    hard = [torch.zeros(cfg.U, cfg.K, hrow, dtype=torch.uint8, device="cuda") for _ in range(2)]
+
+    def step(k, s=stream):
+        run(iq_dev[k % R], llr[k % 2], hard[k % 2], stream=s)
+
+    # graphs are per pointer set: capture every (input, output) combination
+    with torch.cuda.stream(stream):
+        for k in range(max(args.warmup, 2 * R)):
+            step(k)
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+
+    # ---- timed region: K slots, device-resident inputs, graph replay
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record(stream)
+    for k in range(args.steps):
+        step(k)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms / 1e3)
+    launches_per_slot = 2 + (1 if cfg.S % cfg.sg else 0) + 2 * ((cfg.U + args.sym_batch - 1) // args.sym_batch)
+
+    # ---- roofline pass: same slots with per-stage CUDA events (direct launches)
+    run_t = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=False)
+    with torch.cuda.stream(stream):
+        for k in range(3):
+            run_t(iq_dev[k % R], llr[0], hard[0], stream=stream)
+        stream.synchronize()
+        run_t.timing(args.steps)
+        for k in range(args.steps):
+            run_t(iq_dev[k % R], llr[k % 2], hard[k % 2], stream=stream)
+    stream.synchronize()
+    st = run_t.stage_ms()
+    hbm_peak, tc_peak, peak_kind = measured_peaks()
+    sb = args.sym_batch
+    fft_bytes = sb * cfg.M * (cfg.N * 8 + cfg.S * 8)   # samples in, y out
+    fft_ms = st["uplink_fft"] / max(st["n_fft"], 1)
+    eq_ms = st["equalize"] / max(st["n_eq"], 1)
+    eq_bytes = cfg.G * cfg.M * cfg.K * 8 + sb * cfg.M * cfg.S * 8 + sb * cfg.K * (n_valid * 2 + hrow)
+    eq_flops = 8.0 * cfg.K * cfg.M * cfg.S * sb
+    stages = {k: st[k] / max(st["calls"], 1) for k in ("pilot_fft", "zf", "uplink_fft", "equalize", "slot")}
+    # the dominant kernel by share of the slot
+    per_slot_fft = st["uplink_fft"] / max(st["calls"], 1) * (cfg.U / sb) / max((cfg.U / sb - 1), 1)
+    per_slot_eq = stages["equalize"]
+    if per_slot_eq >= per_slot_fft and args.precision == "mixed":
+        ach = eq_flops / (eq_ms / 1e3) / 1e12
+        roof = {"kernel": "equalize (tensor cores)", "bound": "tensor", "achieved": ach, "peak": tc_peak,
+                "unit": "TFLOP/s", "frac": ach / tc_peak, "traffic": None}
+    elif per_slot_eq >= per_slot_fft:
+        ach = eq_bytes / (eq_ms / 1e3) / 1e9
+        roof = {"kernel": "equalize_fp32_kernel", "bound": "hbm", "achieved": ach, "peak": hbm_peak,
+                "unit": "GB/s", "frac": ach / hbm_peak, "traffic": None,
+                "flops_tflops": eq_flops / (eq_ms / 1e3) / 1e12}
+    else:
+        ach = fft_bytes / (fft_ms / 1e3) / 1e9
+        roof = {"kernel": "fft_kernel<12, uplink>", "bound": "hbm", "achieved": ach, "peak": hbm_peak,
+                "unit": "GB/s", "frac": ach / hbm_peak, "traffic": None}
+    roof["peak_source"] = f"{peak_kind} (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback"
+    roof["stage_ms_per_slot"] = stages
+    roof["uplink_fft"] = {"ms_per_launch": fft_ms, "bytes_per_launch": fft_bytes,
+                          "GB_s": fft_bytes / (fft_ms / 1e3) / 1e9}
+    roof["equalize"] = {"ms_per_launch": eq_ms, "bytes_per_launch": eq_bytes,
+                        "GB_s": eq_bytes / (eq_ms / 1e3) / 1e9, "TFLOP_s": eq_flops / (eq_ms / 1e3) / 1e12}
+    slot_bytes = algorithmic_bytes(cfg)
+    roof["slot"] = {"bytes": slot_bytes, "GB_s": slot_bytes * value / world / 1e9,
+                    "frac_of_hbm": slot_bytes * value / world / 1e9 / hbm_peak}
+
+    # ---- e2e: public API with host buffers, H2D of each slot and D2H of LLRs+bits
+    e2e = None
+    if not args.no_e2e:
+        cp_s, d2h_s = torch.cuda.Stream(), torch.cuda.Stream()
+        dev_in = [torch.empty_like(iq_dev[0]) for _ in range(2)]
+        host_llr = [torch.empty(llr[0].shape, dtype=llr[0].dtype).pin_memory() for _ in range(2)]
+        host_hard = [torch.empty(hard[0].shape, dtype=hard[0].dtype).pin_memory() for _ in range(2)]
+        ev_in = [torch.cuda.Event() for _ in range(2)]
+        ev_done = [torch.cuda.Event() for _ in range(2)]
+        ev_free = [torch.cuda.Event() for _ in range(2)]
+        ev_out = [torch.cuda.Event() for _ in range(2)]
+        run_e = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=True)
+
+        def e2e_steps(n, t_start=None, t_end=None):
+            for k in range(n):
+                b = k % 2
+                with torch.cuda.stream(cp_s):
+                    if k >= 2:
+                        cp_s.wait_event(ev_free[b])
+                    if k == 0 and t_start is not None:
+                        t_start.record(cp_s)
+                    dev_in[b].copy_(iq_host, non_blocking=True)
+                    ev_in[b].record(cp_s)
+                stream.wait_event(ev_in[b])
+                if k >= 2:
+                    stream.wait_event(ev_out[b])
+                run_e(dev_in[b], llr[b], hard[b], stream=stream)
+                ev_done[b].record(stream)
+                ev_free[b].record(stream)
+                with torch.cuda.stream(d2h_s):
+                    d2h_s.wait_event(ev_done[b])
+                    host_llr[b].copy_(llr[b], non_blocking=True)
+                    host_hard[b].copy_(hard[b], non_blocking=True)
+                    ev_out[b].record(d2h_s)
+            if t_end is not None:
+                for b in range(2):
+                    stream.wait_event(ev_out[b])
+                t_end.record(stream)
+
+        e2e_steps(4)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        e2e_steps(args.steps, a0, a1)
+        torch.cuda.synchronize()
+        ems = a0.elapsed_time(a1)
+        if dist:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * args.steps / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": iq_host.numel() * iq_host.element_size(),
+               "d2h_bytes_per_step": llr[0].numel() * 2 + hard[0].numel(),
+               "pipeline": "double-buffered: H2D of slot k+1 and D2H of slot k-1 overlap slot k"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(cfg, d, args.cpu_seconds)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "us_per_slot": 1e3 * ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator, megastation_b200.datagen)",
+            "config": workload_config(cfg, args), "clocks": clk, "e2e": e2e,
+            "gpu_launches": launches_per_slot * args.steps, "roofline": roof, "cpu_baseline": cpu,
+            "parallelism": f"replicas x{world}"}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

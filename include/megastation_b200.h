@@ -70,6 +70,11 @@ const char *mb_version(void);
  * every create function for the current device. */
 mb_status mb_tables_init(int device);
 
+/* Device error word of the current device: bits set by kernels whose
+ * bounded waits gave up (1 = mbarrier wait timeout).  Synchronises the
+ * device, copies the word to *out and clears it when clear != 0. */
+mb_status mb_device_error(int *out, int clear);
+
 /* Host-side pilot sequence p/|p|^2 of length S (fft/fft_op.cu:176-192 over
  * utils.h:54-95).  out: S host complex values. */
 mb_status mb_pilot_sign(uint64_t S, mb_c32 *out);
@@ -198,6 +203,21 @@ mb_status mb_equalize(const mb_c32 *W, const mb_c32 *y, uint32_t K,
                       uint8_t *hard, const mb_scrambler *scr, mb_c32 *x,
                       void *stream);
 
+/* Mixed-precision equalize on the tensor cores (no reference counterpart;
+ * same contract and outputs as mb_equalize): BF16 W and y, FP32
+ * accumulation (tcgen05.mma), the same FP16 demapper and layouts.  The
+ * caller provides two device scratch buffers whose sizes
+ * mb_equalize_tc_scratch returns.  Requires sg % 8 == 0 and K <= 64. */
+mb_status mb_equalize_tc_scratch(uint32_t K, uint32_t M, uint32_t S,
+                                 uint32_t sg, uint32_t n_sym,
+                                 uint64_t *img_bytes, uint64_t *ylp_bytes);
+mb_status mb_equalize_tc(const mb_c32 *W, const mb_c32 *y, uint32_t K,
+                         uint32_t M, uint32_t S, uint32_t sg, uint32_t n_sym,
+                         uint32_t Qm, uint64_t cb_size, uint64_t cb_stride,
+                         uint64_t zeros, uint32_t cb_blocks, uint16_t *llr,
+                         uint8_t *hard, const mb_scrambler *scr, mb_c32 *x,
+                         void *scratch_img, void *scratch_ylp, void *stream);
+
 /* ------------------------------------------------------------ precode --- */
 /* Precode::precode (sgemv/precode.h:59-61, precode_kernel.cuh:255-262)
  * batched over n_sym symbols: out[b][(s + start + N/2) % N] =
@@ -264,6 +284,16 @@ mb_status mb_slot_uplink(mb_slot *slot, const void *iq, uint16_t *llr,
  * out_dtype. */
 mb_status mb_slot_downlink(mb_slot *slot, const mb_c32 *symbols, void *out,
                            void *stream);
+
+/* Stage timing.  mb_slot_timing(slot, n) makes the next n slot calls record
+ * CUDA events around each stage on the launching stream (0 disables);
+ * mb_slot_stage_ms waits for those events and returns, summed over the
+ * recorded calls: [0] pilot FFT, [1] ZF (+ tail fill), [2] uplink FFT
+ * batches issued on the launching stream, [3] equalize, [4] whole slot,
+ * [5] number of uplink FFT launches timed in [2], [6] equalize launches,
+ * [7] recorded calls; then clears the record. */
+mb_status mb_slot_timing(mb_slot *slot, uint32_t max_calls);
+mb_status mb_slot_stage_ms(mb_slot *slot, double *out8);
 
 /* Device views of the slot's internal buffers (for inspection and tests):
  * CSI/W [G][M][K], precoder [G][K][M]. */

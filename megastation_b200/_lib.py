@@ -97,6 +97,10 @@ def _load():
         "mb_scrambler_destroy": (ST, [VP]),
         "mb_equalize": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U64, U64, U64, U32,
                              VP, VP, VP, VP, VP]),
+        "mb_equalize_tc_scratch": (ST, [U32, U32, U32, U32, U32, ctypes.POINTER(U64), ctypes.POINTER(U64)]),
+        "mb_equalize_tc": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U64, U64, U64, U32,
+                                VP, VP, VP, VP, VP, VP, VP]),
+        "mb_device_error": (ST, [ctypes.POINTER(ctypes.c_int), I32]),
         "mb_precode": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U32, VP, VP]),
         "mb_modulate": (ST, [VP, VP, U64, U64, U64, U32, U32, VP, VP]),
         "mb_scramble": (ST, [VP, VP, U64, U64, VP]),
@@ -105,6 +109,8 @@ def _load():
         "mb_slot_uplink": (ST, [VP, VP, VP, VP, VP, VP]),
         "mb_slot_downlink": (ST, [VP, VP, VP, VP]),
         "mb_slot_buffers": (ST, [VP, ctypes.POINTER(VP), ctypes.POINTER(VP)]),
+        "mb_slot_timing": (ST, [VP, U32]),
+        "mb_slot_stage_ms": (ST, [VP, ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

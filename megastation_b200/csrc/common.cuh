@@ -56,9 +56,12 @@ inline int ilog2(uint64_t x) {
 
 // Per-device table registry (twiddles, scrambler bits).
 struct DeviceTables {
-  // twiddle tables w_N[m] = exp(-2 pi i m / N), N = 2^l, l in [4, 13]
+  // Stockham twiddle tables per N = 2^l, l in [4, 13]: for each pass p >= 1
+  // (radix R, Ns = product of earlier radices) the R x Ns block
+  // exp(-2 pi i r k / (Ns R)) at [r][k], blocks concatenated by pass
   float2 *twiddle[14];
   uint32_t *lfsr127_bits;  // 127 bits packed LSB-first in 4 words
+  int *err;                // device error word (mb_tc error bits)
 };
 const DeviceTables *device_tables();  // for the current device; nullptr on error
 

@@ -1,0 +1,36 @@
+// eq_tc.cuh -- tensor-core equalizer interface.
+#pragma once
+#include <cuda_bf16.h>
+
+#include "sgemv.cuh"
+
+namespace mb {
+
+struct EqTcParams {
+  EqParams p;                 // shapes, layout and epilogue outputs
+  const uint8_t *a_img;       // per-group detector images (BF16)
+  const __nv_bfloat16 *y_lp;  // [nb][re|im][M][S_pad]
+  uint32_t S_pad, Mp, nkt, N, l0, tmem_cols;
+  int *err;
+};
+
+struct TcShape {
+  uint32_t MM;               // MMA rows: 64 (K <= 32) or 128 (K <= 64)
+  uint32_t Mp;               // antennas padded to the 64-wide k tile
+  uint32_t nkt;              // k tiles: 2 * Mp / 64
+  uint64_t img_group_bytes;  // detector image bytes per group
+};
+
+TcShape tc_shape(uint32_t M, uint32_t K);
+bool equalize_tc_supported(uint32_t K, uint32_t sg, uint32_t nb);
+// W [G][M][K] c32 -> detector images
+mb_status w_image(const float2 *W, void *img, uint32_t G, uint32_t M, uint32_t K,
+                  cudaStream_t st);
+// equalize nb symbols (outputs at symbol offset l0 of p's outputs)
+mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, uint32_t S_pad,
+                      uint32_t l0, uint32_t nb, int *err, cudaStream_t st);
+// y [nb][M][S] c32 -> y_lp [nb][re|im][M][S_pad] BF16
+mb_status y_to_lp(const float2 *y, void *y_lp, uint32_t nb, uint32_t M, uint32_t S,
+                  uint32_t S_pad, cudaStream_t st);
+
+}  // namespace mb

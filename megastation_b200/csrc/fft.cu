@@ -14,23 +14,28 @@
 // discrete Fourier transforms on graphics processors", SC'08), radix 16
 // passes plus one radix 2/4/8 pass for N = 2^n, n in [4, 13].  Each thread
 // owns 16 complex values; a row of N points uses N/16 threads, and a CTA
-// holds max(1, 256/(N/16)) rows.  Twiddles come from a per-device table
-// w_N[m] = exp(-2 pi i m/N) computed in double at init.
+// holds max(1, 256/(N/16)) rows.  Twiddles come from per-device tables
+// computed in double at init and laid out per pass as [r][k], so a warp's
+// twiddle loads are coalesced.
+#include <cuda_bf16.h>
+
 #include <atomic>
 
 #include "common.cuh"
+#include "fft.cuh"
 
 namespace mb {
 
-enum FftMode { kUplink = 0, kPilot = 1, kIfft = 2 };
+enum FftMode { kUplink = 0, kPilot = 1, kIfft = 2, kUplinkLP = 3 };
 
 struct FftParams {
   const void *in;
   void *out;
-  const float2 *tw;      // w_N table
+  const float2 *tw;      // Stockham twiddle table of N
   const float2 *pilot;   // pilot sign (kPilot), device
   uint64_t rows;         // n_sym * M
   uint32_t M, S, start, K, sg, ue_start;
+  uint32_t S_pad;        // kUplinkLP row pitch (elements)
   int in_dtype, out_dtype;
 };
 
@@ -145,8 +150,16 @@ struct Plan {
   static constexpr int RLAST = 1 << (LOGN % 4);    // trailing radix (1: none)
   static constexpr int PASSES = P16 + (RLAST > 1 ? 1 : 0);
   static constexpr int PADN = N + N / 16;          // padded smem row
-  static __device__ __forceinline__ int radix(int p) {
+  static __host__ __device__ __forceinline__ constexpr int radix(int p) {
     return p < P16 ? 16 : RLAST;
+  }
+  // product of the radices before pass p
+  static __host__ __device__ __forceinline__ constexpr int ns(int p) {
+    return p == 0 ? 1 : ns(p - 1) * radix(p - 1);
+  }
+  // offset of pass p's [r][k] block in the twiddle table
+  static __host__ __device__ __forceinline__ constexpr int tw_off(int p) {
+    return p <= 1 ? 0 : tw_off(p - 1) + radix(p - 1) * ns(p - 1);
   }
 };
 
@@ -178,6 +191,15 @@ __device__ __forceinline__ void epilogue(const FftParams &p, uint64_t row,
   if constexpr (MODE == kUplink) {
     uint32_t i = (k - p.start - N / 2) & (N - 1);
     if (i < p.S) reinterpret_cast<float2 *>(p.out)[row * p.S + i] = v;
+  } else if constexpr (MODE == kUplinkLP) {
+    // planar BF16 rows for the tensor-core equalizer: [sym][re|im][M][S_pad]
+    uint32_t i = (k - p.start - N / 2) & (N - 1);
+    if (i < p.S) {
+      const uint64_t sym = row / p.M, b = row % p.M;
+      __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(p.out);
+      o[((sym * 2 + 0) * p.M + b) * p.S_pad + i] = __float2bfloat16_rn(v.x);
+      o[((sym * 2 + 1) * p.M + b) * p.S_pad + i] = __float2bfloat16_rn(v.y);
+    }
   } else if constexpr (MODE == kPilot) {
     uint32_t i = (k - p.start - N / 2) & (N - 1);
     if (i < p.S) {
@@ -260,7 +282,7 @@ __global__ void __launch_bounds__(Plan<LOGN>::THREADS)
       for (int bi = 0; bi < 16; bi++) {
         const int j = t + (bi / R) * T, r = bi % R;
         if (r) {
-          const int m = r * (j % Ns) * (N / (Ns * R));
+          const int m = PL::tw_off(pass) + r * Ns + (j % Ns);
           float2 w = __ldg(p.tw + m);
           if (INV) w.y = -w.y;
           v[bi] = cmul(v[bi], w);
@@ -408,6 +430,22 @@ extern "C" mb_status mb_fft_uplink(mb_fft *f, const void *iq, int iq_dtype,
   p.start = f->d.ofdm_start;
   p.in_dtype = iq_dtype;
   return launch_fft<kUplink>(f->logn, p, as_stream(stream));
+}
+
+mb_status mb::fft_uplink_lp(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
+                            void *y_lp, uint32_t S_pad, cudaStream_t st) {
+  if (!f || !iq || !y_lp || !dtype_ok(iq_dtype) || S_pad < f->d.ofdm_num) return MB_BAD_ARG;
+  FftParams p{};
+  p.in = iq;
+  p.out = y_lp;
+  p.tw = f->tw;
+  p.rows = (uint64_t)n_sym * f->d.bs_num;
+  p.M = f->d.bs_num;
+  p.S = f->d.ofdm_num;
+  p.start = f->d.ofdm_start;
+  p.S_pad = S_pad;
+  p.in_dtype = iq_dtype;
+  return launch_fft<kUplinkLP>(f->logn, p, st);
 }
 
 extern "C" mb_status mb_fft_pilot(mb_fft *f, const void *iq, int iq_dtype,

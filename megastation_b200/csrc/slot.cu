@@ -9,6 +9,7 @@
 // FFT forked onto a side stream so it overlaps the ZF solve.  Optionally the
 // whole uplink slot is captured once into a CUDA graph and replayed.
 #include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 #include "sgemv.cuh"
@@ -37,7 +38,53 @@ struct mb_slot {
   uint8_t *g_hard;
   int32_t *g_status;
   cudaStream_t g_stream;
+  // stage timing: per recorded call, events at stage boundaries
+  struct Marks {
+    cudaEvent_t start, pilot, zf, end;
+    std::vector<cudaEvent_t> fft_b, fft_e, eq_b, eq_e;
+  };
+  std::vector<Marks> marks;
+  uint32_t marks_used = 0, marks_max = 0;
 };
+
+static cudaEvent_t new_event() {
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// the current call's marks, or null when timing is off or exhausted
+static mb_slot::Marks *next_marks(mb_slot *s) {
+  if (s->marks_used >= s->marks_max) return nullptr;
+  if (s->marks.size() <= s->marks_used) {
+    mb_slot::Marks m;
+    m.start = new_event();
+    m.pilot = new_event();
+    m.zf = new_event();
+    m.end = new_event();
+    const uint32_t nb = (s->c.U + s->c.sym_batch - 1) / s->c.sym_batch + 1;
+    for (uint32_t i = 0; i < nb; i++) {
+      m.fft_b.push_back(new_event());
+      m.fft_e.push_back(new_event());
+      m.eq_b.push_back(new_event());
+      m.eq_e.push_back(new_event());
+    }
+    s->marks.push_back(m);
+  }
+  return &s->marks[s->marks_used++];
+}
+
+static void free_marks(mb_slot *s) {
+  for (auto &m : s->marks) {
+    cudaEventDestroy(m.start);
+    cudaEventDestroy(m.pilot);
+    cudaEventDestroy(m.zf);
+    cudaEventDestroy(m.end);
+    for (auto *v : {&m.fft_b, &m.fft_e, &m.eq_b, &m.eq_e})
+      for (auto e : *v) cudaEventDestroy(e);
+  }
+  s->marks.clear();
+}
 
 static size_t iq_elem_bytes(int dt) {
   return dt == MB_IQ_C32 ? 8 : dt == MB_IQ_I8 ? 2 : 4;
@@ -46,6 +93,7 @@ static size_t iq_elem_bytes(int dt) {
 extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   if (!s) return MB_BAD_ARG;
   if (s->graph) cudaGraphExecDestroy(s->graph);
+  free_marks(s);
   if (s->fft) mb_fft_destroy(s->fft);
   if (s->scr) mb_scrambler_destroy(s->scr);
   cudaFree(s->csi);
@@ -115,8 +163,11 @@ extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
 
 static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
                               uint8_t *hard, int32_t *status,
-                              cudaStream_t st) {
+                              cudaStream_t st, mb_slot::Marks *mk) {
   const mb_cell_desc &c = s->c;
+#define MARK(ev) \
+  if (mk) MB_CUDA_TRY(cudaEventRecord((ev), st))
+  MARK(mk->start);
   const size_t sym_bytes = iq_elem_bytes(c.iq_dtype) * c.M * c.N;
   const char *iq_b = reinterpret_cast<const char *>(iq);
   mb_status r;
@@ -133,6 +184,7 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   // pilots -> CSI -> W (+ precoder)
   r = mb_fft_pilot(s->fft, iq, c.iq_dtype, c.P, 0, reinterpret_cast<mb_c32 *>(s->csi), st);
   if (r != MB_OK) return r;
+  MARK(mk->pilot);
   r = zf_fill_tail(s->csi, s->G, c.S, c.sg, c.M, c.K, st);
   if (r != MB_OK) return r;
   float2 *prec = c.D ? s->precoder : nullptr;
@@ -143,21 +195,32 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, st);
   }
   if (r != MB_OK) return r;
-  if (!c.U) return MB_OK;
+  MARK(mk->zf);
+  if (!c.U) {
+    MARK(mk->end);
+    return MB_OK;
+  }
   MB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
   const uint64_t llr_sym = (uint64_t)c.K * c.cb_stride;
   const uint64_t hard_sym = (uint64_t)c.K * s->hrow;
-  for (uint32_t l0 = 0; l0 < c.U; l0 += c.sym_batch) {
+  uint32_t bi = 0;
+  for (uint32_t l0 = 0; l0 < c.U; l0 += c.sym_batch, bi++) {
     const uint32_t nb = std::min(c.sym_batch, c.U - l0);
     if (l0) {
+      MARK(mk->fft_b[bi]);
       r = mb_fft_uplink(s->fft, iq_b + (size_t)(c.P + l0) * sym_bytes, c.iq_dtype, nb,
                         reinterpret_cast<mb_c32 *>(s->y), st);
       if (r != MB_OK) return r;
+      MARK(mk->fft_e[bi]);
     }
+    MARK(mk->eq_b[bi]);
     r = slot_equalize(s->c, s->csi, s->y, s->y_lp, nb, llr + l0 * llr_sym,
                       hard ? hard + l0 * hard_sym : nullptr, s->scr, st);
     if (r != MB_OK) return r;
+    MARK(mk->eq_e[bi]);
   }
+  MARK(mk->end);
+#undef MARK
   return MB_OK;
 }
 
@@ -177,7 +240,8 @@ extern "C" mb_status mb_slot_uplink(mb_slot *s, const void *iq, uint16_t *llr,
                                     void *stream) {
   if (!s || !iq || (s->c.U && !llr)) return MB_BAD_ARG;
   cudaStream_t st = as_stream(stream);
-  if (!s->c.use_graph) return issue_uplink(s, iq, llr, hard, status, st);
+  if (!s->c.use_graph || s->marks_max)
+    return issue_uplink(s, iq, llr, hard, status, st, next_marks(s));
   if (!st) return MB_BAD_ARG;  // the legacy stream cannot be captured
   if (!s->graph || s->g_iq != iq || s->g_llr != llr || s->g_hard != hard ||
       s->g_status != status || s->g_stream != st) {
@@ -186,7 +250,7 @@ extern "C" mb_status mb_slot_uplink(mb_slot *s, const void *iq, uint16_t *llr,
       s->graph = nullptr;
     }
     MB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    mb_status r = issue_uplink(s, iq, llr, hard, status, st);
+    mb_status r = issue_uplink(s, iq, llr, hard, status, st, nullptr);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (r != MB_OK) {
@@ -222,6 +286,45 @@ extern "C" mb_status mb_slot_downlink(mb_slot *s, const mb_c32 *symbols,
   if (r != MB_OK) return r;
   return mb_ifft_downlink(s->fft, reinterpret_cast<const mb_c32 *>(s->precoded), c.D,
                           out, c.out_dtype, st);
+}
+
+extern "C" mb_status mb_slot_timing(mb_slot *s, uint32_t max_calls) {
+  if (!s) return MB_BAD_ARG;
+  s->marks_max = max_calls;
+  s->marks_used = 0;
+  // create the events now, outside any timed region
+  for (uint32_t i = 0; i < max_calls; i++) next_marks(s);
+  s->marks_used = 0;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_slot_stage_ms(mb_slot *s, double *out) {
+  if (!s || !out) return MB_BAD_ARG;
+  for (int i = 0; i < 8; i++) out[i] = 0;
+  auto ms = [](cudaEvent_t a, cudaEvent_t b) {
+    float v = 0.f;
+    cudaEventElapsedTime(&v, a, b);
+    return (double)v;
+  };
+  for (uint32_t k = 0; k < s->marks_used; k++) {
+    auto &m = s->marks[k];
+    MB_CUDA_TRY(cudaEventSynchronize(m.end));
+    out[0] += ms(m.start, m.pilot);
+    out[1] += ms(m.pilot, m.zf);
+    out[4] += ms(m.start, m.end);
+    uint32_t bi = 0;
+    for (uint32_t l0 = 0; l0 < s->c.U; l0 += s->c.sym_batch, bi++) {
+      if (l0) {
+        out[2] += ms(m.fft_b[bi], m.fft_e[bi]);
+        out[5] += 1;
+      }
+      out[3] += ms(m.eq_b[bi], m.eq_e[bi]);
+      out[6] += 1;
+    }
+    out[7] += 1;
+  }
+  s->marks_used = 0;
+  return MB_OK;
 }
 
 extern "C" mb_status mb_slot_buffers(mb_slot *s, mb_c32 **csi, mb_c32 **precoder) {

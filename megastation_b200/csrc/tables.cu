@@ -25,14 +25,26 @@ static mb_status build_tables(DeviceTables &t) {
   for (int l = 0; l < 14; l++) t.twiddle[l] = nullptr;
   t.lfsr127_bits = nullptr;
   for (int l = 4; l <= 13; l++) {
-    uint32_t n = 1u << l;
-    std::vector<float2> h(n);
-    for (uint32_t m = 0; m < n; m++) {
-      double a = -2.0 * M_PI * (double)m / (double)n;
-      h[m] = make_float2((float)cos(a), (float)sin(a));
+    // Stockham pass tables: pass p >= 1 (radix R, Ns = product of the
+    // earlier radices) holds exp(-2 pi i r k / (Ns R)) at [r][k], so the
+    // threads of a warp (consecutive k) read consecutive entries.
+    std::vector<float2> h;
+    uint32_t ns = 1;
+    const int p16 = l / 4, rlast = 1 << (l % 4);
+    const int passes = p16 + (rlast > 1 ? 1 : 0);
+    for (int p = 0; p < passes; p++) {
+      const uint32_t R = p < p16 ? 16 : rlast;
+      if (p > 0)
+        for (uint32_t r = 0; r < R; r++)
+          for (uint32_t k = 0; k < ns; k++) {
+            double a = -2.0 * M_PI * (double)(r * k) / (double)(ns * R);
+            h.push_back(make_float2((float)cos(a), (float)sin(a)));
+          }
+      ns *= R;
     }
-    MB_CUDA_TRY(cudaMalloc(&t.twiddle[l], sizeof(float2) * n));
-    MB_CUDA_TRY(cudaMemcpy(t.twiddle[l], h.data(), sizeof(float2) * n,
+    if (h.empty()) h.push_back(make_float2(1.f, 0.f));
+    MB_CUDA_TRY(cudaMalloc(&t.twiddle[l], sizeof(float2) * h.size()));
+    MB_CUDA_TRY(cudaMemcpy(t.twiddle[l], h.data(), sizeof(float2) * h.size(),
                            cudaMemcpyHostToDevice));
   }
   // scrambler/scrambler.cu:22-31: x^7 + x^4 + 1 from 0x5D
@@ -44,6 +56,8 @@ static mb_status build_tables(DeviceTables &t) {
     s >>= 1;
     s |= fb << 6;
   }
+  MB_CUDA_TRY(cudaMalloc(&t.err, sizeof(int)));
+  MB_CUDA_TRY(cudaMemset(t.err, 0, sizeof(int)));
   MB_CUDA_TRY(cudaMalloc(&t.lfsr127_bits, sizeof(words)));
   MB_CUDA_TRY(cudaMemcpy(t.lfsr127_bits, words, sizeof(words),
                          cudaMemcpyHostToDevice));
@@ -122,6 +136,16 @@ extern "C" mb_status mb_tables_init(int device) {
   const DeviceTables *t = device_tables();
   if (device != cur) MB_CUDA_TRY(cudaSetDevice(cur));
   return t ? MB_OK : MB_CUDA_ERROR;
+}
+
+extern "C" mb_status mb_device_error(int *out, int clear) {
+  if (!out) return MB_BAD_ARG;
+  const DeviceTables *t = device_tables();
+  if (!t) return MB_CUDA_ERROR;
+  MB_CUDA_TRY(cudaDeviceSynchronize());
+  MB_CUDA_TRY(cudaMemcpy(out, t->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (clear) MB_CUDA_TRY(cudaMemset(t->err, 0, sizeof(int)));
+  return MB_OK;
 }
 
 extern "C" mb_status mb_pilot_sign(uint64_t S, mb_c32 *out) {

@@ -227,6 +227,37 @@ class Equalize:
                               hp, sp, xp, _stream(stream)), "Equalize.equalize")
 
 
+    @staticmethod
+    def equalize_tc(csi, bsVec, ueVec, csi_skip, mod_order, cb_size, zeros, cb_blocks=1,
+                    hard=None, scrambler=None, x=None, stream=None):
+        """Mixed-precision variant on the tensor cores (BF16 W and y, FP32
+        accumulation); scratch is allocated here by torch, outside the library."""
+        M, K = csi.shape[-2], csi.shape[-1]
+        S = bsVec.shape[-1]
+        n_sym = bsVec.numel() // (M * S)
+        img, ylp = _lib.U64(), _lib.U64()
+        check(LIB.mb_equalize_tc_scratch(K, M, S, csi_skip, n_sym, ctypes.byref(img), ctypes.byref(ylp)),
+              "mb_equalize_tc_scratch")
+        s_img = torch.empty(img.value, dtype=torch.uint8, device=csi.device)
+        s_ylp = torch.empty(ylp.value, dtype=torch.uint8, device=csi.device)
+        cb_stride = ueVec.shape[-1]
+        if ueVec.numel() != n_sym * K * cb_blocks * cb_stride:
+            raise ValueError("ueVec must be [n_sym, K*cb_blocks, cb_stride]")
+        hp = _dev(hard, "hard", torch.uint8) if hard is not None else None
+        sp = scrambler._h if scrambler is not None else None
+        xp = _dev(x, "x", torch.complex64) if x is not None else None
+        check(LIB.mb_equalize_tc(_dev(csi, "csi"), _dev(bsVec, "bsVec"), K, M, S, csi_skip, n_sym, mod_order,
+                                 cb_size, cb_stride, zeros, cb_blocks, _dev(ueVec, "ueVec"), hp, sp, xp,
+                                 _dev(s_img, "img"), _dev(s_ylp, "ylp"), _stream(stream)), "Equalize.equalize_tc")
+
+
+def device_error(clear=True):
+    """Error bits of bounded device waits that gave up (0 = none)."""
+    v = ctypes.c_int()
+    check(LIB.mb_device_error(ctypes.byref(v), int(clear)), "mb_device_error")
+    return v.value
+
+
 class Precode:
     """sgemv/precode.h:24-62: precode + FFT-shift scatter into N-point rows."""
 

@@ -55,6 +55,17 @@ class UplinkSlot:
               "mb_slot_downlink")
         return out
 
+    def timing(self, max_calls):
+        """Record per-stage CUDA events for the next max_calls slots."""
+        check(LIB.mb_slot_timing(self._h, max_calls), "mb_slot_timing")
+
+    def stage_ms(self):
+        """Summed stage times of the recorded calls: dict of ms and counts."""
+        out = (ctypes.c_double * 8)()
+        check(LIB.mb_slot_stage_ms(self._h, out), "mb_slot_stage_ms")
+        keys = ["pilot_fft", "zf", "uplink_fft", "equalize", "slot", "n_fft", "n_eq", "calls"]
+        return dict(zip(keys, list(out)))
+
     def buffers(self):
         """(W [G, M, K], precoder [G, K, M]) as torch views of the slot's buffers."""
         c, p = ctypes.c_void_p(), ctypes.c_void_p()
