@@ -26,7 +26,7 @@
 #include <atomic>
 
 #include "common.cuh"
-#include "demod.cuh"
+#include "eq_common.cuh"
 #include "eq_tc.cuh"
 #include "sgemv.cuh"
 #include "tc.cuh"
@@ -34,18 +34,16 @@
 namespace mb {
 
 namespace {
-constexpr int kStages = 3;
+constexpr int kStages = 4;
 constexpr int kKT = 64;  // reduction elements per k tile (4 MMAs of K=16)
 
-__device__ __forceinline__ void cp16(void *dst_smem, const void *src) {
-  uint4 v = __ldg(reinterpret_cast<const uint4 *>(src));
-  *reinterpret_cast<uint4 *>(dst_smem) = v;
-}
 }  // namespace
 
 template <int MM>
-__global__ void __launch_bounds__(128, 1) equalize_tc_kernel(const EqTcParams q) {
+__global__ void __launch_bounds__(128, 1)
+    equalize_tc_kernel(const EqTcParams q, const __grid_constant__ CUtensorMap ymap) {
   extern __shared__ __align__(1024) uint8_t eq_smem[];
+  __shared__ __align__(8) uint64_t full_bar[kStages];
   __shared__ __align__(8) uint64_t empty_bar[kStages];
   __shared__ __align__(8) uint64_t done_bar;
   __shared__ uint32_t tmem_base_slot;
@@ -54,16 +52,24 @@ __global__ void __launch_bounds__(128, 1) equalize_tc_kernel(const EqTcParams q)
   const EqParams &p = q.p;
   const uint32_t g = blockIdx.x;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const uint32_t N = q.N;
-  const uint32_t a_tile = MM * kKT * 2;   // bytes
-  const uint32_t b_tile = kKT * N * 2;    // bytes
-  uint8_t *stage_base = eq_smem;
+  // this CTA's symbols: l_off .. l_off + nbc - 1 of the launch
+  const uint32_t l_off = blockIdx.y * q.spc;
+  const uint32_t nbc = min(q.spc, q.nb - l_off);
+  const uint32_t N = nbc * p.sg;
+  const uint32_t a_tile = MM * kKT * 2;           // bytes
+  const uint32_t b_tile = kKT * q.spc * p.sg * 2; // stage room: N_max/8 boxes of 8 x 64 BF16
+  const uint32_t b_bytes = kKT * N * 2;           // bytes this CTA loads per tile
+  const uint32_t s_base = g * p.sg;
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; s++) tc::mbar_init(&empty_bar[s], 1);
+    for (int s = 0; s < kStages; s++) {
+      tc::mbar_init(&full_bar[s], 1);
+      tc::mbar_init(&empty_bar[s], 1);
+    }
     tc::mbar_init(&done_bar, 1);
     tc::fence_mbar_init();
     timed_out = 0;
+    tc::prefetch_tmap(&ymap);
   }
   if (warp == 0) tc::tmem_alloc(&tmem_base_slot, q.tmem_cols);
   tc::fence_before_sync();
@@ -71,138 +77,111 @@ __global__ void __launch_bounds__(128, 1) equalize_tc_kernel(const EqTcParams q)
   tc::fence_after_sync();
   const uint32_t tmem = tmem_base_slot;
 
-  const uint8_t *a_g = q.a_img + (uint64_t)g * q.nkt * a_tile;
-  const uint32_t s_base = g * p.sg;
-  const uint32_t idesc = tc::idesc_bf16(MM, N, false, true);
-  const uint32_t nchunk_b = (N / 8) * (kKT / 8) * 8;  // 16-byte chunks in a B tile
-  bool ok = true;
-
-  for (uint32_t kt = 0; kt < q.nkt; kt++) {
-    const uint32_t st = kt % kStages;
-    uint8_t *sa = stage_base + st * (a_tile + b_tile);
-    uint8_t *sb = sa + a_tile;
-    if (kt >= kStages) {
-      if (!tc::mbar_wait(&empty_bar[st], ((kt / kStages) - 1) & 1)) ok = false;
-    }
-    if (__syncthreads_or(!ok)) break;
-    // A tile: contiguous image
-    const uint8_t *a_src = a_g + (uint64_t)kt * a_tile;
-    for (uint32_t c = tid; c < a_tile / 16; c += blockDim.x) cp16(sa + c * 16, a_src + c * 16);
-    // B tile: chunk (j, kg, i) -> smem j*1024-style canonical position
-    for (uint32_t c = tid; c < nchunk_b; c += blockDim.x) {
-      const uint32_t i = c % 8, kg = (c / 8) % (kKT / 8), j = c / kKT;
-      const uint32_t kk = kt * kKT + kg * 8 + i;
-      const uint32_t plane = kk / q.Mp, b = kk % q.Mp;
-      const uint32_t col0 = j * 8, l = col0 / p.sg, sl = col0 % p.sg;
-      uint8_t *dst = sb + j * (kKT / 8) * 128 + kg * 128 + i * 16;
-      if (b < p.M) {
-        const __nv_bfloat16 *src =
-            q.y_lp + ((uint64_t)(l * 2 + plane) * p.M + b) * q.S_pad + s_base + sl;
-        cp16(dst, src);
-      } else {
-        *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
+  if (warp == 0 && lane == 0) {
+    // ---- producer: detector image tile by bulk copy, y_lp by tensor boxes
+    const uint8_t *a_g = q.a_img + (uint64_t)g * q.nkt * a_tile;
+    for (uint32_t kt = 0; kt < q.nkt; kt++) {
+      const uint32_t s = kt % kStages, use = kt / kStages;
+      if (use >= 1 && !tc::mbar_wait(&empty_bar[s], (use - 1) & 1)) {
+        timed_out = 1;
+        break;
+      }
+      uint8_t *sa = eq_smem + s * (a_tile + b_tile);
+      uint8_t *sb = sa + a_tile;
+      tc::mbar_arrive_expect_tx(&full_bar[s], a_tile + b_bytes);
+      tc::bulk_g2s(sa, a_g + (uint64_t)kt * a_tile, a_tile, &full_bar[s]);
+      const uint32_t kk0 = kt * kKT, plane = kk0 / q.Mp, b0 = kk0 % q.Mp;
+      for (uint32_t j = 0; j < N / 8; j++) {
+        const uint32_t col0 = j * 8, l = col0 / p.sg, sl = col0 % p.sg;
+        const int32_t row = (int32_t)(((l_off + l) * 2 + plane) * p.M + b0);
+        tc::tma_load_2d(sb + j * 1024, &ymap, (int32_t)(s_base + sl), row, &full_bar[s]);
       }
     }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    const uint32_t idesc = tc::idesc_bf16(MM, N, false, true);
+    bool ok = true;
+    for (uint32_t kt = 0; kt < q.nkt; kt++) {
+      const uint32_t s = kt % kStages, use = kt / kStages;
+      if (!tc::mbar_wait(&full_bar[s], use & 1)) {
+        ok = false;
+        break;
+      }
       tc::fence_after_sync();
-      const uint32_t a0 = tc::smem_u32(sa), b0 = tc::smem_u32(sb);
+      const uint32_t a0 = tc::smem_u32(eq_smem + s * (a_tile + b_tile)), b0 = a0 + a_tile;
 #pragma unroll
       for (int ks = 0; ks < kKT / 16; ks++) {
         // A: K-major, K core matrices 128 B apart, 8-row groups 1024 B apart
         const uint64_t ad = tc::smem_desc(a0 + ks * 256, 128, 1024);
-        // B: MN-major, K groups 128 B apart, MN chunks (kKT/8)*128 B apart
-        const uint64_t bd = tc::smem_desc(b0 + ks * 256, 128, (kKT / 8) * 128);
+        // B: MN-major, 8-antenna K groups 128 B apart, 8-subcarrier MN
+        // chunks 1024 B apart (one tensor box each)
+        const uint64_t bd = tc::smem_desc(b0 + ks * 256, 128, 1024);
         tc::mma_f16(tmem, ad, bd, idesc, (kt | ks) != 0);
       }
-      tc::mma_commit(&empty_bar[st]);
+      tc::mma_commit(&empty_bar[s]);
     }
+    if (ok) tc::mma_commit(&done_bar);
+    else timed_out = 1;
   }
-  if (tid == 0 && ok) tc::mma_commit(&done_bar);
-  if (ok && !tc::mbar_wait(&done_bar, 0)) ok = false;
-  if (!ok) timed_out = 1;
-  __syncthreads();
-  tc::fence_after_sync();
-
-  if (!timed_out) {
-    // epilogue: warp w reads TMEM lanes 32w..32w+31
+  __syncwarp();
+  // everyone: wait for the accumulator (bounded)
+  bool ok = tc::mbar_wait(&done_bar, 0);
+  if (__syncthreads_or(!ok || timed_out)) {
+    if (tid == 0 && q.err) atomicOr(q.err, tc::kErrTimeout);
+  } else {
+    tc::fence_after_sync();
+    // epilogue: warp w reads TMEM lanes 32w..32w+31; rows (2u, 2u+1) are
+    // adjacent lanes, exchanged with one shuffle
     const int rows_per_warp = MM == 64 ? 16 : 32;
     const bool lane_ok = lane < rows_per_warp;
     const uint32_t r = warp * rows_per_warp + lane;  // D row of this lane
     const uint32_t u = r / 2;
     const bool is_im = r & 1;
     const bool valid = lane_ok && u < p.K;
-    const uint32_t nl = N / p.sg;
     for (uint32_t ch = 0; ch < (N + 15) / 16; ch++) {
       float v[16];
       tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + ch * 16, v);
-      float w[16];
+      float re8[8], im8[8];
 #pragma unroll
-      for (int i = 0; i < 16; i++) w[i] = __shfl_xor_sync(0xffffffffu, v[i], 1);
+      for (int i = 0; i < 8; i++) {
+        // even lane keeps columns 0-7, odd lane 8-15
+        const float send = is_im ? v[i] : v[8 + i];
+        const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+        re8[i] = is_im ? recv : v[i];
+        im8[i] = is_im ? v[8 + i] : recv;
+      }
       if (!valid) continue;
-      const int half = is_im ? 1 : 0;  // even lane: columns 0-7, odd: 8-15
-      const uint32_t c0 = ch * 16 + half * 8;
+      const uint32_t c0 = ch * 16 + (is_im ? 8 : 0);
       if (c0 >= N) continue;  // N % 16 == 8: the last chunk is half full
       const uint32_t l = c0 / p.sg, sl0 = c0 % p.sg;
-      (void)nl;
       const uint32_t s0 = s_base + sl0;
+      const uint32_t lg = q.l0 + l_off + l;
+      __half *llr_row = reinterpret_cast<__half *>(p.llr) + ((uint64_t)lg * p.K + u) * p.row_len;
       uint64_t hbits = 0;
       int nbits = 0;
 #pragma unroll
       for (int e = 0; e < 8; e++) {
-        const float re = is_im ? w[half * 8 + e] : v[half * 8 + e];
-        const float im = is_im ? v[half * 8 + e] : w[half * 8 + e];
         const uint32_t s = s0 + e;
         if (s >= p.S) break;
-        const float2 x = make_float2(re, im);
-        __half lv[8];
-        if (p.x) p.x[((uint64_t)(q.l0 + l) * p.K + u) * p.S + s] = x;
-        demod(p.Qm, x, lv);
-        const uint64_t t0 = (uint64_t)s * p.Qm;
-        const uint64_t cb = t0 / p.cb_size;
-        if (cb < p.cb_blocks) {
-          const uint64_t base = cb * p.cb_stride + p.zeros + t0 % p.cb_size;
-          __half *row = reinterpret_cast<__half *>(p.llr) + ((uint64_t)(q.l0 + l) * p.K + u) * p.row_len;
-#pragma unroll
-          for (int qq = 0; qq < 8; qq++)
-            if (qq < (int)p.Qm && base + qq < p.row_len) row[base + qq] = lv[qq];
-        }
-        if (p.hard) {
-          const __half zero = __float2half_rn(0.f);
-#pragma unroll
-          for (int qq = 0; qq < 8; qq++) {
-            if (qq >= (int)p.Qm) break;
-            const uint64_t t = t0 + qq;
-            uint32_t h = 0;
-            if (t < p.n_valid) {
-              h = __hlt(lv[qq], zero) ? 1u : 0u;
-              if (p.seq) {
-                const uint64_t si = t % p.seq_len;
-                h ^= (p.seq[(uint64_t)u * p.seq_stride_words + si / 32] >> (si % 32)) & 1u;
-              }
-            }
-            hbits = (hbits << 1) | h;  // first stream bit ends up most significant
-            nbits++;
-          }
-        }
+        const float2 x = make_float2(re8[e], im8[e]);
+        if (p.x) p.x[((uint64_t)lg * p.K + u) * p.S + s] = x;
+        hbits = (hbits << p.Qm) | eq_demap_store(p, llr_row, s, x);
+        nbits += p.Qm;
       }
       if (p.hard && nbits) {
-        // nbits = 8*Qm unless the group is cut short by S; bytes are whole
-        // because sl0 % 8 == 0
-        const uint64_t byte0 = (uint64_t)s0 * p.Qm / 8;
-        uint8_t *hrow = p.hard + ((uint64_t)(q.l0 + l) * p.K + u) * p.hrow;
+        // 8 subcarriers from s0 % 8 == 0 give whole bytes; a group cut short
+        // by S pads the last byte with zeros
+        const uint32_t byte0 = s0 * p.Qm / 8;
+        uint8_t *hrow = p.hard + ((uint64_t)lg * p.K + u) * p.hrow;
         const int nbytes = (nbits + 7) / 8;
         if (nbits % 8) hbits <<= (8 - nbits % 8);
         for (int bI = 0; bI < nbytes; bI++) {
-          const uint64_t gb = byte0 + bI;
-          if (gb * 8 >= p.n_valid) break;
-          hrow[gb] = (uint8_t)(hbits >> (8 * (nbytes - 1 - bI)));
+          const uint32_t gb = byte0 + bI;
+          if (gb * 8 >= p.n_valid32) break;
+          hrow[gb] = (uint8_t)(hbits >> (8 * (nbytes - 1 - bI))) ^ eq_seq_byte(p, u, gb);
         }
       }
     }
-  } else if (tid == 0 && q.err) {
-    atomicOr(q.err, tc::kErrTimeout);
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -255,7 +234,8 @@ bool equalize_tc_supported(uint32_t K, uint32_t sg, uint32_t nb) {
   if (K == 0 || K > 64 || sg % 8 != 0) return false;
   const uint32_t MM = 2 * K <= 64 ? 64 : 128;
   if (N == 0 || N > 256 || N % 8 != 0) return false;  // MMA N rule for M = 64
-  if (MM == 128 && N % 16 != 0) return false;          // and for M = 128
+  // M = 128 needs N % 16: keep every per-CTA symbol chunk legal
+  if (MM == 128 && sg % 16 != 0) return false;
   return true;
 }
 
@@ -271,7 +251,12 @@ mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, ui
   q.S_pad = S_pad;
   q.Mp = s.Mp;
   q.nkt = s.nkt;
-  q.N = nb * p.sg;
+  // symbols per CTA: about 32 columns, so a launch has several CTAs per
+  // group and each CTA's epilogue stays short
+  q.spc = std::max<uint32_t>(1, std::min<uint32_t>(nb, 32 / p.sg));
+  while (q.spc > 1 && (q.spc * p.sg) % (s.MM == 64 ? 8 : 16)) q.spc--;
+  q.nb = nb;
+  q.N = q.spc * p.sg;
   q.l0 = l0;
   q.err = err;
   q.tmem_cols = 32;
@@ -300,10 +285,16 @@ mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, ui
     }
     configured[which].fetch_or(bit);
   }
+  // tensor map over y_lp rows [nb * 2 * M][S_pad], box 8 subcarriers x 64
+  // antennas (one 1 KB group of MN-major core matrices)
+  CUtensorMap ymap;
+  mb_status tr = make_tmap_2d_bf16(&ymap, y_lp, S_pad, (uint64_t)nb * 2 * p.M, S_pad, 8, kKT);
+  if (tr != MB_OK) return tr;
+  const dim3 grid(G, (nb + q.spc - 1) / q.spc);
   if (s.MM == 64)
-    equalize_tc_kernel<64><<<G, 128, smem, st>>>(q);
+    equalize_tc_kernel<64><<<grid, 128, smem, st>>>(q, ymap);
   else
-    equalize_tc_kernel<128><<<G, 128, smem, st>>>(q);
+    equalize_tc_kernel<128><<<grid, 128, smem, st>>>(q, ymap);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }

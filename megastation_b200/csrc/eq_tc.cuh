@@ -11,6 +11,7 @@ struct EqTcParams {
   const uint8_t *a_img;       // per-group detector images (BF16)
   const __nv_bfloat16 *y_lp;  // [nb][re|im][M][S_pad]
   uint32_t S_pad, Mp, nkt, N, l0, tmem_cols;
+  uint32_t spc, nb;           // symbols per CTA, symbols in the launch
   int *err;
 };
 

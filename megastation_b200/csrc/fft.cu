@@ -146,6 +146,9 @@ struct Plan {
   static constexpr int T = N / 16;                 // threads per row
   static constexpr int ROWS = T >= 256 ? 1 : 256 / T;
   static constexpr int THREADS = T * ROWS;
+  // resident CTAs per SM the register budget must allow (64 regs/thread at
+  // 256 threads x 4): keeps 32 warps per SM in flight for the HBM stream
+  static constexpr int MIN_BLOCKS = THREADS >= 512 ? 2 : 4;
   static constexpr int P16 = LOGN / 4;             // radix-16 passes
   static constexpr int RLAST = 1 << (LOGN % 4);    // trailing radix (1: none)
   static constexpr int PASSES = P16 + (RLAST > 1 ? 1 : 0);
@@ -185,35 +188,59 @@ __device__ __forceinline__ float2 load_iq(const FftParams &p, uint64_t e) {
   }
 }
 
+// Per-row output context, computed once per thread so that the per-element
+// epilogue needs no 64-bit division.
+struct RowCtx {
+  void *o0;       // row base of the output (LP: real plane)
+  void *o1;       // LP: imaginary plane row
+  uint32_t u0;    // pilot: first user of this symbol's comb
+  uint32_t b;     // pilot: antenna
+};
+
 template <int MODE, int N>
-__device__ __forceinline__ void epilogue(const FftParams &p, uint64_t row,
-                                         uint32_t k, float2 v) {
+__device__ __forceinline__ RowCtx row_ctx(const FftParams &p, uint64_t row) {
+  RowCtx c{};
+  const uint32_t sym = (uint32_t)(row / p.M), b = (uint32_t)(row - (uint64_t)sym * p.M);
   if constexpr (MODE == kUplink) {
-    uint32_t i = (k - p.start - N / 2) & (N - 1);
-    if (i < p.S) reinterpret_cast<float2 *>(p.out)[row * p.S + i] = v;
+    c.o0 = reinterpret_cast<float2 *>(p.out) + row * p.S;
+  } else if constexpr (MODE == kUplinkLP) {
+    __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(p.out);
+    c.o0 = o + ((uint64_t)(sym * 2 + 0) * p.M + b) * p.S_pad;
+    c.o1 = o + ((uint64_t)(sym * 2 + 1) * p.M + b) * p.S_pad;
+  } else if constexpr (MODE == kPilot) {
+    c.u0 = p.ue_start + sym * p.sg;
+    c.b = b;
+  } else {
+    c.o0 = reinterpret_cast<char *>(p.out) + row * N * (p.out_dtype == MB_IQ_C32 ? 8 : p.out_dtype == MB_IQ_I8 ? 2 : 4);
+  }
+  return c;
+}
+
+template <int MODE, int N>
+__device__ __forceinline__ void epilogue(const FftParams &p, const RowCtx &c, uint32_t k,
+                                         float2 v) {
+  if constexpr (MODE == kUplink) {
+    const uint32_t i = (k - p.start - N / 2) & (N - 1);
+    if (i < p.S) reinterpret_cast<float2 *>(c.o0)[i] = v;
   } else if constexpr (MODE == kUplinkLP) {
     // planar BF16 rows for the tensor-core equalizer: [sym][re|im][M][S_pad]
-    uint32_t i = (k - p.start - N / 2) & (N - 1);
+    const uint32_t i = (k - p.start - N / 2) & (N - 1);
     if (i < p.S) {
-      const uint64_t sym = row / p.M, b = row % p.M;
-      __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(p.out);
-      o[((sym * 2 + 0) * p.M + b) * p.S_pad + i] = __float2bfloat16_rn(v.x);
-      o[((sym * 2 + 1) * p.M + b) * p.S_pad + i] = __float2bfloat16_rn(v.y);
+      reinterpret_cast<__nv_bfloat16 *>(c.o0)[i] = __float2bfloat16_rn(v.x);
+      reinterpret_cast<__nv_bfloat16 *>(c.o1)[i] = __float2bfloat16_rn(v.y);
     }
   } else if constexpr (MODE == kPilot) {
-    uint32_t i = (k - p.start - N / 2) & (N - 1);
+    const uint32_t i = (k - p.start - N / 2) & (N - 1);
     if (i < p.S) {
-      uint32_t sym = (uint32_t)(row / p.M), b = (uint32_t)(row % p.M);
-      uint32_t u = p.ue_start + sym * p.sg + i % p.sg;
+      const uint32_t g = i / p.sg;
+      const uint32_t u = c.u0 + (i - g * p.sg);
       if (u < p.K) {
-        float2 ps = __ldg(p.pilot + i);
-        float2 e = make_float2(v.x * ps.x + v.y * ps.y, v.x * ps.y - v.y * ps.x);
-        uint64_t o = (uint64_t)(i / p.sg) * p.M * p.K + (uint64_t)b * p.K + u;
-        reinterpret_cast<float2 *>(p.out)[o] = e;
+        const float2 ps = __ldg(p.pilot + i);
+        const float2 e = make_float2(v.x * ps.x + v.y * ps.y, v.x * ps.y - v.y * ps.x);
+        reinterpret_cast<float2 *>(p.out)[((uint64_t)g * p.M + c.b) * p.K + u] = e;
       }
     }
   } else {
-    uint64_t o = row * N + k;
     if (p.out_dtype == MB_IQ_I16 || p.out_dtype == MB_IQ_I8) {
       const bool i16 = p.out_dtype == MB_IQ_I16;
       const float qmax = i16 ? 32767.f : 127.f, qmin = i16 ? -32768.f : -128.f;
@@ -223,22 +250,21 @@ __device__ __forceinline__ void epilogue(const FftParams &p, uint64_t row,
       if (re > qmax) qr = (int)qmax; else if (re < qmin) qr = (int)qmin;
       if (im > qmax) qi = (int)qmax; else if (im < qmin) qi = (int)qmin;
       if (i16)
-        reinterpret_cast<short2 *>(p.out)[o] = make_short2((short)qr, (short)qi);
+        reinterpret_cast<short2 *>(c.o0)[k] = make_short2((short)qr, (short)qi);
       else
-        reinterpret_cast<char2 *>(p.out)[o] = make_char2((char)qr, (char)qi);
+        reinterpret_cast<char2 *>(c.o0)[k] = make_char2((char)qr, (char)qi);
     } else if (p.out_dtype == MB_IQ_F16) {
       const float sc = 1.f / (float)N;
-      reinterpret_cast<__half2 *>(p.out)[o] =
-          __floats2half2_rn(v.x * sc, v.y * sc);
+      reinterpret_cast<__half2 *>(c.o0)[k] = __floats2half2_rn(v.x * sc, v.y * sc);
     } else {
       const float sc = 1.f / (float)N;
-      reinterpret_cast<float2 *>(p.out)[o] = make_float2(v.x * sc, v.y * sc);
+      reinterpret_cast<float2 *>(c.o0)[k] = make_float2(v.x * sc, v.y * sc);
     }
   }
 }
 
 template <int LOGN, int MODE>
-__global__ void __launch_bounds__(Plan<LOGN>::THREADS)
+__global__ void __launch_bounds__(Plan<LOGN>::THREADS, Plan<LOGN>::MIN_BLOCKS)
     fft_kernel(const FftParams p) {
   using PL = Plan<LOGN>;
   constexpr int N = PL::N, T = PL::T;
@@ -313,11 +339,12 @@ __global__ void __launch_bounds__(Plan<LOGN>::THREADS)
       }
       __syncthreads();
     } else if (active) {
+      const RowCtx ctx = row_ctx<MODE, N>(p, row);
 #pragma unroll
       for (int bi = 0; bi < 16; bi++) {
         const int j = t + (bi / R) * T, r = bi % R;
         // last pass: Ns = N / R, so idxD = j
-        epilogue<MODE, N>(p, row, (uint32_t)(j + r * Ns), v[bi]);
+        epilogue<MODE, N>(p, ctx, (uint32_t)(j + r * Ns), v[bi]);
       }
     }
     Ns *= R;

@@ -14,52 +14,28 @@
 #include <algorithm>
 
 #include "common.cuh"
-#include "demod.cuh"
+#include "eq_common.cuh"
 #include "sgemv.cuh"
 
 namespace mb {
 
-__device__ __forceinline__ uint32_t seq_bit(const EqParams &p, uint32_t u,
-                                            uint64_t t) {
-  if (!p.seq) return 0;
-  uint64_t i = t % p.seq_len;
-  return (p.seq[(uint64_t)u * p.seq_stride_words + i / 32] >> (i % 32)) & 1u;
-}
-
-// Epilogue shared by the FP32 and tensor-core equalizers: demap x of
-// (symbol l, user u, subcarrier s) and store LLRs; hard bits are ORed into
-// the CTA's word buffer hw (per (l_local, u) row of hw_words words, bit
-// offset relative to the group's first stream bit).
+// SIMT epilogue: demap, store LLRs, OR the Qm hard bits into the CTA's
+// word buffer hw (per (l_local, u) row of hw_words words, bit offsets
+// relative to the group's first stream bit, MSB-first bytes).
 __device__ __forceinline__ void equalize_store(const EqParams &p, uint32_t l,
                                                uint32_t l_local, uint32_t u,
                                                uint32_t s, uint32_t s_local,
                                                float2 x, uint32_t *hw) {
-  __half lv[8];
   if (p.x) p.x[((uint64_t)l * p.K + u) * p.S + s] = x;
-  demod(p.Qm, x, lv);
-  const uint64_t t0 = (uint64_t)s * p.Qm;
-  const uint64_t cb = t0 / p.cb_size;
-  if (cb < p.cb_blocks) {
-    const uint64_t base = cb * p.cb_stride + p.zeros + t0 % p.cb_size;
-    __half *row = reinterpret_cast<__half *>(p.llr) + ((uint64_t)l * p.K + u) * p.row_len;
-#pragma unroll
-    for (int q = 0; q < 8; q++)
-      if (q < (int)p.Qm && base + q < p.row_len) row[base + q] = lv[q];
-  }
-  if (hw) {
-    const __half zero = __float2half_rn(0.f);
+  __half *row = reinterpret_cast<__half *>(p.llr) + ((uint64_t)l * p.K + u) * p.row_len;
+  const uint32_t hb = eq_demap_store(p, row, s, x);
+  if (hw && hb) {
     uint32_t *w = hw + ((uint64_t)l_local * p.K + u) * p.hw_words;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      if (q >= (int)p.Qm) break;
-      const uint64_t t = t0 + q;
-      if (t >= p.n_valid) break;
-      uint32_t h = (__hlt(lv[q], zero) ? 1u : 0u) ^ seq_bit(p, u, t);
-      if (h) {
-        const uint32_t rel = s_local * p.Qm + q;  // bit within the group
-        const uint32_t byte = rel >> 3, bit = 7 - (rel & 7);
-        atomicOr(w + byte / 4, 1u << (8 * (byte % 4) + bit));
-      }
+    for (uint32_t q = 0; q < p.Qm; q++) {
+      if (!((hb >> (p.Qm - 1 - q)) & 1u)) continue;
+      const uint32_t rel = s_local * p.Qm + q;  // bit within the group
+      const uint32_t byte = rel >> 3, bit = 7 - (rel & 7);
+      atomicOr(w + byte / 4, 1u << (8 * (byte % 4) + bit));
     }
   }
 }
@@ -80,7 +56,7 @@ __device__ __forceinline__ void equalize_flush_hard(const EqParams &p,
     uint32_t word = hw[(uint64_t)lu * p.hw_words + rb / 4];
     uint8_t v = (uint8_t)(word >> (8 * (rb % 4)));
     uint32_t l = l0 + lu / p.K, u = lu % p.K;
-    p.hard[((uint64_t)l * p.K + u) * p.hrow + gb] = v;
+    p.hard[((uint64_t)l * p.K + u) * p.hrow + gb] = v ^ eq_seq_byte(p, u, (uint32_t)gb);
   }
 }
 
@@ -301,18 +277,22 @@ mb_status precode_fp32(const float2 *P, const float2 *s, float2 *out,
 
 using namespace mb;
 
+// The descrambling sequence is stored expanded into MSB-first bytes (bit t
+// of the stream is bit 7 - t % 8 of byte t / 8, the byte order of
+// scrambler_kernel.cuh:43-50), so descrambling packed hard bits is one XOR
+// per byte.
 struct mb_scrambler {
-  uint32_t *bits;        // device, packed LSB-first
-  uint64_t seq_len;      // period / length in bits
-  uint64_t stride_words; // 0: shared by all users
+  uint8_t *bytes;       // device
+  uint64_t nbits;       // bits available per user
+  uint64_t row_bytes;   // byte stride between users (0: shared by all users)
   uint32_t num_ue;
 };
 
-const uint32_t *mb::scrambler_bits(const mb_scrambler *s, uint64_t *seq_len,
-                                   uint64_t *stride_words) {
-  *seq_len = s->seq_len;
-  *stride_words = s->stride_words;
-  return s->bits;
+const uint8_t *mb::scrambler_bytes(const mb_scrambler *s, uint64_t *nbits,
+                                   uint64_t *row_bytes) {
+  *nbits = s->nbits;
+  *row_bytes = s->row_bytes;
+  return s->bytes;
 }
 
 extern "C" mb_status mb_scrambler_create(int mode, uint32_t c_init,
@@ -320,57 +300,56 @@ extern "C" mb_status mb_scrambler_create(int mode, uint32_t c_init,
                                          mb_scrambler **out) {
   if (!out) return MB_BAD_ARG;
   *out = nullptr;
-  const DeviceTables *tab = device_tables();
-  if (!tab) return MB_CUDA_ERROR;
-  mb_scrambler *s = new mb_scrambler();
-  s->num_ue = num_ue;
+  if (!device_tables()) return MB_CUDA_ERROR;
+  std::vector<uint8_t> h;
+  uint64_t nbits = 0, row_bytes = 0;
   if (mode == MB_SCR_LFSR127) {
-    s->seq_len = 127;
-    s->stride_words = 0;
-    cudaError_t e = cudaMalloc(&s->bits, 4 * sizeof(uint32_t));
-    if (e == cudaSuccess)
-      e = cudaMemcpy(s->bits, tab->lfsr127_bits, 4 * sizeof(uint32_t),
-                     cudaMemcpyDeviceToDevice);
-    if (e != cudaSuccess) {
-      delete s;
-      return record_error(e);
+    // scrambler/scrambler.cu:22-31: period 127, the same for every user;
+    // expanded over the largest stream a symbol can carry (8192 x 8 bits)
+    nbits = std::max<uint64_t>(num_bits, 65536);
+    uint8_t seq[127];
+    uint8_t st = 0x5D;
+    for (int i = 0; i < 127; i++) {
+      const uint8_t fb = (st ^ (st >> 3)) & 1;
+      seq[i] = fb;
+      st = (uint8_t)((st >> 1) | (fb << 6));
     }
+    h.assign((nbits + 7) / 8, 0);
+    for (uint64_t t = 0; t < nbits; t++)
+      if (seq[t % 127]) h[t / 8] |= (uint8_t)(0x80u >> (t % 8));
   } else if (mode == MB_SCR_GOLD) {
-    if (num_ue == 0 || num_bits == 0) {
-      delete s;
-      return MB_BAD_SHAPE;
-    }
-    s->seq_len = num_bits;
-    s->stride_words = (num_bits + 31) / 32;
-    std::vector<uint32_t> h(s->stride_words * num_ue, 0);
+    if (num_ue == 0 || num_bits == 0) return MB_BAD_SHAPE;
     // TS 38.211 5.2.1, c_init(u) = c_init + u
+    nbits = num_bits;
+    row_bytes = (num_bits + 7) / 8;
+    h.assign(row_bytes * num_ue, 0);
     const uint64_t Nc = 1600;
     for (uint32_t u = 0; u < num_ue; u++) {
-      uint32_t ci = c_init + u;
-      uint32_t x1 = 1, x2 = ci & 0x7fffffffu;  // 31-bit shift registers
+      uint32_t x1 = 1, x2 = (c_init + u) & 0x7fffffffu;  // 31-bit registers
       for (uint64_t n = 0; n < Nc + num_bits; n++) {
-        if (n >= Nc) {
-          uint64_t t = n - Nc;
-          uint32_t c = (x1 ^ x2) & 1u;
-          h[u * s->stride_words + t / 32] |= c << (t % 32);
+        if (n >= Nc && ((x1 ^ x2) & 1u)) {
+          const uint64_t t = n - Nc;
+          h[u * row_bytes + t / 8] |= (uint8_t)(0x80u >> (t % 8));
         }
-        uint32_t f1 = ((x1 >> 3) ^ x1) & 1u;
-        uint32_t f2 = ((x2 >> 3) ^ (x2 >> 2) ^ (x2 >> 1) ^ x2) & 1u;
+        const uint32_t f1 = ((x1 >> 3) ^ x1) & 1u;
+        const uint32_t f2 = ((x2 >> 3) ^ (x2 >> 2) ^ (x2 >> 1) ^ x2) & 1u;
         x1 = (x1 >> 1) | (f1 << 30);
         x2 = (x2 >> 1) | (f2 << 30);
       }
     }
-    cudaError_t e = cudaMalloc(&s->bits, h.size() * sizeof(uint32_t));
-    if (e == cudaSuccess)
-      e = cudaMemcpy(s->bits, h.data(), h.size() * sizeof(uint32_t),
-                     cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-      delete s;
-      return record_error(e);
-    }
   } else {
-    delete s;
     return MB_BAD_ARG;
+  }
+  mb_scrambler *s = new mb_scrambler();
+  s->nbits = nbits;
+  s->row_bytes = row_bytes;
+  s->num_ue = num_ue;
+  cudaError_t e = cudaMalloc(&s->bytes, h.size());
+  if (e == cudaSuccess) e = cudaMemcpy(s->bytes, h.data(), h.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(s->bytes);
+    delete s;
+    return record_error(e);
   }
   *out = s;
   return MB_OK;
@@ -378,7 +357,7 @@ extern "C" mb_status mb_scrambler_create(int mode, uint32_t c_init,
 
 extern "C" mb_status mb_scrambler_destroy(mb_scrambler *s) {
   if (!s) return MB_BAD_ARG;
-  cudaFree(s->bits);
+  cudaFree(s->bytes);
   delete s;
   return MB_OK;
 }
@@ -413,9 +392,17 @@ mb_status mb::equalize_prepare(EqParams &p, const mb_c32 *W, const mb_c32 *y,
   p.n_valid = std::min<uint64_t>((uint64_t)S * Qm, cb_size * cb_blocks);
   p.hrow = (p.n_valid + 7) / 8;
   p.hw_words = (sg * Qm / 8 + 3) / 4;
+  if (p.row_len >= (1ull << 31) || (uint64_t)S * Qm >= (1ull << 31)) return MB_BAD_SHAPE;
+  p.cb_size32 = (uint32_t)cb_size;
+  p.cb_stride32 = (uint32_t)cb_stride;
+  p.zeros32 = (uint32_t)zeros;
+  p.row_len32 = (uint32_t)p.row_len;
+  p.n_valid32 = (uint32_t)p.n_valid;
   if (scr && hard) {
-    p.seq = scrambler_bits(scr, &p.seq_len, &p.seq_stride_words);
-    if (p.seq_stride_words && scr->num_ue < K) return MB_BAD_SHAPE;
+    uint64_t nbits = 0;
+    p.seqb = scrambler_bytes(scr, &nbits, &p.seq_row_bytes);
+    if (p.seq_row_bytes && scr->num_ue < K) return MB_BAD_SHAPE;
+    if (nbits < p.n_valid) return MB_BAD_SHAPE;  // sequence shorter than the stream
   }
   return MB_OK;
 }

@@ -13,7 +13,8 @@
 
 #include "common.cuh"
 #include "sgemv.cuh"
-#include "slot.cuh"
+#include "eq_tc.cuh"
+#include "fft.cuh"
 #include "zf.cuh"
 
 using namespace mb;
@@ -26,18 +27,27 @@ struct mb_slot {
   mb_scrambler *scr;
   float2 *csi;        // [G][M][K]: CSI, then W in place
   float2 *precoder;   // [G][K][M]
-  float2 *y;          // [sym_batch][M][S] uplink FFT output
-  void *y_lp;         // low-precision copy of y for the mixed path
+  float2 *y;          // [sym_batch][M][S] uplink FFT output (FP32 path)
+  void *y_lp;         // [sym_batch][re|im][M][S_pad] BF16 (mixed path)
+  void *img_w;        // detector images for the tensor-core equalizer
+  void *img_c;        // mixed ZF scratch
+  uint32_t S_pad;
   float2 *precoded;   // [D][M][N]
   cudaStream_t side;
   cudaEvent_t ev_fork, ev_join;
-  // graph cache
-  cudaGraphExec_t graph;
-  const void *g_iq;
-  uint16_t *g_llr;
-  uint8_t *g_hard;
-  int32_t *g_status;
-  cudaStream_t g_stream;
+  // captured uplink slots, one per (input, outputs, stream) pointer set,
+  // least recently used evicted beyond kGraphCache entries
+  struct GraphEntry {
+    const void *iq;
+    uint16_t *llr;
+    uint8_t *hard;
+    int32_t *status;
+    cudaStream_t stream;
+    cudaGraphExec_t exec;
+    uint64_t last_use;
+  };
+  std::vector<GraphEntry> graphs;
+  uint64_t graph_clock = 0;
   // stage timing: per recorded call, events at stage boundaries
   struct Marks {
     cudaEvent_t start, pilot, zf, end;
@@ -46,6 +56,9 @@ struct mb_slot {
   std::vector<Marks> marks;
   uint32_t marks_used = 0, marks_max = 0;
 };
+
+static mb_status slot_equalize(mb_slot *s, uint32_t nb, uint16_t *llr, uint8_t *hard,
+                               cudaStream_t st);
 
 static cudaEvent_t new_event() {
   cudaEvent_t e = nullptr;
@@ -92,7 +105,7 @@ static size_t iq_elem_bytes(int dt) {
 
 extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   if (!s) return MB_BAD_ARG;
-  if (s->graph) cudaGraphExecDestroy(s->graph);
+  for (auto &e : s->graphs) cudaGraphExecDestroy(e.exec);
   free_marks(s);
   if (s->fft) mb_fft_destroy(s->fft);
   if (s->scr) mb_scrambler_destroy(s->scr);
@@ -100,6 +113,8 @@ extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   cudaFree(s->precoder);
   cudaFree(s->y);
   cudaFree(s->y_lp);
+  cudaFree(s->img_w);
+  cudaFree(s->img_c);
   cudaFree(s->precoded);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
@@ -137,10 +152,24 @@ extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
   const size_t gmk = (size_t)s->G * c.M * c.K;
   alloc((void **)&s->csi, sizeof(float2) * gmk);
   alloc((void **)&s->precoder, sizeof(float2) * gmk);
-  alloc((void **)&s->y, sizeof(float2) * (size_t)s->c.sym_batch * c.M * c.S);
   alloc((void **)&s->precoded, sizeof(float2) * (size_t)c.D * c.M * c.N);
-  if (st == MB_OK && c.zf_precision == MB_ZF_MIXED)
-    alloc(&s->y_lp, sizeof(uint32_t) * (size_t)s->c.sym_batch * c.M * c.S);
+  const bool mixed = c.zf_precision == MB_ZF_MIXED;
+  if (mixed && st == MB_OK && !equalize_tc_supported(c.K, c.sg, s->c.sym_batch))
+    st = MB_UNSUPPORTED;
+  s->S_pad = (c.S + 7) / 8 * 8;
+  const size_t ylp_bytes = (size_t)s->c.sym_batch * 2 * c.M * s->S_pad * 2;
+  if (mixed) {
+    alloc(&s->y_lp, ylp_bytes);
+    alloc(&s->img_w, zf_mixed_scratch_bytes(s->G, c.M, c.K));
+    alloc(&s->img_c, zf_mixed_scratch_bytes(s->G, c.M, c.K));
+    if (st == MB_OK) {
+      // the S_pad - S padding columns are never written by the FFT
+      cudaError_t e = cudaMemset(s->y_lp, 0, ylp_bytes);
+      if (e != cudaSuccess) st = record_error(e);
+    }
+  } else {
+    alloc((void **)&s->y, sizeof(float2) * (size_t)s->c.sym_batch * c.M * c.S);
+  }
   if (st == MB_OK) {
     cudaError_t e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
@@ -171,13 +200,20 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   const size_t sym_bytes = iq_elem_bytes(c.iq_dtype) * c.M * c.N;
   const char *iq_b = reinterpret_cast<const char *>(iq);
   mb_status r;
+  const bool mixed = c.zf_precision == MB_ZF_MIXED;
+  // uplink FFT of nb symbols from l0: FP32 rows for the SIMT equalizer, or
+  // planar BF16 rows for the tensor-core equalizer
+  auto fft_batch = [&](uint32_t l0, uint32_t nb, cudaStream_t fs) {
+    const void *src = iq_b + (size_t)(c.P + l0) * sym_bytes;
+    return mixed ? fft_uplink_lp(s->fft, src, c.iq_dtype, nb, s->y_lp, s->S_pad, fs)
+                 : mb_fft_uplink(s->fft, src, c.iq_dtype, nb, reinterpret_cast<mb_c32 *>(s->y), fs);
+  };
   // fork: the first uplink FFT batch only needs the samples
   const uint32_t nb0 = std::min(c.sym_batch, c.U);
   if (c.U) {
     MB_CUDA_TRY(cudaEventRecord(s->ev_fork, st));
     MB_CUDA_TRY(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
-    r = mb_fft_uplink(s->fft, iq_b + (size_t)c.P * sym_bytes, c.iq_dtype, nb0,
-                      reinterpret_cast<mb_c32 *>(s->y), s->side);
+    r = fft_batch(0, nb0, s->side);
     if (r != MB_OK) return r;
     MB_CUDA_TRY(cudaEventRecord(s->ev_join, s->side));
   }
@@ -188,9 +224,10 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   r = zf_fill_tail(s->csi, s->G, c.S, c.sg, c.M, c.K, st);
   if (r != MB_OK) return r;
   float2 *prec = c.D ? s->precoder : nullptr;
-  if (c.zf_precision == MB_ZF_MIXED) {
+  if (mixed) {
     mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, 0};
-    r = zf_mixed(s->csi, prec, s->G, c.M, c.K, &o, status, nullptr, st);
+    r = zf_mixed_run(s->csi, s->img_w, s->img_c, s->G, c.M, c.K, &o, status, nullptr, st);
+    if (r == MB_OK && prec) r = precoder_launch(s->csi, prec, c.M, c.K, s->G, st);
   } else {
     r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, st);
   }
@@ -208,14 +245,12 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     const uint32_t nb = std::min(c.sym_batch, c.U - l0);
     if (l0) {
       MARK(mk->fft_b[bi]);
-      r = mb_fft_uplink(s->fft, iq_b + (size_t)(c.P + l0) * sym_bytes, c.iq_dtype, nb,
-                        reinterpret_cast<mb_c32 *>(s->y), st);
+      r = fft_batch(l0, nb, st);
       if (r != MB_OK) return r;
       MARK(mk->fft_e[bi]);
     }
     MARK(mk->eq_b[bi]);
-    r = slot_equalize(s->c, s->csi, s->y, s->y_lp, nb, llr + l0 * llr_sym,
-                      hard ? hard + l0 * hard_sym : nullptr, s->scr, st);
+    r = slot_equalize(s, nb, llr + l0 * llr_sym, hard ? hard + l0 * hard_sym : nullptr, st);
     if (r != MB_OK) return r;
     MARK(mk->eq_e[bi]);
   }
@@ -224,15 +259,24 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   return MB_OK;
 }
 
-mb_status mb::slot_equalize(const mb_cell_desc &c, const float2 *W,
-                            const float2 *y, void *y_lp, uint32_t nb,
-                            uint16_t *llr, uint8_t *hard,
-                            const mb_scrambler *scr, cudaStream_t st) {
-  (void)y_lp;
-  return mb_equalize(reinterpret_cast<const mb_c32 *>(W),
-                     reinterpret_cast<const mb_c32 *>(y), c.K, c.M, c.S, c.sg,
-                     nb, c.Qm, c.cb_size, c.cb_stride, c.zeros, 1, llr, hard,
-                     scr, nullptr, st);
+// equalize one batch of nb symbols whose FFT output sits in the slot's
+// y (FP32) or y_lp (BF16) buffer; llr / hard point at the batch's rows
+static mb_status slot_equalize(mb_slot *s, uint32_t nb, uint16_t *llr, uint8_t *hard,
+                               cudaStream_t st) {
+  const mb_cell_desc &c = s->c;
+  if (c.zf_precision != MB_ZF_MIXED)
+    return mb_equalize(reinterpret_cast<const mb_c32 *>(s->csi),
+                       reinterpret_cast<const mb_c32 *>(s->y), c.K, c.M, c.S, c.sg, nb,
+                       c.Qm, c.cb_size, c.cb_stride, c.zeros, 1, llr, hard, s->scr,
+                       nullptr, st);
+  EqParams p;
+  mb_status r = equalize_prepare(p, reinterpret_cast<const mb_c32 *>(s->csi),
+                                 reinterpret_cast<const mb_c32 *>(s->y_lp), c.K, c.M, c.S,
+                                 c.sg, nb, c.Qm, c.cb_size, c.cb_stride, c.zeros, 1, llr,
+                                 hard, s->scr);
+  if (r != MB_OK) return r;
+  const DeviceTables *tab = device_tables();
+  return equalize_tc(p, s->img_w, s->y_lp, s->S_pad, 0, nb, tab ? tab->err : nullptr, st);
 }
 
 extern "C" mb_status mb_slot_uplink(mb_slot *s, const void *iq, uint16_t *llr,
@@ -243,12 +287,11 @@ extern "C" mb_status mb_slot_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   if (!s->c.use_graph || s->marks_max)
     return issue_uplink(s, iq, llr, hard, status, st, next_marks(s));
   if (!st) return MB_BAD_ARG;  // the legacy stream cannot be captured
-  if (!s->graph || s->g_iq != iq || s->g_llr != llr || s->g_hard != hard ||
-      s->g_status != status || s->g_stream != st) {
-    if (s->graph) {
-      cudaGraphExecDestroy(s->graph);
-      s->graph = nullptr;
-    }
+  constexpr size_t kGraphCache = 16;
+  mb_slot::GraphEntry *hit = nullptr;
+  for (auto &e : s->graphs)
+    if (e.iq == iq && e.llr == llr && e.hard == hard && e.status == status && e.stream == st) hit = &e;
+  if (!hit) {
     MB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     mb_status r = issue_uplink(s, iq, llr, hard, status, st, nullptr);
     cudaGraph_t g = nullptr;
@@ -258,19 +301,22 @@ extern "C" mb_status mb_slot_uplink(mb_slot *s, const void *iq, uint16_t *llr,
       return r;
     }
     if (e != cudaSuccess) return record_error(e);
-    e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-      s->graph = nullptr;
-      return record_error(e);
+    if (e != cudaSuccess) return record_error(e);
+    if (s->graphs.size() >= kGraphCache) {
+      auto lru = s->graphs.begin();
+      for (auto it = s->graphs.begin(); it != s->graphs.end(); ++it)
+        if (it->last_use < lru->last_use) lru = it;
+      cudaGraphExecDestroy(lru->exec);
+      s->graphs.erase(lru);
     }
-    s->g_iq = iq;
-    s->g_llr = llr;
-    s->g_hard = hard;
-    s->g_status = status;
-    s->g_stream = st;
+    s->graphs.push_back({iq, llr, hard, status, st, exec, 0});
+    hit = &s->graphs.back();
   }
-  MB_CUDA_TRY(cudaGraphLaunch(s->graph, st));
+  hit->last_use = ++s->graph_clock;
+  MB_CUDA_TRY(cudaGraphLaunch(hit->exec, st));
   return MB_OK;
 }
 

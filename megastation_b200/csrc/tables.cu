@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "tc.cuh"
 
 namespace mb {
 
@@ -107,6 +108,36 @@ static void cyclic_shift(std::vector<float2> &seq, const std::vector<float2> &in
     float2 v = in[i];
     seq[i] = make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
   }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+mb_status make_tmap_2d_bf16(CUtensorMap *map, const void *base, uint64_t width, uint64_t rows,
+                            uint64_t pitch_elems, uint32_t box_x, uint32_t box_y) {
+  static EncodeTiledFn fn = nullptr;
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!fn) {
+      void *p = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      MB_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+      if (q != cudaDriverEntryPointSuccess || !p) return MB_CUDA_ERROR;
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+  }
+  if ((pitch_elems * 2) % 16 || (reinterpret_cast<uintptr_t>(base) % 16)) return MB_BAD_ARG;
+  cuuint64_t dims[2] = {width, rows};
+  cuuint64_t strides[1] = {pitch_elems * 2};
+  cuuint32_t box[2] = {box_x, box_y};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? MB_OK : MB_BAD_ARG;
 }
 
 }  // namespace mb

@@ -6,6 +6,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include "common.cuh"
+
 namespace mb {
 namespace tc {
 
@@ -142,4 +144,48 @@ __host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N, bool a
 }
 
 }  // namespace tc
+}  // namespace mb
+
+#include <cuda.h>
+
+namespace mb {
+namespace tc {
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// 1-D bulk copy global -> shared, completion counted on the mbarrier
+// (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// 2-D tiled tensor copy global -> shared (box from the tensor map), no
+// multicast; x must be a multiple of 16 bytes / element size
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int32_t x, int32_t y,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+}  // namespace tc
+
+// Host: a 2-D BF16 tensor map over rows of `pitch_elems` elements (row pitch
+// a multiple of 16 bytes), box = box_x elements by box_y rows, no swizzle.
+mb_status make_tmap_2d_bf16(CUtensorMap *map, const void *base, uint64_t width, uint64_t rows,
+                            uint64_t pitch_elems, uint32_t box_x, uint32_t box_y);
+
 }  // namespace mb

@@ -55,3 +55,103 @@ def test_equalize_tc_vs_oracle(mb, K, M, S, sg, n_sym, Qm):
         bits_r = np.unpackbits(hard_r, axis=1)[:, :n_valid]
         sure = np.abs(lr[:, zeros:zeros + n_valid]) > 4.0
         assert (bits_g[sure] == bits_r[sure]).all()
+
+
+@pytest.mark.parametrize("M,K,G", [(256, 32, 7), (64, 16, 5), (128, 64, 3), (200, 24, 4), (8, 4, 2)])
+def test_zf_mixed_vs_oracle(mb, M, K, G):
+    # split-BF16 Gram on tensor cores + FP32 inverse + 2 Newton-Schulz steps;
+    # W via tensor cores: within 1% of max|W| of the FP64 oracle
+    rng = np.random.default_rng(M + K)
+    csi = ((rng.standard_normal((G, M, K)) + 1j * rng.standard_normal((G, M, K))) / np.sqrt(2)).astype(np.complex64)
+    d = dev(csi)
+    status = torch.full((G,), -1, dtype=torch.int32, device="cuda")
+    cond = torch.zeros(G, dtype=torch.float32, device="cuda")
+    mb.Beamform(M, K, G, precision=1).beamform_uplink(d, S=G * 16, sc_group=16, status=status, cond=cond)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    W, cond_r, _ = orc.zf(csi, S=G * 16, sg=16, with_cond=True)
+    got = d.cpu().numpy()
+    assert (status.cpu().numpy() == 0).all()
+    c = cond.cpu().numpy()
+    # 1-norm estimate vs 2-norm condition: within a factor K either way
+    assert ((c >= cond_r / K) & (c <= cond_r * K)).all(), (c, cond_r)
+    for g in range(G):
+        assert np.abs(got[g] - W[g]).max() <= 0.01 * np.abs(W[g]).max(), g
+
+
+def test_zf_mixed_fp64_fallback(mb):
+    # group 1 has two nearly collinear users (user 3 = user 2 + 1e-3 * an
+    # independent vector): cond ~ 1e7 > 1e4 -> FP64 path
+    M, K, G = 64, 8, 3
+    rng = np.random.default_rng(77)
+    csi = ((rng.standard_normal((G, M, K)) + 1j * rng.standard_normal((G, M, K))) / np.sqrt(2)).astype(np.complex64)
+    z = ((rng.standard_normal(M) + 1j * rng.standard_normal(M)) / np.sqrt(2)).astype(np.complex64)
+    csi[1, :, 3] = csi[1, :, 2] + 1e-3 * z
+    d = dev(csi)
+    status = torch.full((G,), -1, dtype=torch.int32, device="cuda")
+    cond = torch.zeros(G, dtype=torch.float32, device="cuda")
+    mb.Beamform(M, K, G, precision=1).beamform_uplink(d, S=G * 16, sc_group=16, status=status, cond=cond)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    st = status.cpu().numpy()
+    assert st[0] == 0 and st[2] == 0 and st[1] == 2, (st, cond.cpu().numpy())
+    W = orc.zf(csi, S=G * 16, sg=16)
+    got = d.cpu().numpy()
+    assert np.abs(got[1] - W[1]).max() <= 1e-4 * np.abs(W[1]).max()
+
+
+CASES = [
+    dict(M=64, K=16, N=2048, S=1200, sg=16, Qm=4, U=5, snr_db=20.0, seed=11),
+    dict(M=128, K=32, N=1024, S=600, sg=16, Qm=6, U=4, snr_db=28.0, seed=12, channel="tdl", rho=0.5,
+         n_taps=4, tap_decay=1.0),
+    dict(M=32, K=8, N=256, S=200, sg=8, Qm=2, U=3, snr_db=12.0, seed=13, iq_dtype="int16"),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"{c['M']}x{c['K']}Q{c['Qm']}" for c in CASES])
+def test_slot_uplink_mixed_vs_oracle(mb, case):
+    from megastation_b200 import datagen, slot
+    cfg = datagen.CellConfig(**case)
+    d = datagen.make_slot(cfg)
+    run = slot.UplinkSlot(cfg, precision="mixed", sym_batch=4, use_graph=True)
+    iq = torch.from_numpy(d["iq"]).cuda()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        run(iq, stream=s)
+        llr, hard = run(iq, stream=s)
+    s.synchronize()
+    assert mb.ops.device_error() == 0
+    assert (run.status.cpu().numpy() == 0).all()
+    llr, hard = llr.cpu().numpy(), hard.cpu().numpy()
+    cb, zeros, stride = cfg.ldpc()
+    n_valid = min(cb, cfg.S * cfg.Qm)
+    ps = orc.pilot_sign(cfg.S)
+    csi = np.zeros((cfg.G, cfg.M, cfg.K), np.complex64)
+    for p in range(cfg.P):
+        orc.pilot_fft(d["iq"][p], cfg.N, cfg.S, cfg.start, cfg.K, cfg.sg, p * cfg.sg, ps, csi)
+    W = orc.zf(csi, S=cfg.S, sg=cfg.sg)
+    for l in range(cfg.U):
+        y = orc.uplink_fft(d["iq"][cfg.P + l], cfg.N, cfg.S, cfg.start)
+        llr_r, _, hard_r = orc.equalize(W, y, cfg.sg, cfg.Qm, cb, stride, zeros, seq=d["seq"][0])
+        lr = llr_r.astype(np.float32)
+        sure = np.abs(lr[:, zeros:zeros + n_valid]) > 4.0
+        bg = np.unpackbits(hard[l], axis=1)[:, :n_valid]
+        br = np.unpackbits(hard_r, axis=1)[:, :n_valid]
+        assert (bg[sure] == br[sure]).all()
+        assert np.abs(llr[l].astype(np.float32) - lr).max() <= 1.0 + 0.02 * np.abs(lr).max()
+
+
+def test_zf_mixed_forced_fp64_path(mb):
+    # a condition threshold below 1 sends every group down the FP64 path
+    M, K, G = 96, 16, 4
+    rng = np.random.default_rng(5)
+    csi = ((rng.standard_normal((G, M, K)) + 1j * rng.standard_normal((G, M, K))) / np.sqrt(2)).astype(np.complex64)
+    d = dev(csi)
+    status = torch.full((G,), -1, dtype=torch.int32, device="cuda")
+    mb.Beamform(M, K, G, precision=1, cond_threshold=0.5).beamform_uplink(d, S=G * 16, sc_group=16,
+                                                                         status=status)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    assert (status.cpu().numpy() == 2).all(), status.cpu().numpy()
+    W = orc.zf(csi, S=G * 16, sg=16)
+    np.testing.assert_allclose(d.cpu().numpy(), W, atol=2e-6 * np.abs(W).max())
