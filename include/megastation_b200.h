@@ -44,7 +44,9 @@ typedef enum {
   MB_CUDA_ERROR = 4,   /* a CUDA runtime call failed */
   MB_TIMEOUT = 5,      /* a bounded device-side wait gave up */
   MB_NO_MEMORY = 6,    /* create-time allocation failed */
-  MB_UNSUPPORTED = 7   /* valid request this build does not implement */
+  MB_UNSUPPORTED = 7,  /* valid request this build does not implement */
+  MB_TOO_LARGE = 8     /* request needs more than mb_equalize_tc_noalloc's
+                          fixed scratch */
 } mb_status;
 
 typedef enum {
@@ -217,6 +219,32 @@ mb_status mb_equalize_tc(const mb_c32 *W, const mb_c32 *y, uint32_t K,
                          uint64_t zeros, uint32_t cb_blocks, uint16_t *llr,
                          uint8_t *hard, const mb_scrambler *scr, mb_c32 *x,
                          void *scratch_img, void *scratch_ylp, void *stream);
+
+/* The same mixed-precision equalize for callers that cannot allocate device
+ * memory (no counterpart in the reference): hosts whose real-time threads
+ * may not enter the driver's allocator, or whose device memory is fixed at
+ * start-up by a framework that owns every allocation.  Inputs, outputs and
+ * results are those of mb_equalize_tc, but the scratch lives in one 32 MiB
+ * array compiled into the library (held by every device that loads it until
+ * the process exits), so the caller passes no scratch and nothing is
+ * allocated or freed.  Limit: the BF16 detector images of all groups plus
+ * the BF16 rows of one symbol, 4*M*ceil8(S) bytes, must fit in 32 MiB;
+ * larger requests return MB_TOO_LARGE (e.g. 256 antennas x 32 users with
+ * 3276 subcarriers fits; symbols beyond what fits are processed in turn).
+ * The first call on each device looks the array's device address up with
+ * cudaGetSymbolAddress (device current); make that first call before any
+ * stream capture.  All calls on a device share the array and it keeps the
+ * previous call's contents: calls that can overlap on the GPU (different
+ * streams, other host threads) race and must be serialised by the caller.
+ * Nothing in the scratch needs to start at zero: every byte a call reads was
+ * written earlier in the same call. */
+mb_status mb_equalize_tc_noalloc(const mb_c32 *W, const mb_c32 *y, uint32_t K,
+                                 uint32_t M, uint32_t S, uint32_t sg,
+                                 uint32_t n_sym, uint32_t Qm, uint64_t cb_size,
+                                 uint64_t cb_stride, uint64_t zeros,
+                                 uint32_t cb_blocks, uint16_t *llr,
+                                 uint8_t *hard, const mb_scrambler *scr,
+                                 mb_c32 *x, void *stream);
 
 /* ------------------------------------------------------------ precode --- */
 /* Precode::precode (sgemv/precode.h:59-61, precode_kernel.cuh:255-262)

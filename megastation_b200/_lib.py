@@ -18,6 +18,7 @@ MB_CUDA_ERROR = 4
 MB_TIMEOUT = 5
 MB_NO_MEMORY = 6
 MB_UNSUPPORTED = 7
+MB_TOO_LARGE = 8
 
 # mb_iq_dtype
 MB_IQ_C32 = 0
@@ -100,6 +101,8 @@ def _load():
         "mb_equalize_tc_scratch": (ST, [U32, U32, U32, U32, U32, ctypes.POINTER(U64), ctypes.POINTER(U64)]),
         "mb_equalize_tc": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U64, U64, U64, U32,
                                 VP, VP, VP, VP, VP, VP, VP]),
+        "mb_equalize_tc_noalloc": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U64, U64, U64, U32,
+                                        VP, VP, VP, VP, VP]),
         "mb_device_error": (ST, [ctypes.POINTER(ctypes.c_int), I32]),
         "mb_precode": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U32, VP, VP]),
         "mb_modulate": (ST, [VP, VP, U64, U64, U64, U32, U32, VP, VP]),

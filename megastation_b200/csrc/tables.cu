@@ -154,6 +154,7 @@ extern "C" const char *mb_status_str(mb_status s) {
     case MB_TIMEOUT: return "device wait timed out";
     case MB_NO_MEMORY: return "out of device memory";
     case MB_UNSUPPORTED: return "unsupported";
+    case MB_TOO_LARGE: return "request exceeds the fixed scratch of mb_equalize_tc_noalloc";
   }
   return "unknown status";
 }
