@@ -1,27 +1,32 @@
 // eq_tc.cu -- equalize + demodulate on the 5th-generation tensor cores.
 //
 // The mixed-precision replacement of the reference's SIMT equalizer
-// (sgemv/equalize_kernel.cuh:27-481).  One CTA per subcarrier group g
-// computes, for all nb symbols of the launch at once, the real-block GEMM
-//     D (MM x N) = A_g (MM x 2*Mp) * B_g (2*Mp x N),   N = nb * sg,
+// (sgemv/equalize_kernel.cuh:27-481).  A CTA takes one subcarrier group g
+// and up to 128 / sg of the launch's symbols, and computes the real-block
+// GEMM
+//     D (128 x N) = Y (128 x 2*Mp) * A_g^T (2*Mp x N),   N = 2K padded to 16,
 // with BF16 operands and FP32 accumulation in tensor memory:
+//   Y   = the planar BF16 FFT output y_lp[sym][plane][b][s], one row per
+//         (symbol, subcarrier) column of the group, reduction index
+//         kk = plane*Mp + b; MN-major in shared memory (each 8 x 16-byte
+//         core matrix is 8 antennas x 8 consecutive subcarriers, one tensor
+//         box of 8 subcarriers x 64 antennas per 1 KB);
 //   A_g = R(W_g^T) with rows interleaved (2u: real part of user u, 2u+1:
-//         imaginary part) and reduction index kk = plane*Mp + b
-//         (plane 0 multiplies Re y, plane 1 multiplies Im y); the ZF kernel
-//         writes A_g into global memory already in the shared-memory image
-//         of the K-major no-swizzle canonical layout, one 64-wide k tile at
-//         a time, so the CTA copies it with plain 16-byte loads;
-//   B_g = the planar BF16 FFT output y_lp[sym][plane][b][s], MN-major: each
-//         8 x 16-byte core matrix is 8 antennas x 8 consecutive subcarriers.
-// Row pairs (2u, 2u+1) land in adjacent TMEM lanes, so after tcgen05.ld one
-// shuffle gives each thread the complex x of 8 subcarriers, which it demaps
-// (modulation/demodulation.h:30-67 in FP16), stores as LLRs in the code-block
-// layout and packs into descrambled hard-bit bytes.
+//         imaginary part); the ZF kernel writes it into global memory already
+//         in the shared-memory image of the K-major no-swizzle canonical
+//         layout, one 64-wide k tile at a time, so one bulk copy per tile
+//         stages it.
+// D row i sits in TMEM lane i: every thread of the epilogue owns one
+// (symbol, subcarrier) and reads the complex x of all K users from its own
+// lane, demaps each (modulation/demodulation.h:30-67 in FP16), and stores the
+// LLRs, so that consecutive lanes write consecutive stretches of each user's
+// LLR row.  Hard bits of 8 neighbouring subcarriers are gathered with three
+// shuffles into whole descrambled bytes.
 //
-// Pipeline: 3 shared-memory stages; all 128 threads stage tile kt while the
-// tensor core works on tile kt-1; one thread issues the 4 MMAs per tile and
-// commits them to the stage's mbarrier.  Every wait is bounded in time and
-// reports a timeout through the device error word.
+// Pipeline: kStages shared-memory stages fed by one producer thread (bulk
+// copy + tensor boxes); one thread issues the 4 MMAs per tile and commits
+// them to the stage's mbarrier.  Every wait is bounded in time and reports a
+// timeout through the device error word.
 #include <algorithm>
 #include <atomic>
 
@@ -34,12 +39,12 @@
 namespace mb {
 
 namespace {
-constexpr int kStages = 4;
-constexpr int kKT = 64;  // reduction elements per k tile (4 MMAs of K=16)
-
+constexpr int kStages = 3;
+constexpr int kKT = 64;     // reduction elements per k tile (4 MMAs of K=16)
+constexpr int kCols = 128;  // MMA M: (symbol, subcarrier) columns per CTA
 }  // namespace
 
-template <int MM>
+template <int MM, int QM>
 __global__ void __launch_bounds__(128, 1)
     equalize_tc_kernel(const EqTcParams q, const __grid_constant__ CUtensorMap ymap) {
   extern __shared__ __align__(1024) uint8_t eq_smem[];
@@ -55,10 +60,11 @@ __global__ void __launch_bounds__(128, 1)
   // this CTA's symbols: l_off .. l_off + nbc - 1 of the launch
   const uint32_t l_off = blockIdx.y * q.spc;
   const uint32_t nbc = min(q.spc, q.nb - l_off);
-  const uint32_t N = nbc * p.sg;
-  const uint32_t a_tile = MM * kKT * 2;           // bytes
-  const uint32_t b_tile = kKT * q.spc * p.sg * 2; // stage room: N_max/8 boxes of 8 x 64 BF16
-  const uint32_t b_bytes = kKT * N * 2;           // bytes this CTA loads per tile
+  const uint32_t ncols = nbc * p.sg;                 // valid columns, <= 128
+  constexpr uint32_t y_tile = kCols * kKT * 2;       // 16 KB: 128 columns x 64 kk
+  constexpr uint32_t a_tile = MM * kKT * 2;          // detector image k tile
+  constexpr uint32_t stage_bytes = y_tile + a_tile;
+  const uint32_t y_bytes = ncols * kKT * 2;          // bytes this CTA loads per tile
   const uint32_t s_base = g * p.sg;
 
   if (tid == 0) {
@@ -78,7 +84,7 @@ __global__ void __launch_bounds__(128, 1)
   const uint32_t tmem = tmem_base_slot;
 
   if (warp == 0 && lane == 0) {
-    // ---- producer: detector image tile by bulk copy, y_lp by tensor boxes
+    // ---- producer: y columns by tensor boxes, detector image by bulk copy
     const uint8_t *a_g = q.a_img + (uint64_t)g * q.nkt * a_tile;
     for (uint32_t kt = 0; kt < q.nkt; kt++) {
       const uint32_t s = kt % kStages, use = kt / kStages;
@@ -86,20 +92,21 @@ __global__ void __launch_bounds__(128, 1)
         timed_out = 1;
         break;
       }
-      uint8_t *sa = eq_smem + s * (a_tile + b_tile);
-      uint8_t *sb = sa + a_tile;
-      tc::mbar_arrive_expect_tx(&full_bar[s], a_tile + b_bytes);
+      uint8_t *sy = eq_smem + s * stage_bytes;
+      uint8_t *sa = sy + y_tile;
+      tc::mbar_arrive_expect_tx(&full_bar[s], y_bytes + a_tile);
       tc::bulk_g2s(sa, a_g + (uint64_t)kt * a_tile, a_tile, &full_bar[s]);
       const uint32_t kk0 = kt * kKT, plane = kk0 / q.Mp, b0 = kk0 % q.Mp;
-      for (uint32_t j = 0; j < N / 8; j++) {
+      for (uint32_t j = 0; j < ncols / 8; j++) {
         const uint32_t col0 = j * 8, l = col0 / p.sg, sl = col0 % p.sg;
         const int32_t row = (int32_t)(((l_off + l) * 2 + plane) * p.M + b0);
-        tc::tma_load_2d(sb + j * 1024, &ymap, (int32_t)(s_base + sl), row, &full_bar[s]);
+        tc::tma_load_2d(sy + j * 1024, &ymap, (int32_t)(s_base + sl), row, &full_bar[s]);
       }
     }
   } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer
-    const uint32_t idesc = tc::idesc_bf16(MM, N, false, true);
+    // ---- MMA issuer.  Columns ncols..127 of the y stage are never loaded:
+    // their D rows are garbage and no thread stores them.
+    const uint32_t idesc = tc::idesc_bf16(kCols, q.N, true, false);
     bool ok = true;
     for (uint32_t kt = 0; kt < q.nkt; kt++) {
       const uint32_t s = kt % kStages, use = kt / kStages;
@@ -108,15 +115,15 @@ __global__ void __launch_bounds__(128, 1)
         break;
       }
       tc::fence_after_sync();
-      const uint32_t a0 = tc::smem_u32(eq_smem + s * (a_tile + b_tile)), b0 = a0 + a_tile;
+      const uint32_t y0 = tc::smem_u32(eq_smem + s * stage_bytes), a0 = y0 + y_tile;
 #pragma unroll
       for (int ks = 0; ks < kKT / 16; ks++) {
-        // A: K-major, K core matrices 128 B apart, 8-row groups 1024 B apart
-        const uint64_t ad = tc::smem_desc(a0 + ks * 256, 128, 1024);
-        // B: MN-major, 8-antenna K groups 128 B apart, 8-subcarrier MN
+        // Y: MN-major, 8-antenna K groups 128 B apart, 8-subcarrier MN
         // chunks 1024 B apart (one tensor box each)
-        const uint64_t bd = tc::smem_desc(b0 + ks * 256, 128, 1024);
-        tc::mma_f16(tmem, ad, bd, idesc, (kt | ks) != 0);
+        const uint64_t yd = tc::smem_desc(y0 + ks * 256, 128, 1024);
+        // image: K-major, K core matrices 128 B apart, 8-row groups 1024 B apart
+        const uint64_t ad = tc::smem_desc(a0 + ks * 256, 128, 1024);
+        tc::mma_f16(tmem, yd, ad, idesc, (kt | ks) != 0);
       }
       tc::mma_commit(&empty_bar[s]);
     }
@@ -130,56 +137,82 @@ __global__ void __launch_bounds__(128, 1)
     if (tid == 0 && q.err) atomicOr(q.err, tc::kErrTimeout);
   } else {
     tc::fence_after_sync();
-    // epilogue: warp w reads TMEM lanes 32w..32w+31; rows (2u, 2u+1) are
-    // adjacent lanes, exchanged with one shuffle
-    const int rows_per_warp = MM == 64 ? 16 : 32;
-    const bool lane_ok = lane < rows_per_warp;
-    const uint32_t r = warp * rows_per_warp + lane;  // D row of this lane
-    const uint32_t u = r / 2;
-    const bool is_im = r & 1;
-    const bool valid = lane_ok && u < p.K;
-    for (uint32_t ch = 0; ch < (N + 15) / 16; ch++) {
+    // thread = D row = TMEM lane 32 warp + lane = column (symbol l, subcarrier sl)
+    const uint32_t c = warp * 32 + lane;
+    const uint32_t l = c / p.sg, sl = c % p.sg;
+    const uint32_t s = s_base + sl;
+    const bool valid = c < ncols && s < p.S;
+    const uint32_t lg = q.l0 + l_off + l;
+    // LLR placement of subcarrier s (equalize_kernel.cuh:272-287), the same
+    // for every user: code block cb, offset base in the (symbol, user) row
+    const uint32_t t0 = s * QM;
+    const uint32_t cb = t0 / p.cb_size32;
+    const uint32_t base = cb * p.cb_stride32 + p.zeros32 + (t0 - cb * p.cb_size32);
+    const bool llr_on = valid && cb < p.cb_blocks;
+    const bool pair = base + QM <= p.row_len32 && ((p.row_len32 | base) & 1) == 0 &&
+                      (reinterpret_cast<uintptr_t>(p.llr) & 3) == 0;
+    __half *lpu = reinterpret_cast<__half *>(p.llr) + (uint64_t)lg * p.K * p.row_len + base;
+    // hard bits: stream positions < n_valid only, first bit most significant
+    uint32_t nvm = 0;
+#pragma unroll
+    for (int qb = 0; qb < QM; qb++)
+      if (t0 + qb < p.n_valid32) nvm |= 1u << (QM - 1 - qb);
+    if (!valid) nvm = 0;
+    // 8-lane groups hold 8 consecutive subcarriers of one symbol (sg % 8 ==
+    // 0); after the OR-reduction lane gl of a group writes byte gl of the
+    // group's QM bytes (a group cut short by S pads its last byte with zeros)
+    const uint32_t gl = lane & 7;
+    const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
+    const uint32_t nvalid = __popc((vmask >> (lane & ~7u)) & 0xFFu);
+    const uint32_t gb = (s - gl) * QM / 8 + gl;
+    const bool byte_on = p.hard && gl < (nvalid * QM + 7) / 8 && gb * 8 < p.n_valid32;
+    const uint32_t end = p.n_valid32 - gb * 8;
+    const uint8_t seq_mask = byte_on && end < 8 ? (uint8_t)(0xFF00u >> end) : (uint8_t)0xFF;
+    uint8_t *hpu = p.hard ? p.hard + (uint64_t)lg * p.K * p.hrow + gb : nullptr;
+    const uint8_t *spu = p.seqb ? p.seqb + gb : nullptr;
+    float2 *xpu = p.x ? p.x + (uint64_t)lg * p.K * p.S + s : nullptr;
+    const __half zero = __float2half_rn(0.f);
+    for (uint32_t ch = 0; ch < q.N / 16; ch++) {
       float v[16];
       tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + ch * 16, v);
-      float re8[8], im8[8];
 #pragma unroll
-      for (int i = 0; i < 8; i++) {
-        // even lane keeps columns 0-7, odd lane 8-15
-        const float send = is_im ? v[i] : v[8 + i];
-        const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
-        re8[i] = is_im ? recv : v[i];
-        im8[i] = is_im ? v[8 + i] : recv;
-      }
-      if (!valid) continue;
-      const uint32_t c0 = ch * 16 + (is_im ? 8 : 0);
-      if (c0 >= N) continue;  // N % 16 == 8: the last chunk is half full
-      const uint32_t l = c0 / p.sg, sl0 = c0 % p.sg;
-      const uint32_t s0 = s_base + sl0;
-      const uint32_t lg = q.l0 + l_off + l;
-      __half *llr_row = reinterpret_cast<__half *>(p.llr) + ((uint64_t)lg * p.K + u) * p.row_len;
-      uint64_t hbits = 0;
-      int nbits = 0;
+      for (int j = 0; j < 8; j++) {
+        if (ch * 8 + j >= p.K) break;
+        const float2 x = make_float2(v[2 * j], v[2 * j + 1]);
+        __half lv[8];
+        demod(QM, x, lv);
+        if (llr_on) {
+          if (pair) {
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
-        const uint32_t s = s0 + e;
-        if (s >= p.S) break;
-        const float2 x = make_float2(re8[e], im8[e]);
-        if (p.x) p.x[((uint64_t)lg * p.K + u) * p.S + s] = x;
-        hbits = (hbits << p.Qm) | eq_demap_store(p, llr_row, s, x);
-        nbits += p.Qm;
-      }
-      if (p.hard && nbits) {
-        // 8 subcarriers from s0 % 8 == 0 give whole bytes; a group cut short
-        // by S pads the last byte with zeros
-        const uint32_t byte0 = s0 * p.Qm / 8;
-        uint8_t *hrow = p.hard + ((uint64_t)lg * p.K + u) * p.hrow;
-        const int nbytes = (nbits + 7) / 8;
-        if (nbits % 8) hbits <<= (8 - nbits % 8);
-        for (int bI = 0; bI < nbytes; bI++) {
-          const uint32_t gb = byte0 + bI;
-          if (gb * 8 >= p.n_valid32) break;
-          hrow[gb] = (uint8_t)(hbits >> (8 * (nbytes - 1 - bI))) ^ eq_seq_byte(p, u, gb);
+            for (int qb = 0; qb < QM; qb += 2)
+              reinterpret_cast<__half2 *>(lpu)[qb / 2] = __halves2half2(lv[qb], lv[qb + 1]);
+          } else {
+#pragma unroll
+            for (int qb = 0; qb < QM; qb++)
+              if (base + qb < p.row_len32) lpu[qb] = lv[qb];
+          }
         }
+        if (hpu) {
+          uint32_t hb = 0;
+#pragma unroll
+          for (int qb = 0; qb < QM; qb++) hb = (hb << 1) | (__hlt(lv[qb], zero) ? 1u : 0u);
+          uint64_t w = (uint64_t)(hb & nvm) << (64 - QM * (gl + 1));
+          w |= __shfl_xor_sync(0xffffffffu, w, 1);
+          w |= __shfl_xor_sync(0xffffffffu, w, 2);
+          w |= __shfl_xor_sync(0xffffffffu, w, 4);
+          if (byte_on) {
+            uint8_t bt = (uint8_t)(w >> (56 - 8 * gl));
+            if (spu) bt ^= __ldg(spu) & seq_mask;
+            *hpu = bt;
+          }
+          hpu += p.hrow;
+          if (spu) spu += p.seq_row_bytes;
+        }
+        if (xpu) {
+          if (valid) *xpu = x;
+          xpu += p.S;
+        }
+        lpu += p.row_len;
       }
     }
   }
@@ -229,14 +262,40 @@ mb_status w_image(const float2 *W, void *img, uint32_t G, uint32_t M, uint32_t K
   return MB_OK;
 }
 
+using EqTcKernel = void (*)(const EqTcParams, const CUtensorMap);
+
+template <int MM>
+static EqTcKernel eq_tc_kernel_of(uint32_t Qm) {
+  switch (Qm) {
+    case 2: return equalize_tc_kernel<MM, 2>;
+    case 4: return equalize_tc_kernel<MM, 4>;
+    case 6: return equalize_tc_kernel<MM, 6>;
+    default: return equalize_tc_kernel<MM, 8>;
+  }
+}
+
+// raises the dynamic shared memory limit of the (MM, Qm) kernel once per device
+static mb_status equalize_tc_configure(uint32_t MM, uint32_t Qm, int dev) {
+  static std::atomic<uint64_t> configured[8] = {};
+  const int which = (MM == 64 ? 0 : 4) + (Qm == 2 ? 0 : Qm == 4 ? 1 : Qm == 6 ? 2 : 3);
+  const uint64_t bit = 1ull << (dev & 63);
+  if (configured[which].load() & bit) return MB_OK;
+  int maxs = 0;
+  MB_CUDA_TRY(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const EqTcKernel k = MM == 64 ? eq_tc_kernel_of<64>(Qm) : eq_tc_kernel_of<128>(Qm);
+  cudaFuncAttributes fa;
+  MB_CUDA_TRY(cudaFuncGetAttributes(&fa, k));
+  MB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   maxs - (int)fa.sharedSizeBytes));
+  configured[which].fetch_or(bit);
+  return MB_OK;
+}
+
 bool equalize_tc_supported(uint32_t K, uint32_t sg, uint32_t nb) {
-  const uint32_t N = nb * sg;
-  if (K == 0 || K > 64 || sg % 8 != 0) return false;
-  const uint32_t MM = 2 * K <= 64 ? 64 : 128;
-  if (N == 0 || N > 256 || N % 8 != 0) return false;  // MMA N rule for M = 64
-  // M = 128 needs N % 16: keep every per-CTA symbol chunk legal
-  if (MM == 128 && sg % 16 != 0) return false;
-  return true;
+  // a CTA holds whole symbols of one group in its 128 columns; the MMA's N
+  // is 2K rounded up to 16 (at most the image's MM rows)
+  if (K == 0 || K > 64 || sg == 0 || sg % 8 != 0 || sg > (uint32_t)kCols) return false;
+  return nb >= 1;
 }
 
 mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, uint32_t S_pad,
@@ -251,50 +310,30 @@ mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, ui
   q.S_pad = S_pad;
   q.Mp = s.Mp;
   q.nkt = s.nkt;
-  // symbols per CTA: about 32 columns, so a launch has several CTAs per
-  // group and each CTA's epilogue stays short
-  q.spc = std::max<uint32_t>(1, std::min<uint32_t>(nb, 32 / p.sg));
-  while (q.spc > 1 && (q.spc * p.sg) % (s.MM == 64 ? 8 : 16)) q.spc--;
+  // symbols per CTA: as many as fill 128 columns, spread evenly over the
+  // CTAs a group needs
+  const uint32_t spc_max = kCols / p.sg;
+  const uint32_t ny = (nb + spc_max - 1) / spc_max;
+  q.spc = (nb + ny - 1) / ny;
   q.nb = nb;
-  q.N = q.spc * p.sg;
+  q.N = (2 * p.K + 15) / 16 * 16;
   q.l0 = l0;
   q.err = err;
   q.tmem_cols = 32;
   while (q.tmem_cols < q.N) q.tmem_cols *= 2;
-  const size_t smem = (size_t)kStages * (s.MM * kKT * 2 + kKT * q.N * 2);
+  const size_t smem = (size_t)kStages * ((size_t)kCols * kKT * 2 + (size_t)s.MM * kKT * 2);
   const uint32_t G = (p.S + p.sg - 1) / p.sg;
-  static std::atomic<uint64_t> configured[2] = {{0}, {0}};
   int dev = 0;
   MB_CUDA_TRY(cudaGetDevice(&dev));
-  const uint64_t bit = 1ull << (dev & 63);
-  const int which = s.MM == 64 ? 0 : 1;
-  if (!(configured[which].load() & bit)) {
-    int maxs = 0;
-    MB_CUDA_TRY(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    cudaFuncAttributes fa;
-    if (which == 0) {
-      MB_CUDA_TRY(cudaFuncGetAttributes(&fa, equalize_tc_kernel<64>));
-      MB_CUDA_TRY(cudaFuncSetAttribute(equalize_tc_kernel<64>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       maxs - (int)fa.sharedSizeBytes));
-    } else {
-      MB_CUDA_TRY(cudaFuncGetAttributes(&fa, equalize_tc_kernel<128>));
-      MB_CUDA_TRY(cudaFuncSetAttribute(equalize_tc_kernel<128>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       maxs - (int)fa.sharedSizeBytes));
-    }
-    configured[which].fetch_or(bit);
-  }
+  mb_status cs = equalize_tc_configure(s.MM, p.Qm, dev);
+  if (cs != MB_OK) return cs;
   // tensor map over y_lp rows [nb * 2 * M][S_pad], box 8 subcarriers x 64
   // antennas (one 1 KB group of MN-major core matrices)
   CUtensorMap ymap;
   mb_status tr = make_tmap_2d_bf16(&ymap, y_lp, S_pad, (uint64_t)nb * 2 * p.M, S_pad, 8, kKT);
   if (tr != MB_OK) return tr;
-  const dim3 grid(G, (nb + q.spc - 1) / q.spc);
-  if (s.MM == 64)
-    equalize_tc_kernel<64><<<grid, 128, smem, st>>>(q, ymap);
-  else
-    equalize_tc_kernel<128><<<grid, 128, smem, st>>>(q, ymap);
+  const dim3 grid(G, ny);
+  (s.MM == 64 ? eq_tc_kernel_of<64>(p.Qm) : eq_tc_kernel_of<128>(p.Qm))<<<grid, 128, smem, st>>>(q, ymap);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }

@@ -30,7 +30,6 @@ struct mb_slot {
   float2 *y;          // [sym_batch][M][S] uplink FFT output (FP32 path)
   void *y_lp;         // [sym_batch][re|im][M][S_pad] BF16 (mixed path)
   void *img_w;        // detector images for the tensor-core equalizer
-  void *img_c;        // mixed ZF scratch
   uint32_t S_pad;
   float2 *precoded;   // [D][M][N]
   cudaStream_t side;
@@ -114,7 +113,6 @@ extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   cudaFree(s->y);
   cudaFree(s->y_lp);
   cudaFree(s->img_w);
-  cudaFree(s->img_c);
   cudaFree(s->precoded);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
@@ -161,7 +159,6 @@ extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
   if (mixed) {
     alloc(&s->y_lp, ylp_bytes);
     alloc(&s->img_w, zf_mixed_scratch_bytes(s->G, c.M, c.K));
-    alloc(&s->img_c, zf_mixed_scratch_bytes(s->G, c.M, c.K));
     if (st == MB_OK) {
       // the S_pad - S padding columns are never written by the FFT
       cudaError_t e = cudaMemset(s->y_lp, 0, ylp_bytes);
@@ -226,7 +223,7 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   float2 *prec = c.D ? s->precoder : nullptr;
   if (mixed) {
     mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, 0};
-    r = zf_mixed_run(s->csi, s->img_w, s->img_c, s->G, c.M, c.K, &o, status, nullptr, st);
+    r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, st);
     if (r == MB_OK && prec) r = precoder_launch(s->csi, prec, c.M, c.K, s->G, st);
   } else {
     r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, st);

@@ -287,7 +287,7 @@ using namespace mb;
 
 struct mb_zf {
   uint32_t M, K, max_groups;
-  void *img_w, *img_c;  // mixed-precision scratch, sized for max_groups
+  void *img_w;  // mixed-precision detector images, sized for max_groups
 };
 
 extern "C" mb_status mb_zf_create(uint32_t num_bs, uint32_t num_ue,
@@ -297,13 +297,10 @@ extern "C" mb_status mb_zf_create(uint32_t num_bs, uint32_t num_ue,
   if (num_bs == 0 || num_ue == 0 || num_ue > num_bs || num_ue > 64)
     return MB_BAD_SHAPE;
   if (!device_tables()) return MB_CUDA_ERROR;
-  mb_zf *z = new mb_zf{num_bs, num_ue, max_groups, nullptr, nullptr};
+  mb_zf *z = new mb_zf{num_bs, num_ue, max_groups, nullptr};
   const uint64_t bytes = zf_mixed_scratch_bytes(max_groups, num_bs, num_ue);
   cudaError_t e = cudaSuccess;
-  if (bytes) {
-    e = cudaMalloc(&z->img_w, bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&z->img_c, bytes);
-  }
+  if (bytes) e = cudaMalloc(&z->img_w, bytes);
   if (e != cudaSuccess) {
     cudaFree(z->img_w);
     delete z;
@@ -316,7 +313,6 @@ extern "C" mb_status mb_zf_create(uint32_t num_bs, uint32_t num_ue,
 extern "C" mb_status mb_zf_destroy(mb_zf *z) {
   if (!z) return MB_BAD_ARG;
   cudaFree(z->img_w);
-  cudaFree(z->img_c);
   delete z;
   return MB_OK;
 }
@@ -340,7 +336,7 @@ extern "C" mb_status mb_zf_uplink(mb_zf *z, mb_c32 *csi, uint32_t groups,
     case MB_ZF_FP64:
       return zf_chol(c, nullptr, groups, z->M, z->K, true, status, cond, st);
     case MB_ZF_MIXED:
-      return zf_mixed_run(c, z->img_w, z->img_c, groups, z->M, z->K, opts, status, cond, st);
+      return zf_mixed_run(c, z->img_w, groups, z->M, z->K, opts, status, cond, st);
   }
   return MB_BAD_ARG;
 }

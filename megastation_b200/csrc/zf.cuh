@@ -12,12 +12,10 @@ mb_status zf_chol(float2 *csi, float2 *precoder, uint32_t groups, uint32_t M,
                   uint32_t K, bool dbl, int32_t *status, float *cond,
                   cudaStream_t st);
 // mixed precision ZF (zf_mixed.cu): W in place (FP32) plus the detector
-// images for the tensor-core equalizer in img_w; img_c is scratch of the same
-// size (zf_mixed_scratch_bytes each)
+// images for the tensor-core equalizer in img_w (zf_mixed_scratch_bytes)
 uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K);
-mb_status zf_mixed_run(float2 *csi, void *img_w, void *img_c, uint32_t groups, uint32_t M,
-                       uint32_t K, const mb_zf_opts *opts, int32_t *status, float *cond,
-                       cudaStream_t st);
+mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
+                       const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st);
 mb_status precoder_launch(const float2 *W, float2 *P, uint32_t M, uint32_t K,
                           uint32_t groups, cudaStream_t st);
 size_t zf_chol_smem(uint32_t M, uint32_t K, bool dbl);

@@ -5,18 +5,22 @@
 // one CTA per group does, in one kernel:
 //  1. Gram on tcgen05: with R(C) the real embedding of C (row 2u = [Re C_u,
 //     -Im C_u], row 2u+1 = [Im C_u, Re C_u] over the reduction index
-//     kk = plane*Mp + b), R(G) = R(C) R(C)^T.  R(C) is split into BF16
-//     hi + lo parts and R(G) ~ hi hi^T + hi lo^T + lo hi^T accumulates in
-//     FP32 in tensor memory: BF16 operands, FP32 accumulation, and a Gram
-//     accurate to ~2^-16 (a plain BF16 Gram costs ~0.25 dB of EVM at
-//     256x32, which the split removes).  The same shared-memory tile is both
-//     MMA operands (A = R(C), B^T = R(C), both K-major).
-//  2. FP32 Cholesky of G, explicit inverse X, 1-norm condition estimate
-//     ||G||_1 ||X||_1, then ns_iters Newton-Schulz steps X <- X (2I - G X).
-//  3. W = X C on tcgen05: D = R(X) R(C) gives, row for row, the detector
-//     image the tensor-core equalizer consumes (eq_tc.cu); the hi image of
-//     R(C) written in step 1 is re-read as the MN-major B operand.  The
-//     epilogue stores that image (BF16) and W in the CSI layout (FP32).
+//     kk = plane*Mp + b), R(G) = R(C) R(C)^T.  Plane 1 of R(C) is P times
+//     plane 0 (P = diag of [[0,-1],[1,0]] blocks), so only the plane-0 tiles
+//     T are multiplied: A = sum T T^T and R(G) = A + P A P^T.  T is split
+//     into BF16 hi + lo parts and A ~ hi hi^T + hi lo^T + lo hi^T
+//     accumulates in FP32 in tensor memory: BF16 operands, FP32
+//     accumulation, and a Gram accurate to ~2^-16 (a plain BF16 Gram costs
+//     ~0.25 dB of EVM at 256x32, which the split removes).  The same
+//     shared-memory tile is both MMA operands (A = T, B^T = T, both K-major).
+//  2. FP32 Gauss-Jordan inverse X of G (registers, one barrier per pivot),
+//     ns_iters Newton-Schulz steps X <- X (2I - G X), then the 1-norm
+//     condition estimate ||G||_1 ||X||_1.
+//  3. W = X C on tcgen05: D0 = R(X) T over the plane-0 tiles, which stay in
+//     shared memory from step 1 (re-built from the CSI when they do not
+//     fit), gives row for row the plane-0 half of the detector image the
+//     tensor-core equalizer consumes (eq_tc.cu); the plane-1 half is P D0.
+//     The epilogue stores that image (BF16) and W in the CSI layout (FP32).
 //  4. Groups whose Gram is not positive definite in FP32, or whose condition
 //     estimate exceeds cond_threshold, are redone in FP64 (Gram, Cholesky,
 //     solve) and reported with status 2 (1 if even FP64 fails).
@@ -35,13 +39,14 @@ constexpr int kKT = 64;        // reduction elements per k tile
 constexpr int kThreads = 256;  // 8 warps; warps w and w+4 share TMEM lane quadrant w
 
 struct ZfmParams {
-  float2 *csi;       // [G][M][K]: in CSI, out W (FP32)
-  uint8_t *img_w;    // [G] detector images for the equalizer (BF16)
-  uint8_t *img_c;    // [G] scratch: hi image of R(C)
+  float2 *csi;        // [G][M][K]: in CSI, out W (FP32)
+  uint8_t *img_w;     // [G] detector images for the equalizer (BF16)
   int32_t *status;
   float *cond;
   int *err;
   uint32_t M, K, Mp, nkt, ns_iters;
+  uint32_t nh;        // plane-0 k tiles: Mp / 64
+  uint32_t resident;  // 1: all nh hi tiles stay in shared memory for W = X C
   float cond_thr;
 };
 
@@ -49,10 +54,6 @@ __device__ __forceinline__ uint32_t img_off(uint32_t r, uint32_t kk, uint32_t MM
   // canonical K-major, no swizzle: [k tile][row group][k chunk][row][8]
   const uint32_t kt = kk / kKT, kin = kk % kKT;
   return kt * (MM * kKT * 2) + (r / 8) * 1024 + (kin / 8) * 128 + (r % 8) * 16 + (kin % 8) * 2;
-}
-
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
 // In-place Cholesky of the K x K Hermitian matrix A (lower, leading dim lda)
@@ -91,6 +92,130 @@ __device__ bool chol_smem(C *A, uint32_t K, uint32_t lda, int *flag) {
   }
   return *flag == 0;
 }
+
+// In-place inverse of the K x K Hermitian positive definite matrix G (leading
+// dim ld) into X by Gauss-Jordan on [G | I] without pivoting: every pivot of
+// a positive definite matrix is real and positive.  The matrix is padded to
+// KP x KP with an identity block.  Thread t holds row t / TPR of [G | I] in
+// registers, columns t % TPR + TPR m; the pivot row goes through shared
+// memory (prow, two buffers of 2 KP), so each pivot costs one barrier.
+// Returns false when a pivot is not positive (the output is then garbage).
+template <int KP>
+__device__ __forceinline__ bool gj_inverse(const float2 *G, float2 *X, uint32_t K, uint32_t ld,
+                                           float2 *prow, int *bad) {
+  constexpr int TPR = kThreads / KP, NC = 2 * KP / TPR;
+  const uint32_t i = threadIdx.x / TPR, sub = threadIdx.x % TPR;
+  float2 v[NC];
+#pragma unroll
+  for (int m = 0; m < NC; m++) {
+    const uint32_t c = sub + TPR * m;
+    if (m < NC / 2)
+      v[m] = (i < K && c < K) ? G[i * ld + c] : make_float2(i == c ? 1.f : 0.f, 0.f);
+    else
+      v[m] = make_float2(c - KP == i ? 1.f : 0.f, 0.f);
+  }
+#pragma unroll
+  for (int mk = 0; mk < NC / 2; mk++) {
+#pragma unroll 1
+    for (uint32_t s = 0; s < (uint32_t)TPR; s++) {
+      const uint32_t k = mk * TPR + s;
+      float2 f;  // this row's entry in column k
+      f.x = __shfl_sync(0xffffffffu, v[mk].x, s, TPR);
+      f.y = __shfl_sync(0xffffffffu, v[mk].y, s, TPR);
+      float2 *pr = prow + (k & 1) * 2 * KP;
+      if (i == k) {
+        if (!(f.x > 0.f)) *bad = 1;
+        const float inv = 1.f / f.x;
+#pragma unroll
+        for (int m = 0; m < NC; m++) {
+          v[m].x *= inv;
+          v[m].y *= inv;
+          pr[sub + TPR * m] = v[m];
+        }
+      }
+      __syncthreads();
+      if (i != k) {
+#pragma unroll
+        for (int m = 0; m < NC; m++) {
+          const float2 r = pr[sub + TPR * m];
+          v[m].x -= f.x * r.x - f.y * r.y;
+          v[m].y -= f.x * r.y + f.y * r.x;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const bool ok = *bad == 0;
+  if (i < K) {
+#pragma unroll
+    for (int m = NC / 2; m < NC; m++) {
+      const uint32_t c = sub + TPR * m - KP;
+      if (c < K) X[i * ld + c] = v[m];
+    }
+  }
+  __syncthreads();
+  return ok;
+}
+
+// C = A B for K x K complex matrices in shared memory (leading dims given);
+// out(i, j, c) receives each entry.  Thread t owns the outputs
+// (t / 16 + 16a, t % 16 + 16b), a, b < T: T*T independent accumulators that
+// share each A and B load.  Needs 256 threads and K <= 16 T.
+template <int T, typename Out>
+__device__ __forceinline__ void cmatmul(const float2 *A, uint32_t lda, const float2 *B, uint32_t ldb,
+                                        uint32_t K, Out out) {
+  const uint32_t ti = threadIdx.x / 16, tj = threadIdx.x % 16;
+  float2 acc[T][T];
+#pragma unroll
+  for (int a = 0; a < T; a++)
+#pragma unroll
+    for (int b = 0; b < T; b++) acc[a][b] = make_float2(0.f, 0.f);
+#pragma unroll 4
+  for (uint32_t k = 0; k < K; k++) {
+    float2 av[T], bv[T];
+#pragma unroll
+    for (int a = 0; a < T; a++) {
+      const uint32_t i = ti + 16 * a;
+      av[a] = i < K ? A[i * lda + k] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int b = 0; b < T; b++) {
+      const uint32_t j = tj + 16 * b;
+      bv[b] = j < K ? B[k * ldb + j] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int a = 0; a < T; a++)
+#pragma unroll
+      for (int b = 0; b < T; b++) {
+        acc[a][b].x = fmaf(av[a].x, bv[b].x, fmaf(-av[a].y, bv[b].y, acc[a][b].x));
+        acc[a][b].y = fmaf(av[a].x, bv[b].y, fmaf(av[a].y, bv[b].x, acc[a][b].y));
+      }
+  }
+#pragma unroll
+  for (int a = 0; a < T; a++)
+#pragma unroll
+    for (int b = 0; b < T; b++) {
+      const uint32_t i = ti + 16 * a, j = tj + 16 * b;
+      if (i < K && j < K) out(i, j, acc[a][b]);
+    }
+}
+
+// K <= MM / 2: MM = 64 covers K <= 32, MM = 128 covers K <= 64
+template <int MM, typename Out>
+__device__ __forceinline__ void cmatmul_any(const float2 *A, uint32_t lda, const float2 *B, uint32_t ldb,
+                                            uint32_t K, Out out) {
+  if (MM == 64) {
+    if (K <= 16)
+      cmatmul<1>(A, lda, B, ldb, K, out);
+    else
+      cmatmul<2>(A, lda, B, ldb, K, out);
+  } else {
+    if (K <= 48)
+      cmatmul<3>(A, lda, B, ldb, K, out);
+    else
+      cmatmul<4>(A, lda, B, ldb, K, out);
+  }
+}
 }  // namespace
 
 template <int MM>
@@ -99,26 +224,30 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   __shared__ __align__(8) uint64_t tile_bar[2];
   __shared__ __align__(8) uint64_t mma_bar;
   __shared__ uint32_t tmem_slot;
-  __shared__ int flag, fail;
-  __shared__ float red[kThreads];
+  __shared__ int flag, fail, piv_bad;
+  __shared__ float red[kThreads], red2[kThreads];
+  __shared__ float2 prow[2 * MM];  // Gauss-Jordan pivot rows, two buffers of 2 KP <= MM
 
-  const uint32_t g = blockIdx.x, K = q.K, M = q.M, Mp = q.Mp;
+  constexpr uint32_t tile_bytes = MM * kKT * 2;
+  constexpr uint32_t TC = 256;             // TMEM columns: the Gram (MM) or TCH W tiles
+  constexpr uint32_t TCH = TC / kKT;       // W tiles per TMEM pass
+  constexpr int kIpt = MM / 2 * 8 / kThreads;  // tile items per thread (8K <= 4 MM)
+  const uint32_t g = blockIdx.x, K = q.K, M = q.M, Mp = q.Mp, nh = q.nh;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const uint32_t tile_bytes = MM * kKT * 2;
-  const uint32_t TC = MM == 64 ? 128 : 256;  // TMEM columns
   const uint32_t ld = K + 1;
+  const uint32_t HS = q.resident ? nh : 2;  // hi-tile slots
   // shared memory carve-up
-  uint8_t *hi_t[2] = {zsm, zsm + tile_bytes};
-  uint8_t *lo_t[2] = {zsm + 2 * tile_bytes, zsm + 3 * tile_bytes};
-  uint8_t *ximg = zsm + 4 * tile_bytes;                        // R(X): MM x MM BF16
+  uint8_t *hi_base = zsm;
+  uint8_t *lo_t[2] = {zsm + HS * tile_bytes, zsm + (HS + 1) * tile_bytes};
+  uint8_t *ximg = zsm + (HS + 2) * tile_bytes;                  // R(X): MM x MM BF16
   float2 *Gs = reinterpret_cast<float2 *>(ximg + MM * MM * 2);  // K x ld
-  float2 *Ls = Gs + K * ld;
-  float2 *Xs = Ls + K * ld;
-  // K x K temporary (leading dim K) in the lo tiles, free after the Gram
+  float2 *Xs = Gs + K * ld;                                     // K x ld
+  // Newton-Schulz temporaries (leading dim K): T in the lo tiles, the other
+  // iterate in the R(X) image; both are free between the Gram and W = X C
   float2 *Ts = reinterpret_cast<float2 *>(lo_t[0]);
+  float2 *Xn = reinterpret_cast<float2 *>(ximg);
 
   float2 *cg = q.csi + (uint64_t)g * M * K;
-  uint8_t *imgc = q.img_c + (uint64_t)g * q.nkt * tile_bytes;
   uint8_t *imgw = q.img_w + (uint64_t)g * q.nkt * tile_bytes;
 
   if (tid == 0) {
@@ -127,9 +256,10 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
     tc::mbar_init(&mma_bar, 1);
     tc::fence_mbar_init();
     fail = 0;
+    piv_bad = 0;
   }
   // rows 2K..MM-1 of the R(C) tiles are padding: zero them once
-  for (uint32_t c = tid; c < 4 * tile_bytes / 16; c += kThreads)
+  for (uint32_t c = tid; c < (HS + 2) * tile_bytes / 16; c += kThreads)
     reinterpret_cast<uint4 *>(zsm)[c] = make_uint4(0, 0, 0, 0);
   if (warp == 0) tc::tmem_alloc(&tmem_slot, TC);
   tc::fence_before_sync();
@@ -140,62 +270,75 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   uint32_t mma_phase = 0;
   bool ok = true;
 
-  // ---------------------------------------------------------------- Gram
-  const uint32_t idesc_g = tc::idesc_bf16(MM, MM, false, false);
-  for (uint32_t kt = 0; kt < q.nkt; kt++, tiles_used++) {
-    const uint32_t s = tiles_used % 2, use = tiles_used / 2;
-    if (use >= 1 && !tc::mbar_wait(&tile_bar[s], (use - 1) & 1)) ok = false;
-    if (__syncthreads_or(!ok)) break;
-    const uint32_t kk0 = kt * kKT, plane = kk0 / Mp, b0 = kk0 % Mp;
-    // item (u, 8-antenna chunk): rows 2u and 2u+1, 16 bytes each, hi and lo
-    for (uint32_t e = tid; e < 8 * K; e += kThreads) {
-      const uint32_t u = e % K, bc = e / K;
+  // Tile item e < 8K: user u = e % K and antennas 8 (e / K) .. +7 of the
+  // k tile, i.e. 16 bytes of rows 2u (Re C) and 2u+1 (Im C).
+  auto load_items = [&](uint32_t kt, float2 (&pf)[kIpt][8]) {
+#pragma unroll
+    for (int j = 0; j < kIpt; j++) {
+      const uint32_t e = tid + j * kThreads, u = e % K, b0 = kt * kKT + (e / K) * 8;
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        pf[j][i] = (e < 8 * K && b0 + i < M) ? cg[(b0 + i) * K + u] : make_float2(0.f, 0.f);
+    }
+  };
+  auto store_items = [&](const float2 (&pf)[kIpt][8], uint8_t *hi, uint8_t *lo) {
+#pragma unroll
+    for (int j = 0; j < kIpt; j++) {
+      const uint32_t e = tid + j * kThreads, u = e % K, bc = e / K;
+      if (e >= 8 * K) continue;
       uint32_t h0[4], h1[4], l0[4], l1[4];
 #pragma unroll
       for (int i = 0; i < 8; i += 2) {
-        float v0[2], v1[2];
-#pragma unroll
-        for (int t = 0; t < 2; t++) {
-          const uint32_t b = b0 + bc * 8 + i + t;
-          const float2 c = b < M ? cg[b * K + u] : make_float2(0.f, 0.f);
-          // row 2u: plane 0 -> Re, plane 1 -> -Im; row 2u+1: Im, Re
-          v0[t] = plane == 0 ? c.x : -c.y;
-          v1[t] = plane == 0 ? c.y : c.x;
-        }
-        const __nv_bfloat162 a0 = __floats2bfloat162_rn(v0[0], v0[1]);
-        const __nv_bfloat162 a1 = __floats2bfloat162_rn(v1[0], v1[1]);
+        const __nv_bfloat162 a0 = __floats2bfloat162_rn(pf[j][i].x, pf[j][i + 1].x);
+        const __nv_bfloat162 a1 = __floats2bfloat162_rn(pf[j][i].y, pf[j][i + 1].y);
         const float2 f0 = __bfloat1622float2(a0), f1 = __bfloat1622float2(a1);
-        const __nv_bfloat162 r0 = __floats2bfloat162_rn(v0[0] - f0.x, v0[1] - f0.y);
-        const __nv_bfloat162 r1 = __floats2bfloat162_rn(v1[0] - f1.x, v1[1] - f1.y);
+        const __nv_bfloat162 r0 = __floats2bfloat162_rn(pf[j][i].x - f0.x, pf[j][i + 1].x - f0.y);
+        const __nv_bfloat162 r1 = __floats2bfloat162_rn(pf[j][i].y - f1.x, pf[j][i + 1].y - f1.y);
         h0[i / 2] = *reinterpret_cast<const uint32_t *>(&a0);
         h1[i / 2] = *reinterpret_cast<const uint32_t *>(&a1);
         l0[i / 2] = *reinterpret_cast<const uint32_t *>(&r0);
         l1[i / 2] = *reinterpret_cast<const uint32_t *>(&r1);
       }
       const uint32_t o0 = img_off(2 * u, bc * 8, MM), o1 = img_off(2 * u + 1, bc * 8, MM);
-      *reinterpret_cast<uint4 *>(hi_t[s] + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
-      *reinterpret_cast<uint4 *>(hi_t[s] + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
-      *reinterpret_cast<uint4 *>(lo_t[s] + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
-      *reinterpret_cast<uint4 *>(lo_t[s] + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
-    }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc::fence_after_sync();
-      const uint32_t h0 = tc::smem_u32(hi_t[s]), l0 = tc::smem_u32(lo_t[s]);
-#pragma unroll
-      for (int ks = 0; ks < kKT / 16; ks++) {
-        const uint64_t dh = tc::smem_desc(h0 + ks * 256, 128, 1024);
-        const uint64_t dl = tc::smem_desc(l0 + ks * 256, 128, 1024);
-        tc::mma_f16(tmem, dh, dh, idesc_g, (kt | ks) != 0);
-        tc::mma_f16(tmem, dh, dl, idesc_g, 1);
-        tc::mma_f16(tmem, dl, dh, idesc_g, 1);
+      *reinterpret_cast<uint4 *>(hi + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
+      *reinterpret_cast<uint4 *>(hi + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
+      if (lo) {
+        *reinterpret_cast<uint4 *>(lo + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+        *reinterpret_cast<uint4 *>(lo + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
       }
-      tc::mma_commit(&tile_bar[s]);
     }
-    // keep the hi tile for the W product (overlaps the MMAs)
-    for (uint32_t c = tid; c < tile_bytes / 16; c += kThreads)
-      reinterpret_cast<uint4 *>(imgc + kt * tile_bytes)[c] = reinterpret_cast<const uint4 *>(hi_t[s])[c];
+  };
+
+  // ---------------------------------------------------------------- Gram
+  // A = sum over the plane-0 tiles of T T^T (hi hi + hi lo + lo hi); the
+  // next tile's CSI loads are in flight while the current one is multiplied
+  const uint32_t idesc_g = tc::idesc_bf16(MM, MM, false, false);
+  {
+    float2 pf[kIpt][8];
+    load_items(0, pf);
+    for (uint32_t kt = 0; kt < nh; kt++, tiles_used++) {
+      const uint32_t s = tiles_used % 2, use = tiles_used / 2;
+      if (use >= 1 && !tc::mbar_wait(&tile_bar[s], (use - 1) & 1)) ok = false;
+      if (__syncthreads_or(!ok)) break;
+      uint8_t *hi = hi_base + (q.resident ? kt : s) * tile_bytes;
+      store_items(pf, hi, lo_t[s]);
+      if (kt + 1 < nh) load_items(kt + 1, pf);
+      tc::fence_proxy_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        tc::fence_after_sync();
+        const uint32_t h0 = tc::smem_u32(hi), l0 = tc::smem_u32(lo_t[s]);
+#pragma unroll
+        for (int ks = 0; ks < kKT / 16; ks++) {
+          const uint64_t dh = tc::smem_desc(h0 + ks * 256, 128, 1024);
+          const uint64_t dl = tc::smem_desc(l0 + ks * 256, 128, 1024);
+          tc::mma_f16(tmem, dh, dh, idesc_g, (kt | ks) != 0);
+          tc::mma_f16(tmem, dh, dl, idesc_g, 1);
+          tc::mma_f16(tmem, dl, dh, idesc_g, 1);
+        }
+        tc::mma_commit(&tile_bar[s]);
+      }
+    }
   }
   if (ok) {
     if (tid == 0) tc::mma_commit(&mma_bar);
@@ -209,157 +352,92 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   float cond_est = INFINITY;
   int st = 0;
   if (!fail) {
-    const int rows_per_warp = MM == 64 ? 16 : 32;
+    // R(G) = A + P A P^T (plane 1 of R(C) is P times plane 0): rows 2u and
+    // 2u+1 of A sit in neighbouring TMEM lanes
     if (warp < 4) {
+      const int rows_per_warp = MM == 64 ? 16 : 32;
       const uint32_t r = warp * rows_per_warp + lane;
       for (uint32_t ch = 0; ch < MM / 16; ch++) {
-        float v[16];
+        float v[16], nb[16];
         tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + ch * 16, v);
-        if (lane < rows_per_warp && r / 2 < K) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) nb[i] = __shfl_xor_sync(0xffffffffu, v[i], 1);
+        if (lane < rows_per_warp && !(r & 1) && r / 2 < K) {
 #pragma unroll
           for (int i = 0; i < 16; i += 2) {
-            const uint32_t vcol = (ch * 16 + i) / 2;  // column 2v: Re/Im G[u][v]
-            if (vcol < K) {
-              if (r & 1)
-                Gs[(r / 2) * ld + vcol].y = v[i];
-              else
-                Gs[(r / 2) * ld + vcol].x = v[i];
-            }
+            const uint32_t vcol = (ch * 16 + i) / 2;
+            if (vcol < K) Gs[(r / 2) * ld + vcol] = make_float2(v[i] + nb[i + 1], nb[i] - v[i + 1]);
           }
         }
       }
     }
     tc::fence_before_sync();
     __syncthreads();
-    // warp 0: Cholesky G = L L^H (row-oriented, lane owns rows lane and
-    // lane+32), then T = L^{-1} (lane owns columns), no block barriers
-    if (warp == 0) {
-      bool pd = true;
-      for (uint32_t j = 0; j < K; j++) {
-        if ((j & 31) == (uint32_t)lane) {
-          // four partial sums break the dependent shared-memory chain
-          float d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
-          uint32_t k = 0;
-          for (; k + 4 <= j; k += 4) {
-            const float2 l0 = Ls[j * ld + k], l1 = Ls[j * ld + k + 1];
-            const float2 l2 = Ls[j * ld + k + 2], l3 = Ls[j * ld + k + 3];
-            d0 += l0.x * l0.x + l0.y * l0.y;
-            d1 += l1.x * l1.x + l1.y * l1.y;
-            d2 += l2.x * l2.x + l2.y * l2.y;
-            d3 += l3.x * l3.x + l3.y * l3.y;
-          }
-          for (; k < j; k++) {
-            const float2 l = Ls[j * ld + k];
-            d0 += l.x * l.x + l.y * l.y;
-          }
-          float d = Gs[j * ld + j].x - ((d0 + d1) + (d2 + d3));
-          if (!(d > 0.f)) d = -1.f;
-          Ls[j * ld + j] = make_float2(d > 0.f ? sqrtf(d) : -1.f, 0.f);
-        }
-        __syncwarp();
-        const float ljj = Ls[j * ld + j].x;
-        if (!(ljj > 0.f)) {
-          pd = false;
-          break;
-        }
-        for (uint32_t i = j + 1 + lane; i < K; i += 32) {
-          float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
-          uint32_t k = 0;
-          for (; k + 2 <= j; k += 2) {  // L_ik conj(L_jk), two chains
-            const float2 a0 = Ls[i * ld + k], b0 = Ls[j * ld + k];
-            const float2 a1 = Ls[i * ld + k + 1], b1 = Ls[j * ld + k + 1];
-            s0.x += a0.x * b0.x + a0.y * b0.y;
-            s0.y += a0.y * b0.x - a0.x * b0.y;
-            s1.x += a1.x * b1.x + a1.y * b1.y;
-            s1.y += a1.y * b1.x - a1.x * b1.y;
-          }
-          if (k < j) {
-            const float2 a0 = Ls[i * ld + k], b0 = Ls[j * ld + k];
-            s0.x += a0.x * b0.x + a0.y * b0.y;
-            s0.y += a0.y * b0.x - a0.x * b0.y;
-          }
-          const float2 gij = Gs[i * ld + j];
-          Ls[i * ld + j] = make_float2((gij.x - s0.x - s1.x) / ljj, (gij.y - s0.y - s1.y) / ljj);
-        }
-        __syncwarp();
-      }
-      if (pd) {
-        for (uint32_t c = lane; c < K; c += 32) {
-          Ts[c * K + c] = make_float2(1.f / Ls[c * ld + c].x, 0.f);
-          for (uint32_t i = c + 1; i < K; i++) {
-            float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
-            uint32_t k = c;
-            for (; k + 2 <= i; k += 2) {
-              s0 = cadd(s0, cmulf(Ls[i * ld + k], Ts[k * K + c]));
-              s1 = cadd(s1, cmulf(Ls[i * ld + k + 1], Ts[(k + 1) * K + c]));
-            }
-            if (k < i) s0 = cadd(s0, cmulf(Ls[i * ld + k], Ts[k * K + c]));
-            const float d = Ls[i * ld + i].x;
-            Ts[i * K + c] = make_float2(-(s0.x + s1.x) / d, -(s0.y + s1.y) / d);
-          }
-        }
-      }
-      if (lane == 0) flag = pd ? 0 : 1;
-    }
-    __syncthreads();
-    const bool pd = flag == 0;
+    bool pd;
+    if (MM == 64)
+      pd = K <= 16 ? gj_inverse<16>(Gs, Xs, K, ld, prow, &piv_bad)
+                   : gj_inverse<32>(Gs, Xs, K, ld, prow, &piv_bad);
+    else
+      pd = gj_inverse<64>(Gs, Xs, K, ld, prow, &piv_bad);
     if (pd) {
-      // X = T^H T (T lower triangular)
-      for (uint32_t e = tid; e < K * K; e += kThreads) {
-        const uint32_t i = e / K, j = e % K;
-        float2 s = make_float2(0.f, 0.f);
-        for (uint32_t k = i > j ? i : j; k < K; k++)
-          s = cadd(s, cmulf(cconj(Ts[k * K + i]), Ts[k * K + j]));
-        Xs[i * ld + j] = s;
-      }
-      __syncthreads();
-      // Newton-Schulz: T = 2I - G X; X = X T
+      // Newton-Schulz: T = 2I - G X; X <- X T, ping-ponging Xs and Xn
+      float2 *xc = Xs, *xn = Xn;
+      uint32_t ldc = ld, ldn = K;
       for (uint32_t it = 0; it < q.ns_iters; it++) {
-        for (uint32_t e = tid; e < K * K; e += kThreads) {
-          const uint32_t i = e / K, j = e % K;
-          float2 s = make_float2(0.f, 0.f);
-          for (uint32_t k = 0; k < K; k++) s = cadd(s, cmulf(Gs[i * ld + k], Xs[k * ld + j]));
+        cmatmul_any<MM>(Gs, ld, xc, ldc, K, [&](uint32_t i, uint32_t j, float2 s) {
           Ts[i * K + j] = make_float2((i == j ? 2.f : 0.f) - s.x, -s.y);
-        }
+        });
         __syncthreads();
-        for (uint32_t e = tid; e < K * K; e += kThreads) {
-          const uint32_t i = e / K, j = e % K;
-          float2 s = make_float2(0.f, 0.f);
-          for (uint32_t k = 0; k < K; k++) s = cadd(s, cmulf(Xs[i * ld + k], Ts[k * K + j]));
-          Ls[i * ld + j] = s;  // L is no longer needed
-        }
+        cmatmul_any<MM>(xc, ldc, Ts, K, K, [&](uint32_t i, uint32_t j, float2 s) { xn[i * ldn + j] = s; });
         __syncthreads();
-        for (uint32_t e = tid; e < K * K; e += kThreads) Xs[(e / K) * ld + e % K] = Ls[(e / K) * ld + e % K];
+        float2 *t = xc;
+        xc = xn;
+        xn = t;
+        const uint32_t l = ldc;
+        ldc = ldn;
+        ldn = l;
+      }
+      if (xc != Xs) {
+        for (uint32_t e = tid; e < K * K; e += kThreads) Xs[(e / K) * ld + e % K] = xc[e];
         __syncthreads();
       }
-      // 1-norm condition estimate ||G||_1 ||X||_1 (both Hermitian)
-      float gcol = 0.f, xcol = 0.f;
-      for (uint32_t j = tid; j < K; j += kThreads) {
+      // 1-norm condition estimate ||G||_1 ||X||_1 (both Hermitian): thread
+      // t sums column j0 + t % 32 over rows t / 32, t / 32 + 8, ...; warp 0
+      // adds the eight partial sums and takes the maximum over columns
+      float gmax = 0.f, xmax = 0.f;
+      for (uint32_t j0 = 0; j0 < K; j0 += 32) {
+        const uint32_t j = j0 + lane;
         float sg = 0.f, sx = 0.f;
-        for (uint32_t i = 0; i < K; i++) {
-          const float2 gv = Gs[i * ld + j], xv = Xs[i * ld + j];
-          sg += sqrtf(gv.x * gv.x + gv.y * gv.y);
-          sx += sqrtf(xv.x * xv.x + xv.y * xv.y);
+        if (j < K)
+          for (uint32_t i = warp; i < K; i += kThreads / 32) {
+            const float2 gv = Gs[i * ld + j], xv = Xs[i * ld + j];
+            sg += sqrtf(gv.x * gv.x + gv.y * gv.y);
+            sx += sqrtf(xv.x * xv.x + xv.y * xv.y);
+          }
+        red[tid] = sg;
+        red2[tid] = sx;
+        __syncthreads();
+        if (warp == 0) {
+          float a = 0.f, c = 0.f;
+          for (uint32_t w = 0; w < kThreads / 32; w++) {
+            a += red[w * 32 + lane];
+            c += red2[w * 32 + lane];
+          }
+          for (int o = 16; o > 0; o >>= 1) {
+            a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+            c = fmaxf(c, __shfl_xor_sync(0xffffffffu, c, o));
+          }
+          if (lane == 0) {
+            red[0] = a;
+            red2[0] = c;
+          }
         }
-        gcol = fmaxf(gcol, sg);
-        xcol = fmaxf(xcol, sx);
-      }
-      red[tid] = gcol;
-      __syncthreads();
-      for (int o = kThreads / 2; o > 0; o >>= 1) {
-        if (tid < o) red[tid] = fmaxf(red[tid], red[tid + o]);
+        __syncthreads();
+        gmax = fmaxf(gmax, red[0]);
+        xmax = fmaxf(xmax, red2[0]);
         __syncthreads();
       }
-      const float gn = red[0];
-      __syncthreads();
-      red[tid] = xcol;
-      __syncthreads();
-      for (int o = kThreads / 2; o > 0; o >>= 1) {
-        if (tid < o) red[tid] = fmaxf(red[tid], red[tid + o]);
-        __syncthreads();
-      }
-      cond_est = gn * red[0];
-      __syncthreads();
+      cond_est = gmax * xmax;
       if (!(cond_est <= q.cond_thr)) st = 2;
     } else {
       st = 2;
@@ -367,6 +445,8 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   }
 
   // ----------------------------------------------------- W = X C (tensor)
+  // D0 = R(X) T0 over the plane-0 tiles; plane 1 of the detector image is
+  // P D0 (R(X) commutes with P), so it needs no multiply of its own
   if (!fail && st == 0) {
     // R(X) image, K-major over the reduction index 2v + rj; rows/columns
     // beyond 2K are padding and stay zero
@@ -381,22 +461,32 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
     }
     tc::fence_proxy_async_smem();
     __syncthreads();
-    const uint32_t tiles_per_chunk = TC / kKT;
     const uint32_t idesc_w = tc::idesc_bf16(MM, kKT, false, true);
-    for (uint32_t kt0 = 0; kt0 < q.nkt && ok; kt0 += tiles_per_chunk) {
-      const uint32_t nt = min(tiles_per_chunk, q.nkt - kt0);
-      for (uint32_t t = 0; t < nt; t++, tiles_used++) {
-        const uint32_t s = tiles_used % 2, use = tiles_used / 2;
-        if (use >= 1 && !tc::mbar_wait(&tile_bar[s], (use - 1) & 1)) ok = false;
-        if (__syncthreads_or(!ok)) break;
-        for (uint32_t c = tid; c < tile_bytes / 16; c += kThreads)
-          reinterpret_cast<uint4 *>(hi_t[s])[c] =
-              reinterpret_cast<const uint4 *>(imgc + (kt0 + t) * tile_bytes)[c];
-        tc::fence_proxy_async_smem();
-        __syncthreads();
+    for (uint32_t kt0 = 0; kt0 < nh && ok; kt0 += TCH) {
+      const uint32_t nt = min(TCH, nh - kt0);
+      for (uint32_t t = 0; t < nt; t++) {
+        uint8_t *hi;
+        uint32_t s = 0;
+        if (q.resident) {
+          hi = hi_base + (kt0 + t) * tile_bytes;
+        } else {
+          // rebuild the hi tile from the CSI (not yet overwritten: W rows
+          // of a tile are stored only after all of its pass is multiplied)
+          s = tiles_used % 2;
+          const uint32_t use = tiles_used / 2;
+          tiles_used++;
+          if (use >= 1 && !tc::mbar_wait(&tile_bar[s], (use - 1) & 1)) ok = false;
+          if (__syncthreads_or(!ok)) break;
+          hi = hi_base + s * tile_bytes;
+          float2 pf[kIpt][8];
+          load_items(kt0 + t, pf);
+          store_items(pf, hi, nullptr);
+          tc::fence_proxy_async_smem();
+          __syncthreads();
+        }
         if (tid == 0) {
           tc::fence_after_sync();
-          const uint32_t xa = tc::smem_u32(ximg), cb = tc::smem_u32(hi_t[s]);
+          const uint32_t xa = tc::smem_u32(ximg), cb = tc::smem_u32(hi);
 #pragma unroll
           for (int ks = 0; ks < MM / 16; ks++) {
             // A = R(X): k tile ks/4, k chunk pair ks%4
@@ -406,7 +496,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
             const uint64_t bd = tc::smem_desc(cb + ks * 2 * 1024, 1024, 128);
             tc::mma_f16(tmem + t * kKT, ad, bd, idesc_w, ks != 0);
           }
-          tc::mma_commit(&tile_bar[s]);
+          if (!q.resident) tc::mma_commit(&tile_bar[s]);
         }
       }
       if (!ok) break;
@@ -416,33 +506,37 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
       if (__syncthreads_or(!ok)) break;
       tc::fence_after_sync();
       // epilogue: warp w reads lanes of quadrant w % 4, column chunks
-      // w / 4, w / 4 + 2, ...; row r, column = reduction index kk
+      // w / 4, w / 4 + 2, ...; row r, column = antenna b of plane 0
       const int rows_per_warp = MM == 64 ? 16 : 32;
       const uint32_t quad = warp % 4;
       const uint32_t r = quad * rows_per_warp + lane;
       const uint32_t u = r / 2;
+      const float sgn = (r & 1) ? 1.f : -1.f;  // plane 1: row 2u = -D0[2u+1], row 2u+1 = D0[2u]
       for (uint32_t ch = warp / 4; ch < nt * kKT / 16; ch += kThreads / 128) {
-        float v[16];
+        float v[16], nb[16];
         tc::tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + ch * 16, v);
+#pragma unroll
+        for (int i = 0; i < 16; i++) nb[i] = __shfl_xor_sync(0xffffffffu, v[i], 1);
         if (lane >= rows_per_warp) continue;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const uint32_t kk = kt0 * kKT + ch * 16 + h * 8;
-          uint4 pk;
-          __nv_bfloat162 b01 = __floats2bfloat162_rn(v[h * 8 + 0], v[h * 8 + 1]);
-          __nv_bfloat162 b23 = __floats2bfloat162_rn(v[h * 8 + 2], v[h * 8 + 3]);
-          __nv_bfloat162 b45 = __floats2bfloat162_rn(v[h * 8 + 4], v[h * 8 + 5]);
-          __nv_bfloat162 b67 = __floats2bfloat162_rn(v[h * 8 + 6], v[h * 8 + 7]);
-          pk.x = *reinterpret_cast<uint32_t *>(&b01);
-          pk.y = *reinterpret_cast<uint32_t *>(&b23);
-          pk.z = *reinterpret_cast<uint32_t *>(&b45);
-          pk.w = *reinterpret_cast<uint32_t *>(&b67);
-          *reinterpret_cast<uint4 *>(imgw + img_off(r, kk, MM)) = pk;
-          if (u < K && kk < Mp) {
+          uint32_t p0[4], p1[4];
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const __nv_bfloat162 a = __floats2bfloat162_rn(v[h * 8 + 2 * e], v[h * 8 + 2 * e + 1]);
+            const __nv_bfloat162 c =
+                __floats2bfloat162_rn(sgn * nb[h * 8 + 2 * e], sgn * nb[h * 8 + 2 * e + 1]);
+            p0[e] = *reinterpret_cast<const uint32_t *>(&a);
+            p1[e] = *reinterpret_cast<const uint32_t *>(&c);
+          }
+          *reinterpret_cast<uint4 *>(imgw + img_off(r, kk, MM)) = make_uint4(p0[0], p0[1], p0[2], p0[3]);
+          *reinterpret_cast<uint4 *>(imgw + img_off(r, Mp + kk, MM)) = make_uint4(p1[0], p1[1], p1[2], p1[3]);
+          if (!(r & 1) && u < K) {
 #pragma unroll
             for (int e = 0; e < 8; e++) {
               const uint32_t b = kk + e;
-              if (b < M) reinterpret_cast<float *>(cg + b * K + u)[r & 1] = v[h * 8 + e];
+              if (b < M) cg[b * K + u] = make_float2(v[h * 8 + e], nb[h * 8 + e]);
             }
           }
         }
@@ -456,7 +550,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   // ------------------------------------------------- FP64 fallback groups
   if (!fail && st == 2) {
     using D2 = double2;
-    D2 *Gd = reinterpret_cast<D2 *>(Gs);  // reuses Gs and Ls (2 K*ld float2)
+    D2 *Gd = reinterpret_cast<D2 *>(Gs);  // reuses Gs and Xs (2 K*ld float2)
     const uint32_t ldd = K + 1;
     for (uint32_t e = tid; e < K * K; e += kThreads) {
       const uint32_t i = e / K, j = e % K;
@@ -520,19 +614,18 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   if (warp == 0) tc::tmem_dealloc(tmem, TC);
 }
 
-static size_t zfm_smem(uint32_t K, uint32_t MM) {
+static size_t zfm_smem(uint32_t K, uint32_t MM, uint32_t hi_slots) {
   const size_t tile = (size_t)MM * kKT * 2;
-  return 4 * tile + (size_t)MM * MM * 2 + 3 * (size_t)K * (K + 1) * sizeof(float2);
+  return (hi_slots + 2) * tile + (size_t)MM * MM * 2 + 2 * (size_t)K * (K + 1) * sizeof(float2);
 }
 
 uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K) {
   const TcShape s = tc_shape(M, K);
-  return (uint64_t)groups * s.img_group_bytes;  // one of img_w / img_c
+  return (uint64_t)groups * s.img_group_bytes;
 }
 
-mb_status zf_mixed_run(float2 *csi, void *img_w, void *img_c, uint32_t groups, uint32_t M,
-                       uint32_t K, const mb_zf_opts *opts, int32_t *status, float *cond,
-                       cudaStream_t st) {
+mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
+                       const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st) {
   if (K == 0 || K > 64) return MB_UNSUPPORTED;
   const TcShape s = tc_shape(M, K);
   const DeviceTables *tab = device_tables();
@@ -540,7 +633,6 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, void *img_c, uint32_t groups, u
   ZfmParams q;
   q.csi = csi;
   q.img_w = reinterpret_cast<uint8_t *>(img_w);
-  q.img_c = reinterpret_cast<uint8_t *>(img_c);
   q.status = status;
   q.cond = cond;
   q.err = tab->err;
@@ -548,13 +640,14 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, void *img_c, uint32_t groups, u
   q.K = K;
   q.Mp = s.Mp;
   q.nkt = s.nkt;
+  q.nh = s.Mp / kKT;
   q.ns_iters = opts ? opts->ns_iters : 2;
   q.cond_thr = opts && opts->cond_threshold > 0 ? opts->cond_threshold : 1e4f;
-  const size_t smem = zfm_smem(K, s.MM);
   int dev = 0, maxs = 0;
   MB_CUDA_TRY(cudaGetDevice(&dev));
   MB_CUDA_TRY(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   static std::atomic<uint64_t> configured[2] = {{0}, {0}};
+  static std::atomic<int> static_smem[2] = {{0}, {0}};
   const int which = s.MM == 64 ? 0 : 1;
   const uint64_t bit = 1ull << (dev & 63);
   if (!(configured[which].load() & bit)) {
@@ -568,9 +661,14 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, void *img_c, uint32_t groups, u
       MB_CUDA_TRY(cudaFuncSetAttribute(zf_mixed_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        maxs - (int)fa.sharedSizeBytes));
     }
+    static_smem[which] = (int)fa.sharedSizeBytes;
     configured[which].fetch_or(bit);
   }
-  if (smem + 2048 > (size_t)maxs) return MB_UNSUPPORTED;
+  const size_t avail = (size_t)maxs - (size_t)static_smem[which].load();
+  // keep every hi tile in shared memory when it fits, else stream two
+  q.resident = zfm_smem(K, s.MM, q.nh) <= avail ? 1 : 0;
+  const size_t smem = zfm_smem(K, s.MM, q.resident ? q.nh : 2);
+  if (smem > avail) return MB_UNSUPPORTED;
   if (groups == 0) return MB_OK;
   if (s.MM == 64)
     zf_mixed_kernel<64><<<groups, kThreads, smem, st>>>(q);

@@ -57,10 +57,12 @@ def test_equalize_tc_vs_oracle(mb, K, M, S, sg, n_sym, Qm):
         assert (bits_g[sure] == bits_r[sure]).all()
 
 
-@pytest.mark.parametrize("M,K,G", [(256, 32, 7), (64, 16, 5), (128, 64, 3), (200, 24, 4), (8, 4, 2)])
+@pytest.mark.parametrize("M,K,G", [(256, 32, 7), (64, 16, 5), (128, 64, 3), (200, 24, 4), (8, 4, 2),
+                                   (256, 64, 2), (384, 64, 3)])
 def test_zf_mixed_vs_oracle(mb, M, K, G):
     # split-BF16 Gram on tensor cores + FP32 inverse + 2 Newton-Schulz steps;
-    # W via tensor cores: within 1% of max|W| of the FP64 oracle
+    # W via tensor cores: within 1% of max|W| of the FP64 oracle.  384x64
+    # does not fit its antenna tiles in shared memory and streams them.
     rng = np.random.default_rng(M + K)
     csi = ((rng.standard_normal((G, M, K)) + 1j * rng.standard_normal((G, M, K))) / np.sqrt(2)).astype(np.complex64)
     d = dev(csi)
@@ -105,6 +107,8 @@ CASES = [
     dict(M=128, K=32, N=1024, S=600, sg=16, Qm=6, U=4, snr_db=28.0, seed=12, channel="tdl", rho=0.5,
          n_taps=4, tap_decay=1.0),
     dict(M=32, K=8, N=256, S=200, sg=8, Qm=2, U=3, snr_db=12.0, seed=13, iq_dtype="int16"),
+    # antenna tiles streamed through shared memory in the mixed ZF
+    dict(M=384, K=64, N=512, S=300, sg=16, Qm=4, U=3, snr_db=30.0, seed=14),
 ]
 
 
