@@ -42,10 +42,11 @@ namespace {
 constexpr int kStages = 3;
 constexpr int kKT = 64;     // reduction elements per k tile (4 MMAs of K=16)
 constexpr int kCols = 128;  // MMA M: (symbol, subcarrier) columns per CTA
+constexpr int kEqThreads = 256;  // 8 warps: warps w and w + 4 read TMEM lane quadrant w
 }  // namespace
 
 template <int MM, int QM>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kEqThreads, 1)
     equalize_tc_kernel(const EqTcParams q, const __grid_constant__ CUtensorMap ymap) {
   extern __shared__ __align__(1024) uint8_t eq_smem[];
   __shared__ __align__(8) uint64_t full_bar[kStages];
@@ -137,8 +138,10 @@ __global__ void __launch_bounds__(128, 1)
     if (tid == 0 && q.err) atomicOr(q.err, tc::kErrTimeout);
   } else {
     tc::fence_after_sync();
-    // thread = D row = TMEM lane 32 warp + lane = column (symbol l, subcarrier sl)
-    const uint32_t c = warp * 32 + lane;
+    // thread = D row = TMEM lane 32 (warp % 4) + lane = column (symbol l,
+    // subcarrier sl); warps w and w + 4 take alternate chunks of 8 users
+    const uint32_t quad = warp % 4;
+    const uint32_t c = quad * 32 + lane;
     const uint32_t l = c / p.sg, sl = c % p.sg;
     const uint32_t s = s_base + sl;
     const bool valid = c < ncols && s < p.S;
@@ -151,7 +154,6 @@ __global__ void __launch_bounds__(128, 1)
     const bool llr_on = valid && cb < p.cb_blocks;
     const bool pair = base + QM <= p.row_len32 && ((p.row_len32 | base) & 1) == 0 &&
                       (reinterpret_cast<uintptr_t>(p.llr) & 3) == 0;
-    __half *lpu = reinterpret_cast<__half *>(p.llr) + (uint64_t)lg * p.K * p.row_len + base;
     // hard bits: stream positions < n_valid only, first bit most significant
     uint32_t nvm = 0;
 #pragma unroll
@@ -159,22 +161,29 @@ __global__ void __launch_bounds__(128, 1)
       if (t0 + qb < p.n_valid32) nvm |= 1u << (QM - 1 - qb);
     if (!valid) nvm = 0;
     // 8-lane groups hold 8 consecutive subcarriers of one symbol (sg % 8 ==
-    // 0); after the OR-reduction lane gl of a group writes byte gl of the
-    // group's QM bytes (a group cut short by S pads its last byte with zeros)
+    // 0), i.e. QM whole bytes of the hard-bit row.  Lane gl < QM writes byte
+    // gl; its 8 bits come from the NSUB subcarriers from sa on, fetched with
+    // independent shuffles (a group cut short by S pads with zeros).
+    constexpr uint32_t NSUB = QM == 6 ? 2 : 8 / QM;
     const uint32_t gl = lane & 7;
+    const uint32_t sa = gl < (uint32_t)QM ? 8 * gl / QM : 0;
+    const uint32_t boff = 8 * gl - QM * sa;  // first bit of the byte within sa's bits
     const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
     const uint32_t nvalid = __popc((vmask >> (lane & ~7u)) & 0xFFu);
     const uint32_t gb = (s - gl) * QM / 8 + gl;
     const bool byte_on = p.hard && gl < (nvalid * QM + 7) / 8 && gb * 8 < p.n_valid32;
     const uint32_t end = p.n_valid32 - gb * 8;
     const uint8_t seq_mask = byte_on && end < 8 ? (uint8_t)(0xFF00u >> end) : (uint8_t)0xFF;
-    uint8_t *hpu = p.hard ? p.hard + (uint64_t)lg * p.K * p.hrow + gb : nullptr;
-    const uint8_t *spu = p.seqb ? p.seqb + gb : nullptr;
-    float2 *xpu = p.x ? p.x + (uint64_t)lg * p.K * p.S + s : nullptr;
     const __half zero = __float2half_rn(0.f);
-    for (uint32_t ch = 0; ch < q.N / 16; ch++) {
+    const uint32_t nch = q.N / 16;
+    for (uint32_t ch = warp / 4; ch < nch; ch += kEqThreads / 128) {
       float v[16];
-      tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + ch * 16, v);
+      tc::tmem_ld16(tmem + (quad * 32 << 16) + ch * 16, v);
+      const uint64_t row = (uint64_t)lg * p.K + ch * 8;  // (symbol, first user of the chunk)
+      __half *lpu = reinterpret_cast<__half *>(p.llr) + row * p.row_len + base;
+      uint8_t *hpu = p.hard ? p.hard + row * p.hrow + gb : nullptr;
+      const uint8_t *spu = p.seqb ? p.seqb + (uint64_t)(ch * 8) * p.seq_row_bytes + gb : nullptr;
+      float2 *xpu = p.x ? p.x + row * p.S + s : nullptr;
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         if (ch * 8 + j >= p.K) break;
@@ -196,12 +205,13 @@ __global__ void __launch_bounds__(128, 1)
           uint32_t hb = 0;
 #pragma unroll
           for (int qb = 0; qb < QM; qb++) hb = (hb << 1) | (__hlt(lv[qb], zero) ? 1u : 0u);
-          uint64_t w = (uint64_t)(hb & nvm) << (64 - QM * (gl + 1));
-          w |= __shfl_xor_sync(0xffffffffu, w, 1);
-          w |= __shfl_xor_sync(0xffffffffu, w, 2);
-          w |= __shfl_xor_sync(0xffffffffu, w, 4);
+          hb &= nvm;
+          uint32_t win = 0;
+#pragma unroll
+          for (uint32_t k = 0; k < NSUB; k++)
+            win = (win << QM) | __shfl_sync(0xffffffffu, hb, (lane & ~7) + sa + k);
           if (byte_on) {
-            uint8_t bt = (uint8_t)(w >> (56 - 8 * gl));
+            uint8_t bt = (uint8_t)(win >> (NSUB * QM - boff - 8));
             if (spu) bt ^= __ldg(spu) & seq_mask;
             *hpu = bt;
           }
@@ -333,7 +343,7 @@ mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, ui
   mb_status tr = make_tmap_2d_bf16(&ymap, y_lp, S_pad, (uint64_t)nb * 2 * p.M, S_pad, 8, kKT);
   if (tr != MB_OK) return tr;
   const dim3 grid(G, ny);
-  (s.MM == 64 ? eq_tc_kernel_of<64>(p.Qm) : eq_tc_kernel_of<128>(p.Qm))<<<grid, 128, smem, st>>>(q, ymap);
+  (s.MM == 64 ? eq_tc_kernel_of<64>(p.Qm) : eq_tc_kernel_of<128>(p.Qm))<<<grid, kEqThreads, smem, st>>>(q, ymap);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }
