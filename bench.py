@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed"])
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 path")
     ap.add_argument("--no-evm", action="store_true")
-    ap.add_argument("--sym-batch", type=int, default=4)
+    ap.add_argument("--sym-batch", type=int, default=12)
     ap.add_argument("--rotate", type=int, default=4, help="distinct input slots cycled (L2 flush)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -118,6 +118,80 @@ def measured_peaks():
             d = json.load(f)
         return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
     return 6650.0, 1590.0, "fallback"
+
+
+def profile_traffic(name, unit_name, units):
+    """DRAM bytes per launch from the committed ncu summary profiles/<name>.md
+    (its line "dram bytes per <unit_name>: B", scaled by the units of one
+    launch), or None when the summary is absent."""
+    import re
+    path = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        m = re.search(r"dram bytes per " + re.escape(unit_name) + r": *([0-9.eE+]+)", f.read())
+    return float(m.group(1)) * units if m else None
+
+
+def roofline(cfg, args, st, n_valid, hrow):
+    """Per-kernel times alone (CUDA events, timing mode) and the roofline of
+    the kernel with the largest share of the slot."""
+    hbm_peak, tc_peak, peak_kind = measured_peaks()
+    calls = max(st["calls"], 1)
+    mixed = args.precision == "mixed"
+    n_fft = max(st["n_fft"], 1)                        # launches over all recorded slots
+    n_eq = max(st["n_eq"], 1)
+    rows = cfg.U * cfg.M * calls / n_fft               # antenna rows per uplink FFT launch
+    syms = cfg.U * calls / n_eq                        # symbols per equalize launch
+    out_b = 4 if mixed else 8                          # BF16 planar or c32 per subcarrier
+    tc = {"MM": 64 if 2 * cfg.K <= 64 else 128, "Mp": (cfg.M + 63) // 64 * 64}
+    img_group = 2 * tc["Mp"] * tc["MM"] * 2
+    k = {
+        "fft_uplink": {"ms": st["uplink_fft"] / n_fft, "per_slot_ms": st["uplink_fft"] / calls,
+                       "bound": "hbm", "units": rows, "unit_name": "antenna row",
+                       "bytes": rows * (cfg.N * 8 + cfg.S * out_b)},
+        "fft_pilot": {"ms": st["pilot_fft"] / calls, "per_slot_ms": st["pilot_fft"] / calls,
+                      "bound": "hbm", "units": cfg.P * cfg.M, "unit_name": "pilot row",
+                      "bytes": cfg.P * cfg.M * (cfg.N * 8) + cfg.G * cfg.M * cfg.K * 8},
+        "zf": {"ms": st["zf"] / calls, "per_slot_ms": st["zf"] / calls, "bound": "tensor",
+               "units": cfg.G, "unit_name": "subcarrier group",
+               "flops": cfg.G * (16.0 * cfg.K ** 2 * cfg.M + 40.0 * cfg.K ** 3)},
+        "equalize": {"ms": st["equalize"] / n_eq, "per_slot_ms": st["equalize"] / calls,
+                     "bound": "hbm", "units": syms, "unit_name": "symbol",
+                     "bytes": (cfg.G * img_group if mixed else cfg.G * cfg.M * cfg.K * 8)
+                     + syms * (cfg.M * cfg.S * out_b + cfg.K * (n_valid * 2 + hrow))},
+    }
+    names = {"fft_uplink": "fft_kernel<12, uplink LP>" if mixed else "fft_kernel<12, uplink>",
+             "fft_pilot": "fft_kernel<12, pilot>",
+             "zf": "zf_mixed_kernel<64>" if mixed else "zf_chol_kernel<float>",
+             "equalize": "equalize_tc_kernel<64, 6>" if mixed else "equalize_fp32_kernel"}
+    profiles = {"fft_uplink": "fft_uplink_lp_4096x256", "equalize": "equalize_tc_256x32",
+                "zf": "zf_mixed_256x32", "fft_pilot": "fft_uplink_lp_4096x256"}
+    for key, v in k.items():
+        sec = v["ms"] / 1e3
+        if v["bound"] == "hbm":
+            v["achieved"] = v["bytes"] / sec / 1e9 if sec > 0 else 0.0
+            v["frac"] = v["achieved"] / hbm_peak
+        else:
+            v["achieved"] = v["flops"] / sec / 1e12 if sec > 0 else 0.0
+            v["frac"] = v["achieved"] / tc_peak
+    dom = max(k, key=lambda x: k[x]["per_slot_ms"])
+    v = k[dom]
+    hbm = v["bound"] == "hbm"
+    traffic = profile_traffic(profiles[dom], v["unit_name"], v["units"]) if mixed else None
+    roof = {"kernel": names[dom], "bound": v["bound"], "achieved": v["achieved"],
+            "peak": hbm_peak if hbm else tc_peak, "unit": "GB/s" if hbm else "TFLOP/s",
+            "frac": v["frac"], "traffic": traffic,
+            "algorithmic": (f"{v['bytes'] / v['units']:.0f} bytes per {v['unit_name']} x {v['units']:.0f}"
+                            if hbm else f"{v['flops'] / v['units']:.0f} flops per {v['unit_name']} x "
+                                        f"{v['units']:.0f}"),
+            "ms_per_launch": v["ms"],
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback",
+            "per_kernel": {names[x]: {"ms_per_launch": k[x]["ms"], "ms_per_slot": k[x]["per_slot_ms"],
+                                      "bound": k[x]["bound"], "achieved": k[x]["achieved"],
+                                      "frac": k[x]["frac"]} for x in k},
+            "serial_slot_ms": st["slot"] / calls}
+    return roof
 
 
 def cpu_baseline(cfg, slot_np, seconds):
@@ -310,7 +384,9 @@ def main():
     evm = None if args.no_evm or rank != 0 else evm_report(cfg, d, args.sym_batch)
     launches_per_slot = 2 + (1 if cfg.S % cfg.sg else 0) + 2 * ((cfg.U + args.sym_batch - 1) // args.sym_batch)
 
-    # ---- roofline pass: same slots with per-stage CUDA events (direct launches)
+    # ---- roofline pass: the same slots with every kernel alone on the slot
+    # stream (timing mode serialises the side-stream FFT) and CUDA events at
+    # the stage boundaries
     run_t = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=False)
     with torch.cuda.stream(stream):
         for k in range(3):
@@ -320,39 +396,9 @@ def main():
         for k in range(args.steps):
             run_t(iq_dev[k % R], llr[k % 2], hard[k % 2], stream=stream)
     stream.synchronize()
-    st = run_t.stage_ms()
-    hbm_peak, tc_peak, peak_kind = measured_peaks()
-    sb = args.sym_batch
-    fft_bytes = sb * cfg.M * (cfg.N * 8 + cfg.S * 8)   # samples in, y out
-    fft_ms = st["uplink_fft"] / max(st["n_fft"], 1)
-    eq_ms = st["equalize"] / max(st["n_eq"], 1)
-    eq_bytes = cfg.G * cfg.M * cfg.K * 8 + sb * cfg.M * cfg.S * 8 + sb * cfg.K * (n_valid * 2 + hrow)
-    eq_flops = 8.0 * cfg.K * cfg.M * cfg.S * sb
-    stages = {k: st[k] / max(st["calls"], 1) for k in ("pilot_fft", "zf", "uplink_fft", "equalize", "slot")}
-    # the dominant kernel by share of the slot
-    per_slot_fft = st["uplink_fft"] / max(st["calls"], 1) * (cfg.U / sb) / max((cfg.U / sb - 1), 1)
-    per_slot_eq = stages["equalize"]
-    if per_slot_eq >= per_slot_fft and args.precision == "mixed":
-        ach = eq_flops / (eq_ms / 1e3) / 1e12
-        roof = {"kernel": "equalize (tensor cores)", "bound": "tensor", "achieved": ach, "peak": tc_peak,
-                "unit": "TFLOP/s", "frac": ach / tc_peak, "traffic": None}
-    elif per_slot_eq >= per_slot_fft:
-        ach = eq_bytes / (eq_ms / 1e3) / 1e9
-        roof = {"kernel": "equalize_fp32_kernel", "bound": "hbm", "achieved": ach, "peak": hbm_peak,
-                "unit": "GB/s", "frac": ach / hbm_peak, "traffic": None,
-                "flops_tflops": eq_flops / (eq_ms / 1e3) / 1e12}
-    else:
-        ach = fft_bytes / (fft_ms / 1e3) / 1e9 if fft_ms > 0 else 0.0
-        roof = {"kernel": "fft_kernel<12, uplink>", "bound": "hbm", "achieved": ach, "peak": hbm_peak,
-                "unit": "GB/s", "frac": ach / hbm_peak, "traffic": None}
-    roof["peak_source"] = f"{peak_kind} (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback"
-    roof["stage_ms_per_slot"] = stages
-    roof["uplink_fft"] = {"ms_per_launch": fft_ms, "bytes_per_launch": fft_bytes,
-                          "GB_s": fft_bytes / (fft_ms / 1e3) / 1e9 if fft_ms > 0 else None,
-                          "note": "launches on the slot stream only (the first batch overlaps ZF on a side stream)"}
-    roof["equalize"] = {"ms_per_launch": eq_ms, "bytes_per_launch": eq_bytes,
-                        "GB_s": eq_bytes / (eq_ms / 1e3) / 1e9, "TFLOP_s": eq_flops / (eq_ms / 1e3) / 1e12}
+    roof = roofline(cfg, args, run_t.stage_ms(), n_valid, hrow)
     slot_bytes = algorithmic_bytes(cfg)
+    hbm_peak = measured_peaks()[0]
     roof["slot"] = {"bytes": slot_bytes, "GB_s": slot_bytes * value / world / 1e9,
                     "frac_of_hbm": slot_bytes * value / world / 1e9 / hbm_peak}
 

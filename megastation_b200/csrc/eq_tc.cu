@@ -184,6 +184,12 @@ __global__ void __launch_bounds__(kEqThreads, 1)
       uint8_t *hpu = p.hard ? p.hard + row * p.hrow + gb : nullptr;
       const uint8_t *spu = p.seqb ? p.seqb + (uint64_t)(ch * 8) * p.seq_row_bytes + gb : nullptr;
       float2 *xpu = p.x ? p.x + row * p.S + s : nullptr;
+      // the chunk's descrambling bytes, loaded together ahead of use
+      uint8_t sq[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        sq[j] = (spu && byte_on && ch * 8 + j < p.K) ? (uint8_t)(__ldg(spu + j * p.seq_row_bytes) & seq_mask)
+                                                     : (uint8_t)0;
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         if (ch * 8 + j >= p.K) break;
@@ -210,13 +216,8 @@ __global__ void __launch_bounds__(kEqThreads, 1)
 #pragma unroll
           for (uint32_t k = 0; k < NSUB; k++)
             win = (win << QM) | __shfl_sync(0xffffffffu, hb, (lane & ~7) + sa + k);
-          if (byte_on) {
-            uint8_t bt = (uint8_t)(win >> (NSUB * QM - boff - 8));
-            if (spu) bt ^= __ldg(spu) & seq_mask;
-            *hpu = bt;
-          }
+          if (byte_on) *hpu = (uint8_t)(win >> (NSUB * QM - boff - 8)) ^ sq[j];
           hpu += p.hrow;
-          if (spu) spu += p.seq_row_bytes;
         }
         if (xpu) {
           if (valid) *xpu = x;

@@ -16,7 +16,8 @@
 // owns 16 complex values; a row of N points uses N/16 threads, and a CTA
 // holds max(1, 256/(N/16)) rows.  Twiddles come from per-device tables
 // computed in double at init and laid out per pass as [r][k], so a warp's
-// twiddle loads are coalesced.
+// twiddle loads are coalesced; a radix-16 pass loads the entries of r = 1
+// and 4 and forms the other powers by at most three complex products.
 #include <cuda_bf16.h>
 
 #include <atomic>
@@ -304,14 +305,38 @@ __global__ void __launch_bounds__(Plan<LOGN>::THREADS, Plan<LOGN>::MIN_BLOCKS)
         v[bi] = sm[pad(j + r * (N / R))];
       }
       __syncthreads();  // every thread has read before anyone overwrites
+      if (R == 16) {
+        // W^(r jm), r = 1..15, from the exact table entries of r = 1 and 4
+        // (at most three products from an exact entry): two loads instead
+        // of fifteen
+        const int jm = t % Ns;
+        float2 w[16];
+        w[1] = __ldg(p.tw + PL::tw_off(pass) + Ns + jm);
+        w[4] = __ldg(p.tw + PL::tw_off(pass) + 4 * Ns + jm);
+        if (INV) {
+          w[1].y = -w[1].y;
+          w[4].y = -w[4].y;
+        }
+        w[2] = cmul(w[1], w[1]);
+        w[3] = cmul(w[2], w[1]);
+        w[5] = cmul(w[4], w[1]);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+        w[8] = cmul(w[4], w[4]);
 #pragma unroll
-      for (int bi = 0; bi < 16; bi++) {
-        const int j = t + (bi / R) * T, r = bi % R;
-        if (r) {
-          const int m = PL::tw_off(pass) + r * Ns + (j % Ns);
-          float2 w = __ldg(p.tw + m);
-          if (INV) w.y = -w.y;
-          v[bi] = cmul(v[bi], w);
+        for (int r = 9; r < 16; r++) w[r] = cmul(w[8], w[r - 8]);
+#pragma unroll
+        for (int r = 1; r < 16; r++) v[r] = cmul(v[r], w[r]);
+      } else {
+#pragma unroll
+        for (int bi = 0; bi < 16; bi++) {
+          const int j = t + (bi / R) * T, r = bi % R;
+          if (r) {
+            const int m = PL::tw_off(pass) + r * Ns + (j % Ns);
+            float2 w = __ldg(p.tw + m);
+            if (INV) w.y = -w.y;
+            v[bi] = cmul(v[bi], w);
+          }
         }
       }
     }

@@ -48,8 +48,10 @@ struct mb_slot {
   std::vector<GraphEntry> graphs;
   uint64_t graph_clock = 0;
   // stage timing: per recorded call, events at stage boundaries
+  // With timing on, every kernel runs on the slot stream in turn (no side
+  // stream), so each stage time is that kernel's time alone.
   struct Marks {
-    cudaEvent_t start, pilot, zf, end;
+    cudaEvent_t start, pilot_b, pilot, zf, end;
     std::vector<cudaEvent_t> fft_b, fft_e, eq_b, eq_e;
   };
   std::vector<Marks> marks;
@@ -71,6 +73,7 @@ static mb_slot::Marks *next_marks(mb_slot *s) {
   if (s->marks.size() <= s->marks_used) {
     mb_slot::Marks m;
     m.start = new_event();
+    m.pilot_b = new_event();
     m.pilot = new_event();
     m.zf = new_event();
     m.end = new_event();
@@ -89,6 +92,7 @@ static mb_slot::Marks *next_marks(mb_slot *s) {
 static void free_marks(mb_slot *s) {
   for (auto &m : s->marks) {
     cudaEventDestroy(m.start);
+    cudaEventDestroy(m.pilot_b);
     cudaEventDestroy(m.pilot);
     cudaEventDestroy(m.zf);
     cudaEventDestroy(m.end);
@@ -205,9 +209,15 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     return mixed ? fft_uplink_lp(s->fft, src, c.iq_dtype, nb, s->y_lp, s->S_pad, fs)
                  : mb_fft_uplink(s->fft, src, c.iq_dtype, nb, reinterpret_cast<mb_c32 *>(s->y), fs);
   };
-  // fork: the first uplink FFT batch only needs the samples
+  // fork: the first uplink FFT batch only needs the samples (serialised
+  // and timed on the slot stream when timing is on)
   const uint32_t nb0 = std::min(c.sym_batch, c.U);
-  if (c.U) {
+  if (c.U && mk) {
+    MARK(mk->fft_b[0]);
+    r = fft_batch(0, nb0, st);
+    if (r != MB_OK) return r;
+    MARK(mk->fft_e[0]);
+  } else if (c.U) {
     MB_CUDA_TRY(cudaEventRecord(s->ev_fork, st));
     MB_CUDA_TRY(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
     r = fft_batch(0, nb0, s->side);
@@ -215,6 +225,7 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     MB_CUDA_TRY(cudaEventRecord(s->ev_join, s->side));
   }
   // pilots -> CSI -> W (+ precoder)
+  MARK(mk->pilot_b);
   r = mb_fft_pilot(s->fft, iq, c.iq_dtype, c.P, 0, reinterpret_cast<mb_c32 *>(s->csi), st);
   if (r != MB_OK) return r;
   MARK(mk->pilot);
@@ -234,7 +245,7 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     MARK(mk->end);
     return MB_OK;
   }
-  MB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
+  if (!mk) MB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
   const uint64_t llr_sym = (uint64_t)c.K * c.cb_stride;
   const uint64_t hard_sym = (uint64_t)c.K * s->hrow;
   uint32_t bi = 0;
@@ -352,15 +363,13 @@ extern "C" mb_status mb_slot_stage_ms(mb_slot *s, double *out) {
   for (uint32_t k = 0; k < s->marks_used; k++) {
     auto &m = s->marks[k];
     MB_CUDA_TRY(cudaEventSynchronize(m.end));
-    out[0] += ms(m.start, m.pilot);
+    out[0] += ms(m.pilot_b, m.pilot);
     out[1] += ms(m.pilot, m.zf);
     out[4] += ms(m.start, m.end);
     uint32_t bi = 0;
     for (uint32_t l0 = 0; l0 < s->c.U; l0 += s->c.sym_batch, bi++) {
-      if (l0) {
-        out[2] += ms(m.fft_b[bi], m.fft_e[bi]);
-        out[5] += 1;
-      }
+      out[2] += ms(m.fft_b[bi], m.fft_e[bi]);
+      out[5] += 1;
       out[3] += ms(m.eq_b[bi], m.eq_e[bi]);
       out[6] += 1;
     }
