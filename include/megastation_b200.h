@@ -316,8 +316,9 @@ mb_status mb_slot_downlink(mb_slot *slot, const mb_c32 *symbols, void *out,
 /* Stage timing.  mb_slot_timing(slot, n) makes the next n slot calls record
  * CUDA events around each stage on the launching stream (0 disables);
  * mb_slot_stage_ms waits for those events and returns, summed over the
- * recorded calls: [0] pilot FFT, [1] ZF (+ tail fill), [2] uplink FFT
- * batches issued on the launching stream, [3] equalize, [4] whole slot,
+ * recorded calls (while timing, every kernel runs alone on the launching
+ * stream, the first FFT batch included): [0] pilot FFT, [1] ZF (+ tail
+ * fill), [2] uplink FFT batches, [3] equalize, [4] whole slot,
  * [5] number of uplink FFT launches timed in [2], [6] equalize launches,
  * [7] recorded calls; then clears the record. */
 mb_status mb_slot_timing(mb_slot *slot, uint32_t max_calls);
@@ -326,6 +327,37 @@ mb_status mb_slot_stage_ms(mb_slot *slot, double *out8);
 /* Device views of the slot's internal buffers (for inspection and tests):
  * CSI/W [G][M][K], precoder [G][K][M]. */
 mb_status mb_slot_buffers(mb_slot *slot, mb_c32 **csi, mb_c32 **precoder);
+
+/* -------------------------------------------------------- batched cells --- */
+/* No counterpart in the reference, which processes one cell per
+ * BandProcess.  A set of cells of uneven shape (each an mb_cell_desc) runs
+ * one uplink slot per call as ONE CUDA graph launch: the graph forks into a
+ * branch per cell (that cell's slot) and joins, so the cells' kernels run
+ * concurrently.  Graphs are captured once per (pointer set, stream).  Every
+ * argument array has one entry per cell, in creation order; llr, hard and
+ * group_status arrays (and their entries) may be NULL as in
+ * mb_slot_uplink.  stream must not be the legacy default stream. */
+typedef struct mb_cells mb_cells;
+mb_status mb_cells_create(const mb_cell_desc *cells, uint32_t ncells, mb_cells **out);
+mb_status mb_cells_destroy(mb_cells *cells);
+mb_status mb_cells_uplink(mb_cells *cells, const void *const *iq, uint16_t *const *llr,
+                          uint8_t *const *hard, int32_t *const *group_status, void *stream);
+
+/* Tuning knobs per cell: sym_batch (uplink symbols per FFT/equalize batch,
+ * 1..U) and eq_cols (tensor-core equalizer (symbol, subcarrier) columns per
+ * CTA, a multiple of 8 up to 128).  mb_cells_autotune measures the batched
+ * slot (reps timed graph launches per candidate, CUDA events on stream) and
+ * keeps, per class of equal-shaped cells, the fastest candidate by
+ * coordinate descent; it writes the choice per cell (nullable outputs) and
+ * the tuned time in microseconds per slot.  Outputs of the tuning launches
+ * land in llr / hard. */
+mb_status mb_cells_autotune(mb_cells *cells, const void *const *iq, uint16_t *const *llr,
+                            uint8_t *const *hard, uint32_t reps, void *stream,
+                            uint32_t *sym_batch_out, uint32_t *eq_cols_out,
+                            double *us_per_slot);
+mb_status mb_cells_get_tuning(const mb_cells *cells, uint32_t *sym_batch, uint32_t *eq_cols);
+mb_status mb_cells_set_tuning(mb_cells *cells, const uint32_t *sym_batch,
+                              const uint32_t *eq_cols);
 
 #ifdef __cplusplus
 }

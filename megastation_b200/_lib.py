@@ -114,6 +114,13 @@ def _load():
         "mb_slot_buffers": (ST, [VP, ctypes.POINTER(VP), ctypes.POINTER(VP)]),
         "mb_slot_timing": (ST, [VP, U32]),
         "mb_slot_stage_ms": (ST, [VP, ctypes.POINTER(ctypes.c_double)]),
+        "mb_cells_create": (ST, [ctypes.POINTER(MbCellDesc), U32, ctypes.POINTER(VP)]),
+        "mb_cells_destroy": (ST, [VP]),
+        "mb_cells_uplink": (ST, [VP, VP, VP, VP, VP, VP]),
+        "mb_cells_autotune": (ST, [VP, VP, VP, VP, U32, VP, ctypes.POINTER(U32), ctypes.POINTER(U32),
+                                   ctypes.POINTER(ctypes.c_double)]),
+        "mb_cells_get_tuning": (ST, [VP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
+        "mb_cells_set_tuning": (ST, [VP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -310,7 +310,7 @@ bool equalize_tc_supported(uint32_t K, uint32_t sg, uint32_t nb) {
 }
 
 mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, uint32_t S_pad,
-                      uint32_t l0, uint32_t nb, int *err, cudaStream_t st) {
+                      uint32_t l0, uint32_t nb, int *err, cudaStream_t st, uint32_t max_cols) {
   if (!equalize_tc_supported(p.K, p.sg, nb)) return MB_UNSUPPORTED;
   if (S_pad % 8 || S_pad < p.S) return MB_BAD_SHAPE;
   TcShape s = tc_shape(p.M, p.K);
@@ -321,9 +321,10 @@ mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, ui
   q.S_pad = S_pad;
   q.Mp = s.Mp;
   q.nkt = s.nkt;
-  // symbols per CTA: as many as fill 128 columns, spread evenly over the
-  // CTAs a group needs
-  const uint32_t spc_max = kCols / p.sg;
+  // symbols per CTA: as many as fill max_cols (<= 128) columns, spread
+  // evenly over the CTAs a group needs
+  const uint32_t cols = max_cols ? std::min<uint32_t>(max_cols, kCols) : kCols;
+  const uint32_t spc_max = std::max<uint32_t>(1, cols / p.sg);
   const uint32_t ny = (nb + spc_max - 1) / spc_max;
   q.spc = (nb + ny - 1) / ny;
   q.nb = nb;

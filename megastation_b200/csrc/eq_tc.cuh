@@ -27,9 +27,11 @@ bool equalize_tc_supported(uint32_t K, uint32_t sg, uint32_t nb);
 // W [G][M][K] c32 -> detector images
 mb_status w_image(const float2 *W, void *img, uint32_t G, uint32_t M, uint32_t K,
                   cudaStream_t st);
-// equalize nb symbols (outputs at symbol offset l0 of p's outputs)
+// equalize nb symbols (outputs at symbol offset l0 of p's outputs); a CTA
+// takes the symbols of one group that fit in max_cols (<= 128, 0: 128)
+// (symbol, subcarrier) columns
 mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, uint32_t S_pad,
-                      uint32_t l0, uint32_t nb, int *err, cudaStream_t st);
+                      uint32_t l0, uint32_t nb, int *err, cudaStream_t st, uint32_t max_cols = 0);
 // y [nb][M][S] c32 -> y_lp [nb][re|im][M][S_pad] BF16
 mb_status y_to_lp(const float2 *y, void *y_lp, uint32_t nb, uint32_t M, uint32_t S,
                   uint32_t S_pad, cudaStream_t st);

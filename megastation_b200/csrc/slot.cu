@@ -31,6 +31,8 @@ struct mb_slot {
   void *y_lp;         // [sym_batch][re|im][M][S_pad] BF16 (mixed path)
   void *img_w;        // detector images for the tensor-core equalizer
   uint32_t S_pad;
+  uint32_t sb_cap;    // uplink symbols the y / y_lp buffers hold (>= sym_batch)
+  uint32_t eq_cols;   // tensor-core equalizer columns per CTA (0: 128)
   float2 *precoded;   // [D][M][N]
   cudaStream_t side;
   cudaEvent_t ev_fork, ev_join;
@@ -77,7 +79,7 @@ static mb_slot::Marks *next_marks(mb_slot *s) {
     m.pilot = new_event();
     m.zf = new_event();
     m.end = new_event();
-    const uint32_t nb = (s->c.U + s->c.sym_batch - 1) / s->c.sym_batch + 1;
+    const uint32_t nb = s->c.U + 1;  // batches of any sym_batch
     for (uint32_t i = 0; i < nb; i++) {
       m.fft_b.push_back(new_event());
       m.fft_e.push_back(new_event());
@@ -125,7 +127,9 @@ extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   return MB_OK;
 }
 
-extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
+// sb_cap_all: size the batch buffers for all U symbols, so that sym_batch
+// may later change (the batched-cells autotuner)
+static mb_status slot_create(const mb_cell_desc *cell, bool sb_cap_all, mb_slot **out) {
   if (!cell || !out) return MB_BAD_ARG;
   *out = nullptr;
   const mb_cell_desc &c = *cell;
@@ -139,6 +143,8 @@ extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
   s->c = c;
   if (s->c.sym_batch == 0) s->c.sym_batch = 4;
   s->c.sym_batch = std::min(s->c.sym_batch, std::max<uint32_t>(c.U, 1));
+  s->sb_cap = sb_cap_all ? std::max<uint32_t>(c.U, 1) : s->c.sym_batch;
+  s->eq_cols = 0;
   s->G = (c.S + c.sg - 1) / c.sg;
   s->n_valid = std::min<uint64_t>((uint64_t)c.S * c.Qm, c.cb_size);
   s->hrow = (s->n_valid + 7) / 8;
@@ -159,7 +165,7 @@ extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
   if (mixed && st == MB_OK && !equalize_tc_supported(c.K, c.sg, s->c.sym_batch))
     st = MB_UNSUPPORTED;
   s->S_pad = (c.S + 7) / 8 * 8;
-  const size_t ylp_bytes = (size_t)s->c.sym_batch * 2 * c.M * s->S_pad * 2;
+  const size_t ylp_bytes = (size_t)s->sb_cap * 2 * c.M * s->S_pad * 2;
   if (mixed) {
     alloc(&s->y_lp, ylp_bytes);
     alloc(&s->img_w, zf_mixed_scratch_bytes(s->G, c.M, c.K));
@@ -169,7 +175,7 @@ extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
       if (e != cudaSuccess) st = record_error(e);
     }
   } else {
-    alloc((void **)&s->y, sizeof(float2) * (size_t)s->c.sym_batch * c.M * c.S);
+    alloc((void **)&s->y, sizeof(float2) * (size_t)s->sb_cap * c.M * c.S);
   }
   if (st == MB_OK) {
     cudaError_t e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
@@ -189,6 +195,10 @@ extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
   }
   *out = s;
   return MB_OK;
+}
+
+extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {
+  return slot_create(cell, false, out);
 }
 
 static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
@@ -284,7 +294,8 @@ static mb_status slot_equalize(mb_slot *s, uint32_t nb, uint16_t *llr, uint8_t *
                                  hard, s->scr);
   if (r != MB_OK) return r;
   const DeviceTables *tab = device_tables();
-  return equalize_tc(p, s->img_w, s->y_lp, s->S_pad, 0, nb, tab ? tab->err : nullptr, st);
+  return equalize_tc(p, s->img_w, s->y_lp, s->S_pad, 0, nb, tab ? tab->err : nullptr, st,
+                     s->eq_cols);
 }
 
 extern "C" mb_status mb_slot_uplink(mb_slot *s, const void *iq, uint16_t *llr,
@@ -383,5 +394,291 @@ extern "C" mb_status mb_slot_buffers(mb_slot *s, mb_c32 **csi, mb_c32 **precoder
   if (!s) return MB_BAD_ARG;
   if (csi) *csi = reinterpret_cast<mb_c32 *>(s->csi);
   if (precoder) *precoder = reinterpret_cast<mb_c32 *>(s->precoder);
+  return MB_OK;
+}
+
+// ---------------------------------------------------------------- cells
+// Many cells of uneven shape per slot in ONE CUDA graph launch: the graph
+// forks from the launching stream into one branch per cell (each branch is
+// that cell's slot: pilot FFT, ZF, uplink FFT batches, equalize) and joins
+// back, so the cells' kernels run concurrently and the host issues a single
+// cudaGraphLaunch per slot.  The reference runs one cell per BandProcess and
+// has no batched form.
+struct mb_cells {
+  std::vector<mb_slot *> slots;
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
+  struct Entry {
+    std::vector<const void *> key;
+    cudaGraphExec_t exec;
+    uint64_t last_use;
+  };
+  std::vector<Entry> graphs;
+  uint64_t clock = 0;
+};
+
+static void cells_drop_graphs(mb_cells *cs) {
+  for (auto &e : cs->graphs) cudaGraphExecDestroy(e.exec);
+  cs->graphs.clear();
+}
+
+extern "C" mb_status mb_cells_destroy(mb_cells *cs) {
+  if (!cs) return MB_BAD_ARG;
+  cells_drop_graphs(cs);
+  for (auto *s : cs->slots) mb_slot_destroy(s);
+  for (auto b : cs->branch) cudaStreamDestroy(b);
+  for (auto e : cs->join) cudaEventDestroy(e);
+  if (cs->fork) cudaEventDestroy(cs->fork);
+  delete cs;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_cells_create(const mb_cell_desc *cells, uint32_t n, mb_cells **out) {
+  if (!cells || !out || n == 0) return MB_BAD_ARG;
+  *out = nullptr;
+  mb_cells *cs = new mb_cells();
+  mb_status st = MB_OK;
+  for (uint32_t c = 0; c < n && st == MB_OK; c++) {
+    mb_cell_desc d = cells[c];
+    d.use_graph = 0;  // the cells object captures all of them together
+    mb_slot *s = nullptr;
+    st = slot_create(&d, true, &s);
+    if (st == MB_OK) cs->slots.push_back(s);
+    cudaStream_t b = nullptr;
+    cudaEvent_t e = nullptr;
+    if (st == MB_OK) {
+      cudaError_t ce = cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking);
+      if (ce == cudaSuccess) cs->branch.push_back(b);
+      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+      if (ce == cudaSuccess) cs->join.push_back(e);
+      if (ce != cudaSuccess) st = record_error(ce);
+    }
+  }
+  if (st == MB_OK) {
+    cudaError_t ce = cudaEventCreateWithFlags(&cs->fork, cudaEventDisableTiming);
+    if (ce != cudaSuccess) st = record_error(ce);
+  }
+  if (st != MB_OK) {
+    mb_cells_destroy(cs);
+    return st;
+  }
+  *out = cs;
+  return MB_OK;
+}
+
+// one slot of every cell, captured into one graph per pointer set and stream
+static mb_status cells_launch(mb_cells *cs, const void *const *iq, uint16_t *const *llr,
+                              uint8_t *const *hard, int32_t *const *status, cudaStream_t st) {
+  const uint32_t n = (uint32_t)cs->slots.size();
+  std::vector<const void *> key;
+  key.reserve(4 * n + 1);
+  for (uint32_t c = 0; c < n; c++) {
+    if (!iq[c] || (cs->slots[c]->c.U && (!llr || !llr[c]))) return MB_BAD_ARG;
+    key.push_back(iq[c]);
+    key.push_back(llr ? llr[c] : nullptr);
+    key.push_back(hard ? hard[c] : nullptr);
+    key.push_back(status ? status[c] : nullptr);
+  }
+  key.push_back(st);
+  mb_cells::Entry *hit = nullptr;
+  for (auto &e : cs->graphs)
+    if (e.key == key) hit = &e;
+  if (!hit) {
+    MB_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    mb_status r = MB_OK;
+    cudaError_t ce = cudaEventRecord(cs->fork, st);
+    for (uint32_t c = 0; c < n && r == MB_OK && ce == cudaSuccess; c++) {
+      ce = cudaStreamWaitEvent(cs->branch[c], cs->fork, 0);
+      if (ce != cudaSuccess) break;
+      r = issue_uplink(cs->slots[c], iq[c], llr ? llr[c] : nullptr, hard ? hard[c] : nullptr,
+                       status ? status[c] : nullptr, cs->branch[c], nullptr);
+      if (r != MB_OK) break;
+      ce = cudaEventRecord(cs->join[c], cs->branch[c]);
+      if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, cs->join[c], 0);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(st, &g);
+    if (r != MB_OK || ce != cudaSuccess || ee != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      (void)cudaGetLastError();
+      return r != MB_OK ? r : record_error(ce != cudaSuccess ? ce : ee);
+    }
+    cudaGraphExec_t exec = nullptr;
+    ce = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return record_error(ce);
+    constexpr size_t kGraphCache = 8;
+    if (cs->graphs.size() >= kGraphCache) {
+      auto lru = cs->graphs.begin();
+      for (auto it = cs->graphs.begin(); it != cs->graphs.end(); ++it)
+        if (it->last_use < lru->last_use) lru = it;
+      cudaGraphExecDestroy(lru->exec);
+      cs->graphs.erase(lru);
+    }
+    cs->graphs.push_back({key, exec, 0});
+    hit = &cs->graphs.back();
+  }
+  hit->last_use = ++cs->clock;
+  MB_CUDA_TRY(cudaGraphLaunch(hit->exec, st));
+  return MB_OK;
+}
+
+extern "C" mb_status mb_cells_uplink(mb_cells *cs, const void *const *iq, uint16_t *const *llr,
+                                     uint8_t *const *hard, int32_t *const *status, void *stream) {
+  if (!cs || !iq) return MB_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  if (!st) return MB_BAD_ARG;  // the legacy stream cannot be captured
+  return cells_launch(cs, iq, llr, hard, status, st);
+}
+
+extern "C" mb_status mb_cells_get_tuning(const mb_cells *cs, uint32_t *sym_batch,
+                                         uint32_t *eq_cols) {
+  if (!cs) return MB_BAD_ARG;
+  for (size_t c = 0; c < cs->slots.size(); c++) {
+    if (sym_batch) sym_batch[c] = cs->slots[c]->c.sym_batch;
+    if (eq_cols) eq_cols[c] = cs->slots[c]->eq_cols ? cs->slots[c]->eq_cols : 128;
+  }
+  return MB_OK;
+}
+
+extern "C" mb_status mb_cells_set_tuning(mb_cells *cs, const uint32_t *sym_batch,
+                                         const uint32_t *eq_cols) {
+  if (!cs) return MB_BAD_ARG;
+  for (size_t c = 0; c < cs->slots.size(); c++) {
+    mb_slot *s = cs->slots[c];
+    if (sym_batch && (sym_batch[c] == 0 || sym_batch[c] > s->sb_cap)) return MB_BAD_ARG;
+    if (eq_cols && eq_cols[c] != 0 && (eq_cols[c] % 8 || eq_cols[c] > 128)) return MB_BAD_ARG;
+  }
+  for (size_t c = 0; c < cs->slots.size(); c++) {
+    if (sym_batch) cs->slots[c]->c.sym_batch = sym_batch[c];
+    if (eq_cols) cs->slots[c]->eq_cols = eq_cols[c] == 128 ? 0 : eq_cols[c];
+  }
+  cells_drop_graphs(cs);  // the captured work changes
+  return MB_OK;
+}
+
+// microseconds per slot of the current tuning: warm-up, then reps graph
+// launches timed with CUDA events on st
+static mb_status cells_time(mb_cells *cs, const void *const *iq, uint16_t *const *llr,
+                            uint8_t *const *hard, uint32_t reps, cudaStream_t st, double *us) {
+  for (int w = 0; w < 3; w++) {
+    mb_status r = cells_launch(cs, iq, llr, hard, nullptr, st);
+    if (r != MB_OK) return r;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MB_CUDA_TRY(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return record_error(ce);
+  }
+  mb_status r = MB_OK;
+  ce = cudaEventRecord(e0, st);
+  for (uint32_t k = 0; k < reps && r == MB_OK && ce == cudaSuccess; k++)
+    r = cells_launch(cs, iq, llr, hard, nullptr, st);
+  if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+  if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r != MB_OK) return r;
+  if (ce != cudaSuccess) return record_error(ce);
+  *us = 1e3 * ms / std::max<uint32_t>(reps, 1);
+  return MB_OK;
+}
+
+// Autotuner: the knobs are, per cell, the uplink symbols per FFT/equalize
+// batch (sym_batch) and the tensor-core equalizer's (symbol, subcarrier)
+// columns per CTA (its MMA tile).  Cells of one shape form a class and share
+// a choice; classes are visited by decreasing work, each trying its
+// candidates with the others fixed (coordinate descent on the measured time
+// of the whole batched slot) and keeping a candidate only if it is at least
+// 1% faster.  The tuning stays on the object (later mb_cells_uplink calls
+// use it) and is returned per cell.
+extern "C" mb_status mb_cells_autotune(mb_cells *cs, const void *const *iq, uint16_t *const *llr,
+                                       uint8_t *const *hard, uint32_t reps, void *stream,
+                                       uint32_t *sym_batch_out, uint32_t *eq_cols_out,
+                                       double *us_per_slot) {
+  if (!cs || !iq) return MB_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  if (!st) return MB_BAD_ARG;
+  const uint32_t n = (uint32_t)cs->slots.size();
+  if (reps == 0) reps = 20;
+  // shape classes
+  std::vector<int> cls(n, -1);
+  std::vector<std::vector<uint32_t>> members;
+  std::vector<double> work;
+  for (uint32_t c = 0; c < n; c++) {
+    const mb_cell_desc &a = cs->slots[c]->c;
+    for (size_t k = 0; k < members.size(); k++) {
+      const mb_cell_desc &b = cs->slots[members[k][0]]->c;
+      if (a.M == b.M && a.K == b.K && a.N == b.N && a.S == b.S && a.sg == b.sg && a.Qm == b.Qm &&
+          a.U == b.U && a.P == b.P && a.zf_precision == b.zf_precision) {
+        cls[c] = (int)k;
+        break;
+      }
+    }
+    if (cls[c] < 0) {
+      cls[c] = (int)members.size();
+      members.push_back({});
+      work.push_back(0.0);
+    }
+    members[cls[c]].push_back(c);
+    work[cls[c]] += (double)a.M * a.N * (a.P + a.U);
+  }
+  std::vector<uint32_t> order(members.size());
+  for (size_t k = 0; k < order.size(); k++) order[k] = (uint32_t)k;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return work[a] > work[b]; });
+
+  std::vector<uint32_t> sb(n), cols(n);
+  for (uint32_t c = 0; c < n; c++) {
+    sb[c] = std::max<uint32_t>(cs->slots[c]->c.U, 1);
+    cols[c] = 128;
+  }
+  mb_status r = mb_cells_set_tuning(cs, sb.data(), cols.data());
+  double best = 0.0;
+  if (r == MB_OK) r = cells_time(cs, iq, llr, hard, reps, st, &best);
+  for (uint32_t k : order) {
+    if (r != MB_OK) break;
+    const mb_cell_desc &d = cs->slots[members[k][0]]->c;
+    const uint32_t U = std::max<uint32_t>(d.U, 1);
+    std::vector<std::pair<uint32_t, uint32_t>> cand;
+    for (uint32_t parts = 1; parts <= 3; parts++) {
+      const uint32_t b = (U + parts - 1) / parts;
+      for (uint32_t cl : {128u, 64u}) {
+        if (d.zf_precision != MB_ZF_MIXED && cl != 128) continue;
+        bool dup = false;
+        for (auto &x : cand) dup |= x.first == b && x.second == cl;
+        if (!dup) cand.push_back({b, cl});
+      }
+    }
+    std::pair<uint32_t, uint32_t> cur{sb[members[k][0]], cols[members[k][0]]};
+    for (auto &cv : cand) {
+      if (cv == cur) continue;
+      for (uint32_t c : members[k]) {
+        sb[c] = cv.first;
+        cols[c] = cv.second;
+      }
+      double t = 0.0;
+      r = mb_cells_set_tuning(cs, sb.data(), cols.data());
+      if (r == MB_OK) r = cells_time(cs, iq, llr, hard, reps, st, &t);
+      if (r != MB_OK) break;
+      if (t < 0.99 * best) {
+        best = t;
+        cur = cv;
+      }
+    }
+    for (uint32_t c : members[k]) {
+      sb[c] = cur.first;
+      cols[c] = cur.second;
+    }
+  }
+  if (r == MB_OK) r = mb_cells_set_tuning(cs, sb.data(), cols.data());
+  if (r != MB_OK) return r;
+  if (sym_batch_out) std::copy(sb.begin(), sb.end(), sym_batch_out);
+  if (eq_cols_out) std::copy(cols.begin(), cols.end(), eq_cols_out);
+  if (us_per_slot) *us_per_slot = best;
   return MB_OK;
 }

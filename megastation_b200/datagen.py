@@ -218,3 +218,28 @@ def make_slot(cfg):
     iq = _to_time(cfg, Y, gain)
     return dict(iq=iq, H=H, bits=bits, x=X, noise_var=noise_var, pilot_raw=pilot_raw,
                 seq=seq, gain=gain, Y=Y)
+
+
+# data subcarriers and their FFT size, as the batched-cells workload pairs them
+CELL_SUBCARRIERS = {600: 1024, 1200: 2048, 3276: 4096}
+
+
+def make_cells(n=32, seed=3, symbols=14, sg=16, snr_db=(15.0, 25.0), M_set=(32, 64, 128),
+               K_set=(4, 8, 16, 32), S_set=(600, 1200, 3276), Qm_set=(2, 4, 6)):
+    """Seeded configurations of n uneven cells: antennas from M_set, users
+    from K_set (K <= M), data subcarriers from S_set with the FFT size of
+    CELL_SUBCARRIERS, QAM order from Qm_set, i.i.d. Rayleigh channels per
+    subcarrier group, per-cell SNR uniform in snr_db; P = ceil(K / sg) comb
+    pilot symbols and U = symbols - P data symbols."""
+    rng = np.random.default_rng(seed)
+    cfgs = []
+    for c in range(n):
+        M = int(rng.choice(M_set))
+        K = int(rng.choice([k for k in K_set if k <= M]))
+        S = int(rng.choice(S_set))
+        Qm = int(rng.choice(Qm_set))
+        P = (K + sg - 1) // sg
+        cfgs.append(CellConfig(M=M, K=K, N=CELL_SUBCARRIERS[S], S=S, sg=sg, Qm=Qm, U=symbols - P,
+                               snr_db=float(rng.uniform(*snr_db)), channel="iid_group",
+                               seed=int(rng.integers(1 << 31))))
+    return cfgs
