@@ -359,6 +359,56 @@ mb_status mb_cells_get_tuning(const mb_cells *cells, uint32_t *sym_batch, uint32
 mb_status mb_cells_set_tuning(mb_cells *cells, const uint32_t *sym_batch,
                               const uint32_t *eq_cols);
 
+/* ------------------------------------------------ learned ZF initialiser --- */
+/* No counterpart in the reference.  A 3-layer MLP (n_in -> width -> width
+ * -> n_out, ReLU) with FP32 master weights, BF16 weights in every product
+ * and FP32 accumulation, trained by the library's own forward, backward and
+ * Adam kernels on the quadratic loss y^T A y - 2 b^T y + c per sample
+ * (A [batch][n_out][n_out], b [batch][n_out], c [batch] or NULL for 0),
+ * averaged over the batch.  Parameters are flat FP32: W1 [n_in][width], b1,
+ * W2 [width][width], b2, W3 [width][n_out], b3.  All x / y / A / b / c /
+ * loss pointers are device memory; params and grads copies are host. */
+typedef struct mb_mlp mb_mlp;
+mb_status mb_mlp_create(uint32_t n_in, uint32_t width, uint32_t n_out, uint32_t max_batch,
+                        uint64_t seed, mb_mlp **out);
+mb_status mb_mlp_destroy(mb_mlp *mlp);
+mb_status mb_mlp_num_params(const mb_mlp *mlp, uint64_t *count);
+mb_status mb_mlp_get_params(const mb_mlp *mlp, float *host);
+mb_status mb_mlp_set_params(mb_mlp *mlp, const float *host); /* also resets Adam */
+mb_status mb_mlp_get_grads(const mb_mlp *mlp, float *host);  /* of the last loss_grad */
+mb_status mb_mlp_forward(mb_mlp *mlp, const float *x, uint32_t batch, float *y, void *stream);
+mb_status mb_mlp_loss_grad(mb_mlp *mlp, const float *x, const float *A, const float *b,
+                           const float *c, uint32_t batch, float *loss, void *stream);
+mb_status mb_mlp_adam_step(mb_mlp *mlp, float lr, void *stream);
+
+/* Per-subcarrier ZF from the comb-pilot CSI [G][M][K] (K <= 32, M K <= 3072):
+ * each user's pilots are interpolated linearly along frequency to a CSI
+ * estimate c_s [M][K] per subcarrier, G_s is the reference's Gram C C^H of
+ * it (C[u][b] = c_s[b][u]), the Grams at the group centres (subcarrier g sg + sg/2) are inverted
+ * exactly, and the initial iterate of every subcarrier is the group's own
+ * centre inverse (MB_LZF_COARSE), a blend of the centre inverses of groups
+ * g-1..g+2 with weights from the MLP (MB_LZF_LEARNED; n_in = sg + 6,
+ * n_out = 4), or the exact inverse of G_s (MB_LZF_EXACT); ns_iters
+ * Newton-Schulz steps follow.  W [S][M][K] is the per-subcarrier detector,
+ * usable by mb_equalize with sc_group = 1. */
+enum { MB_LZF_COARSE = 0, MB_LZF_LEARNED = 1, MB_LZF_EXACT = 2 };
+typedef struct mb_lzf mb_lzf;
+mb_status mb_lzf_create(uint32_t M, uint32_t K, uint32_t S, uint32_t sg, mb_lzf **out);
+mb_status mb_lzf_destroy(mb_lzf *lzf);
+uint32_t mb_lzf_num_features(uint32_t sg);
+/* features [S][sg + 6] (device, FP32) of every subcarrier: one-hot offset in
+ * its group, then for the groups g-1, g+1, g+2 the relative Frobenius
+ * distance of their centre Gram to group g's and the trace ratio minus 1 */
+mb_status mb_lzf_features(mb_lzf *lzf, const mb_c32 *csi, float *features, void *stream);
+/* training targets of the blend from an FP64 pass: A [S][4][4], b [S][4] so
+ * that alpha^T A alpha - 2 b^T alpha + 1 = ||X0(alpha) - G_s^{-1}||^2 /
+ * ||G_s^{-1}||^2 */
+mb_status mb_lzf_targets(mb_lzf *lzf, const mb_c32 *csi, float *A, float *b, void *stream);
+mb_status mb_lzf_run(mb_lzf *lzf, const mb_c32 *csi, mb_mlp *mlp, int init, uint32_t ns_iters,
+                     mb_c32 *W, void *stream);
+/* ||I - G_s X_s||_F per subcarrier of the last run, res [S] (device) */
+mb_status mb_lzf_residual(mb_lzf *lzf, float *res, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

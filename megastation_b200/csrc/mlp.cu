@@ -1,0 +1,347 @@
+// mlp.cu -- the network of the learned ZF initialiser: a 3-layer MLP
+// (n_in -> width -> width -> n_out, ReLU after the first two layers) with
+// FP32 master weights, BF16 copies of the weights for every product and FP32
+// accumulation, trained by the project's own forward, backward and Adam
+// kernels.  No counterpart in the reference.
+//
+// The training loss is the quadratic form the initialiser needs: each sample
+// carries a symmetric O x O matrix A, a vector b and a scalar c, and for the
+// network output y the loss is y^T A y - 2 b^T y + c (the squared Frobenius
+// distance of the blended initial iterate to the exact inverse, normalised;
+// see lzf.cu), averaged over the batch.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <random>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mb {
+namespace {
+
+constexpr int kTM = 64, kTN = 64, kTK = 16, kGT = 256;
+
+__device__ __forceinline__ float ldf(const float *p, size_t i) { return p[i]; }
+__device__ __forceinline__ float ldf(const __nv_bfloat16 *p, size_t i) { return __bfloat162float(p[i]); }
+
+// C(m, n) = sum_k A(m, k) B(k, n) with A(m, k) = TRA ? A[k lda + m] : A[m lda + k]
+// and B(k, n) = TRB ? B[n ldb + k] : B[k ldb + n]; epilogue: + bias[n], then
+// optionally times (mask(m, n) > 0) (the ReLU derivative), or ReLU with the
+// pre-activation kept in zout; accumulate adds to C.  64 x 64 tiles, each
+// thread 4 x 4 outputs.
+template <typename TA, typename TB, bool TRA, bool TRB>
+__global__ void __launch_bounds__(kGT) gemm_kernel(int M, int N, int K, const TA *A, int lda,
+                                                   const TB *B, int ldb, float *C, int ldc,
+                                                   const float *bias, const float *mask,
+                                                   float *zout, int relu, int accumulate) {
+  __shared__ float As[kTK][kTM + 4];
+  __shared__ float Bs[kTK][kTN + 4];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += kTK) {
+    for (int e = tid; e < kTM * kTK; e += kGT) {
+      // consecutive threads read consecutive memory in either layout
+      const int mm = TRA ? e % kTM : e / kTK, kk = TRA ? e / kTM : e % kTK;
+      const int m = m0 + mm, k = k0 + kk;
+      As[kk][mm] = (m < M && k < K) ? ldf(A, TRA ? (size_t)k * lda + m : (size_t)m * lda + k) : 0.f;
+    }
+    for (int e = tid; e < kTK * kTN; e += kGT) {
+      const int nn = TRB ? e / kTK : e % kTN, kk = TRB ? e % kTK : e / kTN;
+      const int n = n0 + nn, k = k0 + kk;
+      Bs[kk][nn] = (n < N && k < K) ? ldf(B, TRB ? (size_t)n * ldb + k : (size_t)k * ldb + n) : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kTK; kk++) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
+      if (m >= M || n >= N) continue;
+      const size_t o = (size_t)m * ldc + n;
+      float v = acc[i][j] + (bias ? bias[n] : 0.f);
+      if (mask && !(mask[o] > 0.f)) v = 0.f;
+      if (relu) {
+        if (zout) zout[o] = v;
+        v = fmaxf(v, 0.f);
+      }
+      C[o] = accumulate ? C[o] + v : v;
+    }
+}
+
+template <typename TA, typename TB, bool TRA, bool TRB>
+cudaError_t gemm(int M, int N, int K, const TA *A, int lda, const TB *B, int ldb, float *C, int ldc,
+                 const float *bias, const float *mask, float *zout, int relu, int accumulate,
+                 cudaStream_t st) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  const dim3 grid((N + kTN - 1) / kTN, (M + kTM - 1) / kTM);
+  gemm_kernel<TA, TB, TRA, TRB><<<grid, kGT, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, mask,
+                                                     zout, relu, accumulate);
+  return cudaGetLastError();
+}
+
+// out[n] = sum_m X[m][n] (bias gradients), X row-major [M][N]
+__global__ void colsum_kernel(const float *X, int M, int N, float *out) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  float s = 0.f;
+  for (int m = 0; m < M; m++) s += X[(size_t)m * N + n];
+  out[n] = s;
+}
+
+// per sample: L = y^T A y - 2 b^T y + c; dY = 2 (A y - b) / B; the batch
+// mean of L is accumulated into *loss (zeroed by the caller)
+__global__ void quad_loss_kernel(const float *Y, const float *A, const float *b, const float *c,
+                                 int B, int O, float *dY, float *loss) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float li = 0.f;
+  if (i < B) {
+    const float *y = Y + (size_t)i * O;
+    const float *Ai = A + (size_t)i * O * O;
+    const float *bi = b + (size_t)i * O;
+    float quad = 0.f, lin = 0.f;
+    for (int r = 0; r < O; r++) {
+      float ay = 0.f;
+      for (int q = 0; q < O; q++) ay = fmaf(Ai[r * O + q], y[q], ay);
+      quad = fmaf(y[r], ay, quad);
+      lin = fmaf(bi[r], y[r], lin);
+      dY[(size_t)i * O + r] = 2.f * (ay - bi[r]) / (float)B;
+    }
+    li = (quad - 2.f * lin + (c ? c[i] : 0.f)) / (float)B;
+  }
+  for (int o = 16; o > 0; o >>= 1) li += __shfl_xor_sync(0xffffffffu, li, o);
+  if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, li);
+}
+
+__global__ void adam_kernel(float *p, const float *g, float *m, float *v, uint64_t n, float lr,
+                            float b1, float b2, float eps, float c1, float c2) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void to_bf16_kernel(const float *x, __nv_bfloat16 *y, uint64_t n) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = __float2bfloat16_rn(x[i]);
+}
+
+}  // namespace
+}  // namespace mb
+
+using namespace mb;
+
+struct mb_mlp {
+  uint32_t n_in, width, n_out, max_batch;
+  uint64_t n_params;
+  // flat FP32 layout: W1 [n_in][width], b1, W2 [width][width], b2, W3 [width][n_out], b3
+  uint64_t off[6];
+  float *p, *g, *m, *v;        // params, grads, Adam moments
+  __nv_bfloat16 *wb;           // BF16 copies of p (all entries; only W* are read)
+  float *z1, *h1, *z2, *h2, *y, *dy, *d2, *d1;  // activations and their gradients
+  uint32_t step;
+};
+
+static cudaError_t mlp_refresh_bf16(mb_mlp *n, cudaStream_t st) {
+  const unsigned blocks = (unsigned)((n->n_params + 255) / 256);
+  to_bf16_kernel<<<blocks, 256, 0, st>>>(n->p, n->wb, n->n_params);
+  return cudaGetLastError();
+}
+
+extern "C" mb_status mb_mlp_destroy(mb_mlp *n) {
+  if (!n) return MB_BAD_ARG;
+  for (void *q : {(void *)n->p, (void *)n->g, (void *)n->m, (void *)n->v, (void *)n->wb,
+                  (void *)n->z1, (void *)n->h1, (void *)n->z2, (void *)n->h2, (void *)n->y,
+                  (void *)n->dy, (void *)n->d2, (void *)n->d1})
+    cudaFree(q);
+  delete n;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_mlp_create(uint32_t n_in, uint32_t width, uint32_t n_out,
+                                   uint32_t max_batch, uint64_t seed, mb_mlp **out) {
+  if (!out) return MB_BAD_ARG;
+  *out = nullptr;
+  if (n_in == 0 || width == 0 || n_out == 0 || max_batch == 0 || n_in > 4096 || width > 4096 ||
+      n_out > 64)
+    return MB_BAD_SHAPE;
+  mb_mlp *n = new mb_mlp();
+  n->n_in = n_in;
+  n->width = width;
+  n->n_out = n_out;
+  n->max_batch = max_batch;
+  const uint64_t sizes[6] = {(uint64_t)n_in * width, width, (uint64_t)width * width, width,
+                             (uint64_t)width * n_out, n_out};
+  uint64_t o = 0;
+  for (int i = 0; i < 6; i++) {
+    n->off[i] = o;
+    o += sizes[i];
+  }
+  n->n_params = o;
+  mb_status st = MB_OK;
+  auto alloc = [&](void **q, size_t bytes) {
+    if (st != MB_OK) return;
+    cudaError_t e = cudaMalloc(q, bytes);
+    if (e != cudaSuccess) st = record_error(e);
+  };
+  const size_t P = sizeof(float) * o;
+  alloc((void **)&n->p, P);
+  alloc((void **)&n->g, P);
+  alloc((void **)&n->m, P);
+  alloc((void **)&n->v, P);
+  alloc((void **)&n->wb, sizeof(__nv_bfloat16) * o);
+  const size_t BW = sizeof(float) * (size_t)max_batch * width;
+  alloc((void **)&n->z1, BW);
+  alloc((void **)&n->h1, BW);
+  alloc((void **)&n->z2, BW);
+  alloc((void **)&n->h2, BW);
+  alloc((void **)&n->d2, BW);
+  alloc((void **)&n->d1, BW);
+  alloc((void **)&n->y, sizeof(float) * (size_t)max_batch * n_out);
+  alloc((void **)&n->dy, sizeof(float) * (size_t)max_batch * n_out);
+  if (st == MB_OK) {
+    // He-normal hidden layers; the output layer starts at zero weights so the
+    // untrained network returns its bias (set by the caller)
+    std::vector<float> h(o, 0.f);
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<float> nd(0.f, 1.f);
+    const float s1 = std::sqrt(2.f / n_in), s2 = std::sqrt(2.f / width);
+    for (uint64_t i = 0; i < sizes[0]; i++) h[n->off[0] + i] = s1 * nd(rng);
+    for (uint64_t i = 0; i < sizes[2]; i++) h[n->off[2] + i] = s2 * nd(rng);
+    cudaError_t e = cudaMemcpy(n->p, h.data(), P, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(n->m, 0, P);
+    if (e == cudaSuccess) e = cudaMemset(n->v, 0, P);
+    if (e == cudaSuccess) e = cudaMemset(n->g, 0, P);
+    if (e == cudaSuccess) e = mlp_refresh_bf16(n, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) st = record_error(e);
+  }
+  if (st != MB_OK) {
+    mb_mlp_destroy(n);
+    return st;
+  }
+  *out = n;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_mlp_num_params(const mb_mlp *n, uint64_t *count) {
+  if (!n || !count) return MB_BAD_ARG;
+  *count = n->n_params;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_mlp_get_params(const mb_mlp *n, float *host) {
+  if (!n || !host) return MB_BAD_ARG;
+  MB_CUDA_TRY(cudaMemcpy(host, n->p, sizeof(float) * n->n_params, cudaMemcpyDeviceToHost));
+  return MB_OK;
+}
+
+extern "C" mb_status mb_mlp_get_grads(const mb_mlp *n, float *host) {
+  if (!n || !host) return MB_BAD_ARG;
+  MB_CUDA_TRY(cudaMemcpy(host, n->g, sizeof(float) * n->n_params, cudaMemcpyDeviceToHost));
+  return MB_OK;
+}
+
+extern "C" mb_status mb_mlp_set_params(mb_mlp *n, const float *host) {
+  if (!n || !host) return MB_BAD_ARG;
+  const size_t P = sizeof(float) * n->n_params;
+  MB_CUDA_TRY(cudaMemcpy(n->p, host, P, cudaMemcpyHostToDevice));
+  MB_CUDA_TRY(cudaMemset(n->m, 0, P));
+  MB_CUDA_TRY(cudaMemset(n->v, 0, P));
+  n->step = 0;
+  MB_CUDA_TRY(mlp_refresh_bf16(n, nullptr));
+  MB_CUDA_TRY(cudaDeviceSynchronize());
+  return MB_OK;
+}
+
+// forward into n->y (and the activations), BF16 weights, FP32 accumulation
+static cudaError_t mlp_fwd(mb_mlp *n, const float *x, uint32_t B, float *y, cudaStream_t st) {
+  const int I = n->n_in, W = n->width, O = n->n_out;
+  const __nv_bfloat16 *wb = n->wb;
+  cudaError_t e = gemm<float, __nv_bfloat16, false, false>(B, W, I, x, I, wb + n->off[0], W, n->h1, W,
+                                                          n->p + n->off[1], nullptr, n->z1, 1, 0, st);
+  if (e == cudaSuccess)
+    e = gemm<float, __nv_bfloat16, false, false>(B, W, W, n->h1, W, wb + n->off[2], W, n->h2, W,
+                                                n->p + n->off[3], nullptr, n->z2, 1, 0, st);
+  if (e == cudaSuccess)
+    e = gemm<float, __nv_bfloat16, false, false>(B, O, W, n->h2, W, wb + n->off[4], O, y, O,
+                                                n->p + n->off[5], nullptr, nullptr, 0, 0, st);
+  return e;
+}
+
+extern "C" mb_status mb_mlp_forward(mb_mlp *n, const float *x, uint32_t batch, float *y,
+                                    void *stream) {
+  if (!n || !x || !y) return MB_BAD_ARG;
+  if (batch == 0) return MB_OK;
+  if (batch > n->max_batch) return MB_BAD_SHAPE;
+  MB_CUDA_TRY(mlp_fwd(n, x, batch, y, as_stream(stream)));
+  return MB_OK;
+}
+
+extern "C" mb_status mb_mlp_loss_grad(mb_mlp *n, const float *x, const float *A, const float *b,
+                                      const float *c, uint32_t batch, float *loss, void *stream) {
+  if (!n || !x || !A || !b) return MB_BAD_ARG;
+  if (batch == 0 || batch > n->max_batch) return MB_BAD_SHAPE;
+  cudaStream_t st = as_stream(stream);
+  const int I = n->n_in, W = n->width, O = n->n_out, B = (int)batch;
+  const __nv_bfloat16 *wb = n->wb;
+  float *g = n->g;
+  MB_CUDA_TRY(mlp_fwd(n, x, batch, n->y, st));
+  if (loss) MB_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(float), st));
+  quad_loss_kernel<<<(B + 255) / 256, 256, 0, st>>>(n->y, A, b, c, B, O, n->dy, loss);
+  MB_CUDA_TRY(cudaGetLastError());
+  // layer 3: dW3 = H2^T dY, db3 = colsum dY, dH2 = (dY W3^T) * relu'(Z2)
+  MB_CUDA_TRY((gemm<float, float, true, false>(W, O, B, n->h2, W, n->dy, O, g + n->off[4], O, nullptr,
+                                               nullptr, nullptr, 0, 0, st)));
+  colsum_kernel<<<(O + 255) / 256, 256, 0, st>>>(n->dy, B, O, g + n->off[5]);
+  MB_CUDA_TRY((gemm<float, __nv_bfloat16, false, true>(B, W, O, n->dy, O, wb + n->off[4], O, n->d2, W,
+                                                       nullptr, n->z2, nullptr, 0, 0, st)));
+  // layer 2
+  MB_CUDA_TRY((gemm<float, float, true, false>(W, W, B, n->h1, W, n->d2, W, g + n->off[2], W, nullptr,
+                                               nullptr, nullptr, 0, 0, st)));
+  colsum_kernel<<<(W + 255) / 256, 256, 0, st>>>(n->d2, B, W, g + n->off[3]);
+  MB_CUDA_TRY((gemm<float, __nv_bfloat16, false, true>(B, W, W, n->d2, W, wb + n->off[2], W, n->d1, W,
+                                                       nullptr, n->z1, nullptr, 0, 0, st)));
+  // layer 1
+  MB_CUDA_TRY((gemm<float, float, true, false>(I, W, B, x, I, n->d1, W, g + n->off[0], W, nullptr,
+                                               nullptr, nullptr, 0, 0, st)));
+  colsum_kernel<<<(W + 255) / 256, 256, 0, st>>>(n->d1, B, W, g + n->off[1]);
+  MB_CUDA_TRY(cudaGetLastError());
+  return MB_OK;
+}
+
+extern "C" mb_status mb_mlp_adam_step(mb_mlp *n, float lr, void *stream) {
+  if (!n) return MB_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  n->step++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - std::pow(b1, (float)n->step), c2 = 1.f - std::pow(b2, (float)n->step);
+  const unsigned blocks = (unsigned)((n->n_params + 255) / 256);
+  adam_kernel<<<blocks, 256, 0, st>>>(n->p, n->g, n->m, n->v, n->n_params, lr, b1, b2, 1e-8f, c1, c2);
+  MB_CUDA_TRY(cudaGetLastError());
+  MB_CUDA_TRY(mlp_refresh_bf16(n, st));
+  return MB_OK;
+}

@@ -18,7 +18,8 @@ on subcarrier s as stream bits s*Qm .. s*Qm+Qm-1.
 Channels: "iid_group" draws CN(0,1) per (group of sg subcarriers, antenna,
 user); "tdl" draws an n_taps exponential power-delay-profile channel with
 exponential antenna correlation rho (Kronecker, receive side), normalised
-to unit average power per link.  AWGN is added per subcarrier at the stated
+to unit average power per link; "tdl_ds" is the same with the taps spread
+over three delay spreads given in nanoseconds (tap_profile).  AWGN is added per subcarrier at the stated
 per-user SNR.
 """
 from dataclasses import dataclass, field
@@ -38,10 +39,12 @@ class CellConfig:
     Qm: int = 4            # bits per QAM symbol
     U: int = 13            # uplink data symbols per slot
     snr_db: float = 20.0
-    channel: str = "iid_group"   # or "tdl"
+    channel: str = "iid_group"   # or "tdl", "tdl_ds"
     n_taps: int = 8
     tap_decay: float = 2.0       # PDP e^{-l / tap_decay}, in samples
     rho: float = 0.0             # antenna correlation
+    delay_spread_ns: float = 0.0  # tdl_ds: exponential PDP decay constant
+    scs_hz: float = 30e3          # subcarrier spacing (tdl_ds)
     iq_dtype: str = "c64"        # c64 | int16 | int8 | f16
     scrambler: str = "lfsr127"   # lfsr127 | gold
     c_init: int = 0x1234
@@ -132,6 +135,23 @@ def scrambling_bits(cfg, n_bits):
     return np.tile(seq[np.arange(n_bits) % 127], (cfg.K, 1))
 
 
+def tap_profile(cfg):
+    """Tap delays (in samples) and powers of the TDL channels.  "tdl": taps at
+    0..L-1 samples with PDP e^{-l / tap_decay}.  "tdl_ds": L taps spread over
+    [0, 3 ds] with PDP e^{-tau / ds}, ds = delay_spread_ns at the sample rate
+    N * scs_hz (fractional delays)."""
+    L = cfg.n_taps
+    if cfg.channel == "tdl_ds":
+        fs = cfg.N * cfg.scs_hz
+        ds = max(cfg.delay_spread_ns, 1e-3) * 1e-9 * fs
+        tau = np.arange(L) * (3.0 * ds / max(L - 1, 1))
+        pdp = np.exp(-tau / ds)
+    else:
+        tau = np.arange(L, dtype=np.float64)
+        pdp = np.exp(-tau / cfg.tap_decay)
+    return tau, pdp / pdp.sum()
+
+
 def _channel(cfg, rng):
     """Frequency response H[s][b][u] (complex64) on the S data subcarriers."""
     M, K, S, sg = cfg.M, cfg.K, cfg.S, cfg.sg
@@ -141,8 +161,7 @@ def _channel(cfg, rng):
         return h[np.arange(S) // sg].astype(np.complex64)
     # tdl: taps[l][b][u] with exponential PDP and receive correlation
     L = cfg.n_taps
-    pdp = np.exp(-np.arange(L) / cfg.tap_decay)
-    pdp /= pdp.sum()
+    tau, pdp = tap_profile(cfg)
     w = (rng.standard_normal((L, M, K)) + 1j * rng.standard_normal((L, M, K))) / np.sqrt(2)
     if cfg.rho:
         idx = np.arange(M)
@@ -153,7 +172,7 @@ def _channel(cfg, rng):
     bins = (np.arange(S) + cfg.start + cfg.N // 2) % cfg.N
     # the data bins' physical frequency offset relative to DC
     f = ((bins + cfg.N // 2) % cfg.N) - cfg.N // 2
-    ph = np.exp(-2j * np.pi * np.outer(f, np.arange(L)) / cfg.N)  # [S][L]
+    ph = np.exp(-2j * np.pi * np.outer(f, tau) / cfg.N)  # [S][L], tau in samples
     H = np.tensordot(ph, taps, axes=(1, 0))  # [S][M][K]
     return H.astype(np.complex64)
 
