@@ -164,91 +164,6 @@ __global__ void gather_kernel(const float2 *Gs, const uint32_t *cidx, float2 *Gc
   }
 }
 
-// 4. features of subcarrier s: one-hot of its offset in the group (sg),
-// then for j = -1, +1, +2: ||Gc[g+j] - Gc[g]||_F / ||Gc[g]||_F and
-// tr Gc[g+j] / tr Gc[g] - 1 (0 where g+j leaves the band)
-__global__ void features_kernel(const float2 *Gc, float *F, uint32_t K, uint32_t S, uint32_t sg,
-                                uint32_t G) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S) return;
-  const uint32_t g = s / sg, o = s % sg, nf = sg + 6;
-  float *f = F + (uint64_t)s * nf;
-  for (uint32_t q = 0; q < sg; q++) f[q] = q == o ? 1.f : 0.f;
-  const float2 *C0 = Gc + (uint64_t)g * K * K;
-  float n0 = 0.f, t0 = 0.f;
-  for (uint32_t e = 0; e < K * K; e++) n0 += C0[e].x * C0[e].x + C0[e].y * C0[e].y;
-  for (uint32_t u = 0; u < K; u++) t0 += C0[u * K + u].x;
-  n0 = sqrtf(n0);
-  const int js[3] = {-1, 1, 2};
-  for (int q = 0; q < 3; q++) {
-    const int gj = (int)g + js[q];
-    float d = 0.f, tr = 0.f;
-    if (gj >= 0 && gj < (int)G) {
-      const float2 *Cj = Gc + (uint64_t)gj * K * K;
-      for (uint32_t e = 0; e < K * K; e++) {
-        const float dx = Cj[e].x - C0[e].x, dy = Cj[e].y - C0[e].y;
-        d += dx * dx + dy * dy;
-      }
-      for (uint32_t u = 0; u < K; u++) tr += Cj[u * K + u].x;
-      d = n0 > 0.f ? sqrtf(d) / n0 : 0.f;
-      tr = t0 > 0.f ? tr / t0 - 1.f : 0.f;
-    }
-    f[sg + q] = d;
-    f[sg + 3 + q] = tr;
-  }
-}
-
-// 5. X0_s = sum_j alpha[s][j] Xc[clamp(g + j - 1)] (alpha null: coarse)
-__global__ void blend_kernel(const float *alpha, const float2 *Xc, float2 *X, uint32_t K, uint32_t S,
-                             uint32_t sg, uint32_t G) {
-  const uint64_t total = (uint64_t)S * K * K;
-  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
-       e += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t s = (uint32_t)(e / (K * K)), r = (uint32_t)(e % (K * K));
-    const uint32_t g = s / sg;
-    float2 acc = make_float2(0.f, 0.f);
-    if (!alpha) {
-      acc = Xc[(uint64_t)g * K * K + r];
-    } else {
-      for (int j = 0; j < kBlend; j++) {
-        const int gj = min(max((int)g + j - 1, 0), (int)G - 1);
-        const float a = alpha[(uint64_t)s * kBlend + j];
-        const float2 x = Xc[(uint64_t)gj * K * K + r];
-        acc.x += a * x.x;
-        acc.y += a * x.y;
-      }
-    }
-    X[e] = acc;
-  }
-}
-
-// 6. Newton-Schulz per subcarrier, one CTA of K*K threads: X <- X (2I - G X)
-__global__ void ns_kernel(const float2 *Gm, float2 *X, uint32_t K, uint32_t iters) {
-  extern __shared__ __align__(16) unsigned char nsm[];
-  float2 *g = reinterpret_cast<float2 *>(nsm), *x = g + K * K, *t = x + K * K;
-  const uint32_t s = blockIdx.x, e = threadIdx.x, r = e / K, c = e % K;
-  const bool on = e < K * K;
-  if (on) {
-    g[e] = Gm[(uint64_t)s * K * K + e];
-    x[e] = X[(uint64_t)s * K * K + e];
-  }
-  __syncthreads();
-  for (uint32_t it = 0; it < iters; it++) {
-    float2 acc = make_float2(0.f, 0.f);
-    if (on)
-      for (uint32_t k = 0; k < K; k++) acc = cfma(g[r * K + k], x[k * K + c], acc);
-    if (on) t[e] = make_float2((r == c ? 2.f : 0.f) - acc.x, -acc.y);
-    __syncthreads();
-    acc = make_float2(0.f, 0.f);
-    if (on)
-      for (uint32_t k = 0; k < K; k++) acc = cfma(x[r * K + k], t[k * K + c], acc);
-    __syncthreads();
-    if (on) x[e] = acc;
-    __syncthreads();
-  }
-  if (on) X[(uint64_t)s * K * K + e] = x[e];
-}
-
 // ||I - G_s X_s||_F per subcarrier
 __global__ void residual_kernel(const float2 *Gm, const float2 *X, float *res, uint32_t K, uint32_t S) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -262,23 +177,6 @@ __global__ void residual_kernel(const float2 *Gm, const float2 *X, float *res, u
       acc += v.x * v.x + v.y * v.y;
     }
   res[s] = sqrtf(acc);
-}
-
-// 7. W_s[b][u] = sum_v X_s[u][v] c_s[b][v] (W = G^{-1} C in the CSI layout)
-__global__ void detector_kernel(const float2 *X, const float2 *H, float2 *W, uint32_t M, uint32_t K,
-                                uint32_t S) {
-  const uint64_t total = (uint64_t)S * M * K;
-  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
-       e += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t u = (uint32_t)(e % K);
-    const uint64_t sb = e / K;  // s * M + b
-    const uint32_t s = (uint32_t)(sb / M);
-    const float2 *x = X + (uint64_t)s * K * K + (uint64_t)u * K;
-    const float2 *h = H + sb * K;
-    float2 acc = make_float2(0.f, 0.f);
-    for (uint32_t v = 0; v < K; v++) acc = cfma(x[v], h[v], acc);
-    W[e] = acc;
-  }
 }
 
 // training targets: A [S][4][4], b [S][4] from the FP64 centre inverses Yc
@@ -307,6 +205,228 @@ __global__ void targets_kernel(const double2 *Yc, const double2 *Xs, float *A, f
   }
 }
 
+// interpolation position of subcarrier s for user u: c_s = (1 - t) csi[g0]
+// + t csi[g0 + 1] (integer floor division, then one float division)
+__device__ __forceinline__ void interp_pos(uint32_t s, uint32_t u, uint32_t sg, uint32_t G, int &g0,
+                                           float &t) {
+  const int num = (int)s - (int)(u % sg);
+  int q = num >= 0 ? num / (int)sg : -(((-num) + (int)sg - 1) / (int)sg);
+  const int gmax = (int)G - 2;
+  g0 = max(0, min(q, gmax));
+  t = G > 1 ? fminf(fmaxf((float)(num - g0 * (int)sg) / (float)sg, 0.f), 1.f) : 0.f;
+}
+
+// c_s [M][K] of subcarrier s into shared memory; ig / iw: per (s, u) the
+// lower pilot group and the weight of the upper one (interp_pos, tabulated)
+__device__ __forceinline__ void interp_smem(const float2 *csi, const int *ig, const float *iw, float2 *c,
+                                            uint32_t s, uint32_t M, uint32_t K, uint32_t G) {
+  for (uint32_t e = threadIdx.x; e < M * K; e += blockDim.x) {
+    const uint32_t b = e / K, u = e % K;
+    const int g0 = ig[s * K + u];
+    const float t = iw[s * K + u];
+    const float2 a = csi[((uint64_t)g0 * M + b) * K + u];
+    const float2 d = G > 1 ? csi[((uint64_t)(g0 + 1) * M + b) * K + u] : a;
+    c[e] = make_float2((1.f - t) * a.x + t * d.x, (1.f - t) * a.y + t * d.y);
+  }
+}
+
+__global__ void interp_table_kernel(int *ig, float *iw, uint32_t K, uint32_t S, uint32_t sg, uint32_t G) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= S * K) return;
+  int g0;
+  float t;
+  interp_pos(e / K, e % K, sg, G, g0, t);
+  ig[e] = g0;
+  iw[e] = t;
+}
+
+// Gauss-Jordan inverse of the K x K matrix in the first K columns of A
+// (K x 2K, row-major, the right half set to I by the caller) by all
+// threads; returns false when a pivot is not positive
+template <typename V, typename T>
+__device__ bool gj_smem(V *A, uint32_t K, int *bad) {
+  const uint32_t W = 2 * K;
+  if (threadIdx.x == 0) *bad = 0;
+  __syncthreads();
+  for (uint32_t k = 0; k < K; k++) {
+    const T p = A[k * W + k].x;
+    if (!(p > (T)0)) {
+      if (threadIdx.x == 0) *bad = 1;
+      break;  // uniform: every thread read the same pivot
+    }
+    const T inv = (T)1 / p;
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < W; c += blockDim.x) {
+      V v = A[k * W + c];
+      v.x *= inv;
+      v.y *= inv;
+      A[k * W + c] = v;
+    }
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < K * W; e += blockDim.x) {
+      const uint32_t r = e / W, c = e % W;
+      if (r == k || c == k) continue;
+      const V f = A[r * W + k];
+      const V rk = A[k * W + c];
+      V v = A[r * W + c];
+      v.x -= f.x * rk.x - f.y * rk.y;
+      v.y -= f.x * rk.y + f.y * rk.x;
+      A[r * W + c] = v;
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < K; r += blockDim.x)
+      if (r != k) A[r * W + k] = cz<V>();
+    __syncthreads();
+  }
+  __syncthreads();
+  return *bad == 0;
+}
+
+// per subcarrier: interpolated CSI in shared memory, then its Gram
+__global__ void sub_gram_kernel(const float2 *csi, const int *ig, const float *iw, float2 *Gm, uint32_t M,
+                                uint32_t K, uint32_t G) {
+  extern __shared__ __align__(16) unsigned char sgm[];
+  float2 *c = reinterpret_cast<float2 *>(sgm);
+  const uint32_t s = blockIdx.x;
+  interp_smem(csi, ig, iw, c, s, M, K, G);
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < K * K; e += blockDim.x) {
+    const uint32_t u = e / K, v = e % K;
+    float2 acc = make_float2(0.f, 0.f);
+    for (uint32_t b = 0; b < M; b++) acc = cjfma(c[b * K + v], c[b * K + u], acc);
+    Gm[(uint64_t)s * K * K + e] = acc;
+  }
+}
+
+// per group g: ||Gc[g]||_F, and for j = -1, +1, +2 the relative distance
+// ||Gc[g+j] - Gc[g]|| / ||Gc[g]|| and trace ratio minus 1 -> st[g][6]
+__global__ void group_stats_kernel(const float2 *Gc, float *st, uint32_t K, uint32_t G) {
+  __shared__ float red[8][256];
+  const uint32_t g = blockIdx.x, KK = K * K;
+  const float2 *C0 = Gc + (uint64_t)g * KK;
+  const int js[3] = {-1, 1, 2};
+  float v[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // n0, t0, d[-1], d[1], d[2], t[-1], t[1], t[2]
+  for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x) {
+    const float2 a = C0[e];
+    const bool diag = e / K == e % K;
+    v[0] += a.x * a.x + a.y * a.y;
+    if (diag) v[1] += a.x;
+    for (int q = 0; q < 3; q++) {
+      const int gj = (int)g + js[q];
+      if (gj < 0 || gj >= (int)G) continue;
+      const float2 b = Gc[(uint64_t)gj * KK + e];
+      v[2 + q] += (b.x - a.x) * (b.x - a.x) + (b.y - a.y) * (b.y - a.y);
+      if (diag) v[5 + q] += b.x;
+    }
+  }
+  for (int i = 0; i < 8; i++) red[i][threadIdx.x] = v[i];
+  __syncthreads();
+  for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int i = 0; i < 8; i++) red[i][threadIdx.x] += red[i][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const float n0 = sqrtf(red[0][0]), t0 = red[1][0];
+    for (int q = 0; q < 3; q++) {
+      const int gj = (int)g + js[q];
+      const bool in = gj >= 0 && gj < (int)G;
+      st[g * 6 + q] = in && n0 > 0.f ? sqrtf(red[2 + q][0]) / n0 : 0.f;
+      st[g * 6 + 3 + q] = in && t0 > 0.f ? red[5 + q][0] / t0 - 1.f : 0.f;
+    }
+  }
+}
+
+// features [S][sg + 6]: one-hot offset, then the group's six statistics
+__global__ void features2_kernel(const float *st, float *F, uint32_t S, uint32_t sg) {
+  const uint32_t nf = sg + 6;
+  const uint64_t total = (uint64_t)S * nf;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = (uint32_t)(e / nf), f = (uint32_t)(e % nf);
+    F[e] = f < sg ? (f == s % sg ? 1.f : 0.f) : st[(s / sg) * 6 + (f - sg)];
+  }
+}
+
+// per subcarrier: initial iterate (coarse / learned blend / exact
+// Gauss-Jordan), Newton-Schulz steps, then the detector W_s = X C, all in
+// shared memory; X is also stored for the residual diagnostic
+__global__ void sub_detect_kernel(const float2 *csi, const int *ig, const float *iw, const float2 *Gm,
+                                  const float2 *Xc, const float *alpha, int mode, uint32_t iters,
+                                  float2 *Xout, float2 *W, uint32_t M, uint32_t K, uint32_t sg,
+                                  uint32_t G, int *flag) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ int bad;
+  const uint32_t KK = K * K;
+  float2 *g = reinterpret_cast<float2 *>(dsm), *x = g + KK, *t = x + KK, *aug = t + KK;
+  float2 *c = aug;  // K x 2K for the exact inverse, then M x K of CSI
+  const uint32_t s = blockIdx.x, grp = s / sg;
+  for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x) g[e] = Gm[(uint64_t)s * KK + e];
+  if (mode == 2) {
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < 2 * KK; e += blockDim.x) {
+      const uint32_t r = e / (2 * K), q = e % (2 * K);
+      aug[e] = q < K ? g[r * K + q] : make_float2(q - K == r ? 1.f : 0.f, 0.f);
+    }
+    __syncthreads();
+    const bool ok = gj_smem<float2, float>(aug, K, &bad);
+    if (threadIdx.x == 0 && flag) flag[s] = ok ? 0 : 1;
+    for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x) x[e] = aug[(e / K) * 2 * K + K + e % K];
+  } else {
+    for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x) {
+      float2 acc = make_float2(0.f, 0.f);
+      if (mode == 0) {
+        acc = Xc[(uint64_t)grp * KK + e];
+      } else {
+        for (int j = 0; j < kBlend; j++) {
+          const int gj = min(max((int)grp + j - 1, 0), (int)G - 1);
+          const float a = alpha[(uint64_t)s * kBlend + j];
+          const float2 v = Xc[(uint64_t)gj * KK + e];
+          acc.x += a * v.x;
+          acc.y += a * v.y;
+        }
+      }
+      x[e] = acc;
+    }
+  }
+  __syncthreads();
+  for (uint32_t it = 0; it < iters; it++) {
+    for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x) {
+      const uint32_t r = e / K, q = e % K;
+      float2 acc = make_float2(0.f, 0.f);
+      for (uint32_t k = 0; k < K; k++) acc = cfma(g[r * K + k], x[k * K + q], acc);
+      t[e] = make_float2((r == q ? 2.f : 0.f) - acc.x, -acc.y);
+    }
+    __syncthreads();
+    float2 nx[4];
+    uint32_t n = 0;
+    for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x, n++) {
+      const uint32_t r = e / K, q = e % K;
+      float2 acc = make_float2(0.f, 0.f);
+      for (uint32_t k = 0; k < K; k++) acc = cfma(x[r * K + k], t[k * K + q], acc);
+      nx[n] = acc;
+    }
+    __syncthreads();
+    n = 0;
+    for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x, n++) x[e] = nx[n];
+    __syncthreads();
+  }
+  // X transposed into t (xt[v][u]) so that the lanes of a warp, which hold
+  // consecutive users u, read consecutive words
+  for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x) {
+    if (Xout) Xout[(uint64_t)s * KK + e] = x[e];
+    t[(e % K) * K + e / K] = x[e];
+  }
+  interp_smem(csi, ig, iw, c, s, M, K, G);
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < M * K; e += blockDim.x) {
+    const uint32_t b = e / K, u = e % K;
+    float2 acc = make_float2(0.f, 0.f);
+    for (uint32_t v = 0; v < K; v++) acc = cfma(t[v * K + u], c[b * K + v], acc);
+    W[(uint64_t)s * M * K + e] = acc;
+  }
+}
+
 unsigned grid_for(uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16); }
 
 }  // namespace
@@ -317,16 +437,18 @@ using namespace mb;
 
 struct mb_lzf {
   uint32_t M, K, S, sg, G;
-  float2 *H, *Gs, *Gc, *Xc, *X;   // FP32 working set
-  float *feat, *alpha, *res;
+  float2 *Gs, *Gc, *Xc, *X;       // FP32 working set: per-subcarrier and centre Grams, inverses
+  float *feat, *alpha, *res, *stats;  // stats: per-group feature statistics [G][6]
   uint32_t *cidx;                 // centre subcarrier of each group
+  int *ig;                        // [S][K] lower pilot group of the interpolation
+  float *iw;                      // [S][K] weight of the upper pilot group
   int *flag;                      // per-inverse non-PD flags
   double2 *H64, *Gs64, *Yc64, *X64;  // FP64 training-target set (allocated on first use)
 };
 
 extern "C" mb_status mb_lzf_destroy(mb_lzf *z) {
   if (!z) return MB_BAD_ARG;
-  for (void *p : {(void *)z->H, (void *)z->Gs, (void *)z->Gc, (void *)z->Xc, (void *)z->X,
+  for (void *p : {(void *)z->ig, (void *)z->iw, (void *)z->stats, (void *)z->Gs, (void *)z->Gc, (void *)z->Xc, (void *)z->X,
                   (void *)z->feat, (void *)z->alpha, (void *)z->res, (void *)z->cidx, (void *)z->flag,
                   (void *)z->H64, (void *)z->Gs64, (void *)z->Yc64, (void *)z->X64})
     cudaFree(p);
@@ -350,8 +472,7 @@ extern "C" mb_status mb_lzf_create(uint32_t M, uint32_t K, uint32_t S, uint32_t 
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) st = record_error(e);
   };
-  const size_t smk = (size_t)S * M * K, skk = (size_t)S * K * K, gkk = (size_t)z->G * K * K;
-  alloc((void **)&z->H, sizeof(float2) * smk);
+  const size_t skk = (size_t)S * K * K, gkk = (size_t)z->G * K * K;
   alloc((void **)&z->Gs, sizeof(float2) * skk);
   alloc((void **)&z->X, sizeof(float2) * skk);
   alloc((void **)&z->Gc, sizeof(float2) * gkk);
@@ -359,6 +480,14 @@ extern "C" mb_status mb_lzf_create(uint32_t M, uint32_t K, uint32_t S, uint32_t 
   alloc((void **)&z->feat, sizeof(float) * (size_t)S * (sg + 6));
   alloc((void **)&z->alpha, sizeof(float) * (size_t)S * kBlend);
   alloc((void **)&z->res, sizeof(float) * S);
+  alloc((void **)&z->stats, sizeof(float) * 6 * z->G);
+  alloc((void **)&z->ig, sizeof(int) * (size_t)S * K);
+  alloc((void **)&z->iw, sizeof(float) * (size_t)S * K);
+  if (st == MB_OK) {
+    interp_table_kernel<<<(S * K + 255) / 256, 256>>>(z->ig, z->iw, K, S, sg, z->G);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) st = record_error(e);
+  }
   alloc((void **)&z->cidx, sizeof(uint32_t) * z->G);
   alloc((void **)&z->flag, sizeof(int) * std::max(z->G, S));
   if (st == MB_OK) {
@@ -377,21 +506,28 @@ extern "C" mb_status mb_lzf_create(uint32_t M, uint32_t K, uint32_t S, uint32_t 
 
 extern "C" uint32_t mb_lzf_num_features(uint32_t sg) { return sg + 6; }
 
-// interpolation, Grams, centre Grams and their inverses (FP32)
+// interpolated CSI and Grams per subcarrier, centre Grams and their
+// inverses, per-group feature statistics (FP32)
 static mb_status lzf_front(mb_lzf *z, const mb_c32 *csi, cudaStream_t st) {
   const uint32_t M = z->M, K = z->K, S = z->S;
-  interp_kernel<float><<<grid_for((uint64_t)S * M * K), 256, 0, st>>>(
-      reinterpret_cast<const float2 *>(csi), z->H, M, K, S, z->sg, z->G);
-  gram_kernel<float><<<S, 256, sizeof(float2) * M * K, st>>>(z->H, z->Gs, M, K);
+  sub_gram_kernel<<<S, 256, sizeof(float2) * M * K, st>>>(reinterpret_cast<const float2 *>(csi), z->ig, z->iw,
+                                                          z->Gs, M, K, z->G);
   gather_kernel<<<grid_for((uint64_t)z->G * K * K), 256, 0, st>>>(z->Gs, z->cidx, z->Gc, K, z->G);
   inverse_kernel<float><<<z->G, 256, sizeof(float2) * 2 * K * K, st>>>(z->Gc, nullptr, z->Xc, K, z->flag);
+  group_stats_kernel<<<z->G, 256, 0, st>>>(z->Gc, z->stats, K, z->G);
   MB_CUDA_TRY(cudaGetLastError());
   return MB_OK;
 }
 
+static size_t detect_smem(const mb_lzf *z) {
+  return sizeof(float2) * (3 * (size_t)z->K * z->K + std::max<size_t>(2 * (size_t)z->K * z->K,
+                                                                     (size_t)z->M * z->K));
+}
+
 static mb_status lzf_shared_mem_ok(const mb_lzf *z) {
-  // the Gram kernel stages one subcarrier's M x K channel (FP64 for targets)
-  return (size_t)z->M * z->K * sizeof(double2) <= 48 * 1024 ? MB_OK : MB_UNSUPPORTED;
+  // one subcarrier's M x K CSI is staged in shared memory (FP64 for targets)
+  return (size_t)z->M * z->K * sizeof(double2) <= 48 * 1024 && detect_smem(z) <= 48 * 1024 ? MB_OK
+                                                                                            : MB_UNSUPPORTED;
 }
 
 extern "C" mb_status mb_lzf_features(mb_lzf *z, const mb_c32 *csi, float *features, void *stream) {
@@ -400,7 +536,7 @@ extern "C" mb_status mb_lzf_features(mb_lzf *z, const mb_c32 *csi, float *featur
   cudaStream_t st = as_stream(stream);
   mb_status r = lzf_front(z, csi, st);
   if (r != MB_OK) return r;
-  features_kernel<<<(z->S + 127) / 128, 128, 0, st>>>(z->Gc, features, z->K, z->S, z->sg, z->G);
+  features2_kernel<<<grid_for((uint64_t)z->S * (z->sg + 6)), 256, 0, st>>>(z->stats, features, z->S, z->sg);
   MB_CUDA_TRY(cudaGetLastError());
   return MB_OK;
 }
@@ -414,26 +550,16 @@ extern "C" mb_status mb_lzf_run(mb_lzf *z, const mb_c32 *csi, mb_mlp *mlp, int i
   const uint32_t M = z->M, K = z->K, S = z->S;
   mb_status r = lzf_front(z, csi, st);
   if (r != MB_OK) return r;
-  if (init == MB_LZF_EXACT) {
-    inverse_kernel<float><<<S, 256, sizeof(float2) * 2 * K * K, st>>>(z->Gs, nullptr, z->X, K, z->flag);
-  } else {
-    const float *alpha = nullptr;
-    if (init == MB_LZF_LEARNED) {
-      features_kernel<<<(S + 127) / 128, 128, 0, st>>>(z->Gc, z->feat, K, S, z->sg, z->G);
-      MB_CUDA_TRY(cudaGetLastError());
-      r = mb_mlp_forward(mlp, z->feat, S, z->alpha, st);
-      if (r != MB_OK) return r;
-      alpha = z->alpha;
-    }
-    blend_kernel<<<grid_for((uint64_t)S * K * K), 256, 0, st>>>(alpha, z->Xc, z->X, K, S, z->sg, z->G);
-  }
-  MB_CUDA_TRY(cudaGetLastError());
-  if (ns_iters) {
-    ns_kernel<<<S, ((K * K + 31) / 32) * 32, 3 * sizeof(float2) * K * K, st>>>(z->Gs, z->X, K, ns_iters);
+  if (init == MB_LZF_LEARNED) {
+    features2_kernel<<<grid_for((uint64_t)S * (z->sg + 6)), 256, 0, st>>>(z->stats, z->feat, S, z->sg);
     MB_CUDA_TRY(cudaGetLastError());
+    r = mb_mlp_forward(mlp, z->feat, S, z->alpha, st);
+    if (r != MB_OK) return r;
   }
-  detector_kernel<<<grid_for((uint64_t)S * M * K), 256, 0, st>>>(z->X, z->H, reinterpret_cast<float2 *>(W),
-                                                                 M, K, S);
+  const size_t smem = detect_smem(z);
+  sub_detect_kernel<<<S, 256, smem, st>>>(reinterpret_cast<const float2 *>(csi), z->ig, z->iw, z->Gs, z->Xc,
+                                          init == MB_LZF_LEARNED ? z->alpha : nullptr, init, ns_iters, z->X,
+                                          reinterpret_cast<float2 *>(W), M, K, z->sg, z->G, z->flag);
   MB_CUDA_TRY(cudaGetLastError());
   return MB_OK;
 }

@@ -11,11 +11,14 @@
 // see lzf.cu), averaged over the batch.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <random>
 #include <vector>
 
 #include "common.cuh"
+#include "tc.cuh"
 
 namespace mb {
 namespace {
@@ -142,6 +145,173 @@ __global__ void adam_kernel(float *p, const float *g, float *m, float *v, uint64
   m[i] = mi;
   v[i] = vi;
   p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// Inference: all three layers in one kernel, ROWS samples per CTA with the
+// activations in shared memory; thread n of a layer owns output column n
+// (coalesced BF16 weight loads, activations broadcast from shared memory).
+template <int ROWS>
+__global__ void __launch_bounds__(256) mlp_infer_kernel(const float *x, int B, int I, int W, int O,
+                                                        const __nv_bfloat16 *W1, const float *b1,
+                                                        const __nv_bfloat16 *W2, const float *b2,
+                                                        const __nv_bfloat16 *W3, const float *b3,
+                                                        float *y) {
+  extern __shared__ __align__(16) float msm[];
+  // a0 padded to a multiple of 4 floats so that a1 / a2 rows are 16-byte aligned
+  float *a0 = msm, *a1 = a0 + ((ROWS * I + 3) & ~3), *a2 = a1 + ROWS * W;
+  const int r0 = blockIdx.x * ROWS, nr = min(ROWS, B - r0);
+  for (int e = threadIdx.x; e < ROWS * I; e += blockDim.x) {
+    const int r = e / I;
+    a0[e] = r < nr ? x[(size_t)(r0 + r) * I + e % I] : 0.f;
+  }
+  __syncthreads();
+  // hidden layers: relu(a W + b)
+  for (int layer = 0; layer < 2; layer++) {
+    const float *ain = layer == 0 ? a0 : a1;
+    float *aout = layer == 0 ? a1 : a2;
+    const __nv_bfloat16 *Wl = layer == 0 ? W1 : W2;
+    const float *bl = layer == 0 ? b1 : b2;
+    const int K = layer == 0 ? I : W;
+    for (int n = threadIdx.x; n < W; n += blockDim.x) {
+      float acc[ROWS];
+#pragma unroll
+      for (int r = 0; r < ROWS; r++) acc[r] = bl[n];
+      for (int k0 = 0; k0 < K; k0 += 16) {
+        // sixteen weight loads in flight, then their products
+        float w[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          w[j] = k0 + j < K ? __bfloat162float(Wl[(size_t)(k0 + j) * W + n]) : 0.f;
+        if ((K & 15) == 0) {
+          // activations four at a time (16-byte shared-memory loads)
+#pragma unroll
+          for (int j = 0; j < 16; j += 4) {
+#pragma unroll
+            for (int r = 0; r < ROWS; r++) {
+              const float4 a4 = *reinterpret_cast<const float4 *>(ain + r * K + k0 + j);
+              acc[r] = fmaf(a4.x, w[j], acc[r]);
+              acc[r] = fmaf(a4.y, w[j + 1], acc[r]);
+              acc[r] = fmaf(a4.z, w[j + 2], acc[r]);
+              acc[r] = fmaf(a4.w, w[j + 3], acc[r]);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            if (k0 + j >= K) break;
+#pragma unroll
+            for (int r = 0; r < ROWS; r++) acc[r] = fmaf(ain[r * K + k0 + j], w[j], acc[r]);
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < ROWS; r++) aout[r * W + n] = fmaxf(acc[r], 0.f);
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < nr * O; e += blockDim.x) {
+    const int r = e / O, o = e % O;
+    float acc = b3[o];
+    for (int k0 = 0; k0 < W; k0 += 16) {
+      float w[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) w[j] = k0 + j < W ? __bfloat162float(W3[(size_t)(k0 + j) * O + o]) : 0.f;
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+        if (k0 + j < W) acc = fmaf(a2[r * W + k0 + j], w[j], acc);
+    }
+    y[(size_t)(r0 + r) * O + o] = acc;
+  }
+}
+
+// Inference with every weight staged once per CTA in shared memory (16-byte
+// loads, all in flight together), then ROWS samples at a time through the
+// three layers; CTAs walk the row blocks blockIdx.x, + gridDim.x, ...
+// ws holds W1 [I][W], W2 [W][W], W3 [W][O] (BF16) back to back.
+template <int ROWS>
+__global__ void __launch_bounds__(256) mlp_infer_smem_kernel(const float *x, int B, int I, int W, int O,
+                                                             const __nv_bfloat16 *W1, const __nv_bfloat16 *W2,
+                                                             const __nv_bfloat16 *W3, const float *b1,
+                                                             const float *b2, const float *b3, float *y,
+                                                             int *err) {
+  extern __shared__ __align__(16) unsigned char ism[];
+  const size_t n1 = (size_t)I * W, n2 = (size_t)W * W, n3 = (size_t)W * O;
+  const size_t nw = (n1 + n2 + n3 + 7) & ~(size_t)7;
+  __nv_bfloat16 *ws = reinterpret_cast<__nv_bfloat16 *>(ism);
+  float *a0 = reinterpret_cast<float *>(ism + nw * 2);
+  float *a1 = a0 + ((ROWS * I + 3) & ~3), *a2 = a1 + ROWS * W;
+  // stage the weights with three bulk copies (each block a multiple of 16
+  // bytes and 16-byte aligned: W % 8 == 0, checked by the launcher)
+  __shared__ __align__(8) uint64_t wbar;
+  __shared__ int wok;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&wbar, 1);
+    tc::fence_mbar_init();
+    tc::mbar_arrive_expect_tx(&wbar, (uint32_t)((n1 + n2 + n3) * 2));
+    tc::bulk_g2s(ws, W1, (uint32_t)(n1 * 2), &wbar);
+    tc::bulk_g2s(ws + n1, W2, (uint32_t)(n2 * 2), &wbar);
+    tc::bulk_g2s(ws + n1 + n2, W3, (uint32_t)(n3 * 2), &wbar);
+    wok = tc::mbar_wait(&wbar, 0) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!wok) {
+    if (threadIdx.x == 0 && err) atomicOr(err, tc::kErrTimeout);
+    return;
+  }
+  const __nv_bfloat16 *s1 = ws, *s2 = ws + n1, *s3 = ws + n1 + n2;
+  for (int r0 = blockIdx.x * ROWS; r0 < B; r0 += gridDim.x * ROWS) {
+    const int nr = min(ROWS, B - r0);
+    for (int e = threadIdx.x; e < ROWS * I; e += blockDim.x) {
+      const int r = e / I;
+      a0[e] = r < nr ? x[(size_t)(r0 + r) * I + e % I] : 0.f;
+    }
+    __syncthreads();
+    for (int layer = 0; layer < 2; layer++) {
+      const float *ain = layer == 0 ? a0 : a1;
+      float *aout = layer == 0 ? a1 : a2;
+      const __nv_bfloat16 *Wl = layer == 0 ? s1 : s2;
+      const float *bl = layer == 0 ? b1 : b2;
+      const int K = layer == 0 ? I : W;
+      for (int n = threadIdx.x; n < W; n += blockDim.x) {
+        float acc[ROWS];
+#pragma unroll
+        for (int r = 0; r < ROWS; r++) acc[r] = bl[n];
+        int k = 0;
+        if ((K & 3) == 0) {
+          // four activations per 16-byte shared-memory load
+          for (; k < K; k += 4) {
+            const float w0 = __bfloat162float(Wl[(size_t)k * W + n]);
+            const float w1 = __bfloat162float(Wl[(size_t)(k + 1) * W + n]);
+            const float w2 = __bfloat162float(Wl[(size_t)(k + 2) * W + n]);
+            const float w3 = __bfloat162float(Wl[(size_t)(k + 3) * W + n]);
+#pragma unroll
+            for (int r = 0; r < ROWS; r++) {
+              const float4 a4 = *reinterpret_cast<const float4 *>(ain + r * K + k);
+              acc[r] = fmaf(a4.x, w0, acc[r]);
+              acc[r] = fmaf(a4.y, w1, acc[r]);
+              acc[r] = fmaf(a4.z, w2, acc[r]);
+              acc[r] = fmaf(a4.w, w3, acc[r]);
+            }
+          }
+        }
+        for (; k < K; k++) {
+          const float w = __bfloat162float(Wl[(size_t)k * W + n]);
+#pragma unroll
+          for (int r = 0; r < ROWS; r++) acc[r] = fmaf(ain[r * K + k], w, acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < ROWS; r++) aout[r * W + n] = fmaxf(acc[r], 0.f);
+      }
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < nr * O; e += blockDim.x) {
+      const int r = e / O, o = e % O;
+      float acc = b3[o];
+      for (int k = 0; k < W; k++) acc = fmaf(a2[r * W + k], __bfloat162float(s3[(size_t)k * O + o]), acc);
+      y[(size_t)(r0 + r) * O + o] = acc;
+    }
+    __syncthreads();
+  }
 }
 
 __global__ void to_bf16_kernel(const float *x, __nv_bfloat16 *y, uint64_t n) {
@@ -296,8 +466,45 @@ extern "C" mb_status mb_mlp_forward(mb_mlp *n, const float *x, uint32_t batch, f
                                     void *stream) {
   if (!n || !x || !y) return MB_BAD_ARG;
   if (batch == 0) return MB_OK;
-  if (batch > n->max_batch) return MB_BAD_SHAPE;
-  MB_CUDA_TRY(mlp_fwd(n, x, batch, y, as_stream(stream)));
+  constexpr int kRows = 8;
+  const __nv_bfloat16 *wb = n->wb;
+  {
+    // weights resident in shared memory when they fit (one CTA per SM)
+    const size_t nw = ((size_t)n->n_in * n->width + (size_t)n->width * n->width +
+                       (size_t)n->width * n->n_out + 7) & ~(size_t)7;
+    const size_t smem = nw * 2 + sizeof(float) * (((kRows * n->n_in + 3) & ~3u) + 2 * kRows * n->width);
+    int dev = 0, maxs = 0, sms = 0;
+    MB_CUDA_TRY(cudaGetDevice(&dev));
+    MB_CUDA_TRY(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    MB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (smem + 1024 <= (size_t)maxs && n->width % 8 == 0) {
+      static std::atomic<uint64_t> configured{0};
+      const uint64_t bit = 1ull << (dev & 63);
+      if (!(configured.load() & bit)) {
+        MB_CUDA_TRY(cudaFuncSetAttribute(mlp_infer_smem_kernel<kRows>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, maxs - 1024));
+        configured.fetch_or(bit);
+      }
+      const unsigned grid = (unsigned)std::min<uint64_t>((batch + kRows - 1) / kRows, (uint64_t)sms);
+      mlp_infer_smem_kernel<kRows><<<grid, 256, smem, as_stream(stream)>>>(
+          x, (int)batch, (int)n->n_in, (int)n->width, (int)n->n_out, wb + n->off[0], wb + n->off[2],
+          wb + n->off[4], n->p + n->off[1], n->p + n->off[3], n->p + n->off[5], y,
+          device_tables() ? device_tables()->err : nullptr);
+      MB_CUDA_TRY(cudaGetLastError());
+      return MB_OK;
+    }
+  }
+  const size_t smem = sizeof(float) * (((kRows * n->n_in + 3) & ~3u) + 2 * kRows * n->width);
+  if (smem > 48 * 1024) {
+    // wide networks: the tiled products of the training path
+    if (batch > n->max_batch) return MB_BAD_SHAPE;
+    MB_CUDA_TRY(mlp_fwd(n, x, batch, y, as_stream(stream)));
+    return MB_OK;
+  }
+  mlp_infer_kernel<kRows><<<(batch + kRows - 1) / kRows, 256, smem, as_stream(stream)>>>(
+      x, (int)batch, (int)n->n_in, (int)n->width, (int)n->n_out, wb + n->off[0], n->p + n->off[1],
+      wb + n->off[2], n->p + n->off[3], wb + n->off[4], n->p + n->off[5], y);
+  MB_CUDA_TRY(cudaGetLastError());
   return MB_OK;
 }
 
