@@ -219,13 +219,59 @@ def cpu_baseline(cfg, slot_np, seconds):
 
 
 def run_reference(args, rank, world):
+    """The reference arm.  The reference implements this path only as CUDA
+    operators (cuFFT, cuBLAS/cuSOLVER, its SIMT equalizer); where they were
+    built from the reference tree (oracle/_ref, kind "reference") they run on
+    this GPU in process.cc's order on the same slot shapes with int16
+    samples (the reference FFT takes integer IQ only).  Otherwise the FP32
+    host C++/OpenMP restatement (kind "port") runs on all host cores.  Rank 0
+    only."""
     from megastation_b200 import datagen
     if rank != 0:
         return
     cfg = datagen.CellConfig(**WORKLOAD)
+    from oracle import ref_ops
+    cb, zeros, stride = cfg.ldpc()
+    if ref_ops.available():
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        c16 = datagen.CellConfig(**{**cfg.__dict__, "iq_dtype": "int16"})
+        R = max(2, args.rotate)
+        iqs = [torch.from_numpy(datagen.make_slot(datagen.CellConfig(**{**c16.__dict__, "seed": c16.seed + r}))["iq"]
+                                ).cuda() for r in range(R)]
+        llr = [torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda") for _ in range(2)]
+        ref = ref_ops.RefSlot(cfg.M, cfg.K, cfg.N, cfg.S, cfg.sg, cfg.Qm, cfg.P, cfg.U, cb, zeros, stride)
+        stream = torch.cuda.Stream()
+        for k in range(max(args.warmup, 3)):
+            ref.uplink(iqs[k % R].data_ptr(), llr[k % 2].data_ptr(), stream.cuda_stream)
+        stream.synchronize()
+        clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+        clocks.start()
+        time.sleep(0.3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(args.steps):
+            ref.uplink(iqs[k % R].data_ptr(), llr[k % 2].data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1)
+        v = args.steps / (ms / 1e3)
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded, megastation_b200.datagen), int16 samples",
+                "config": {**workload_config(cfg, args), "iq_dtype": "int16 (the reference FFT takes integer IQ)"},
+                "clocks": clk,
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": 0, "kind": "reference",
+                                 "sample": f"{args.steps} slots through the reference's own CUDA operators "
+                                           "(fft_op.cu, beamform.cu, equalize.cu built from the reference "
+                                           "tree) on this GPU, process.cc order, one stream"},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     d = datagen.make_slot(cfg)
     from oracle import oracle as orc
-    cb, zeros, stride = cfg.ldpc()
     ps = orc.pilot_sign(cfg.S)
     threads = os.cpu_count() or 1
     # bounded sample per step: one full slot per step
