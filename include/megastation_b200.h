@@ -325,7 +325,9 @@ mb_status mb_slot_timing(mb_slot *slot, uint32_t max_calls);
 mb_status mb_slot_stage_ms(mb_slot *slot, double *out8);
 
 /* Device views of the slot's internal buffers (for inspection and tests):
- * CSI/W [G][M][K], precoder [G][K][M]. */
+ * CSI/W [G][M][K], precoder [G][K][M].  In the mixed-precision path without
+ * downlink symbols (D = 0) the equalizer reads only the detector images, and
+ * the CSI/W buffer is left as ZF scratch. */
 mb_status mb_slot_buffers(mb_slot *slot, mb_c32 **csi, mb_c32 **precoder);
 
 /* -------------------------------------------------------- batched cells --- */

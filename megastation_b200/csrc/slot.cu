@@ -244,7 +244,8 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   float2 *prec = c.D ? s->precoder : nullptr;
   if (mixed) {
     mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, 0};
-    r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, st);
+    // W in FP32 only feeds the downlink precoder; the equalizer reads the image
+    r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, st, prec != nullptr);
     if (r == MB_OK && prec) r = precoder_launch(s->csi, prec, c.M, c.K, s->G, st);
   } else {
     r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, st);

@@ -11,11 +11,13 @@ mb_status zf_fill_tail(float2 *csi, uint32_t groups, uint32_t S, uint32_t sg,
 mb_status zf_chol(float2 *csi, float2 *precoder, uint32_t groups, uint32_t M,
                   uint32_t K, bool dbl, int32_t *status, float *cond,
                   cudaStream_t st);
-// mixed precision ZF (zf_mixed.cu): W in place (FP32) plus the detector
-// images for the tensor-core equalizer in img_w (zf_mixed_scratch_bytes)
+// mixed precision ZF (zf_mixed.cu): the detector images for the
+// tensor-core equalizer in img_w (zf_mixed_scratch_bytes) and, with write_w,
+// W in place (FP32); without it csi is left as scratch
 uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K);
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
-                       const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st);
+                       const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
+                       bool write_w = true);
 mb_status precoder_launch(const float2 *W, float2 *P, uint32_t M, uint32_t K,
                           uint32_t groups, cudaStream_t st);
 size_t zf_chol_smem(uint32_t M, uint32_t K, bool dbl);

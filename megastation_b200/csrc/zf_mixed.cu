@@ -47,6 +47,7 @@ struct ZfmParams {
   uint32_t M, K, Mp, nkt, ns_iters;
   uint32_t nh;        // plane-0 k tiles: Mp / 64
   uint32_t resident;  // 1: all nh hi tiles stay in shared memory for W = X C
+  uint32_t write_w;   // 1: also store W (FP32, CSI layout); 0: the detector image only
   float cond_thr;
 };
 
@@ -125,7 +126,7 @@ __device__ __forceinline__ bool gj_inverse(const float2 *G, float2 *X, uint32_t 
       float2 *pr = prow + (k & 1) * 2 * KP;
       if (i == k) {
         if (!(f.x > 0.f)) *bad = 1;
-        const float inv = 1.f / f.x;
+        const float inv = __frcp_rn(f.x);
 #pragma unroll
         for (int m = 0; m < NC; m++) {
           v[m].x *= inv;
@@ -532,7 +533,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
           }
           *reinterpret_cast<uint4 *>(imgw + img_off(r, kk, MM)) = make_uint4(p0[0], p0[1], p0[2], p0[3]);
           *reinterpret_cast<uint4 *>(imgw + img_off(r, Mp + kk, MM)) = make_uint4(p1[0], p1[1], p1[2], p1[3]);
-          if (!(r & 1) && u < K) {
+          if (q.write_w && !(r & 1) && u < K) {
 #pragma unroll
             for (int e = 0; e < 8; e++) {
               const uint32_t b = kk + e;
@@ -625,7 +626,8 @@ uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K) {
 }
 
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
-                       const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st) {
+                       const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
+                       bool write_w) {
   if (K == 0 || K > 64) return MB_UNSUPPORTED;
   const TcShape s = tc_shape(M, K);
   const DeviceTables *tab = device_tables();
@@ -667,6 +669,7 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
   const size_t avail = (size_t)maxs - (size_t)static_smem[which].load();
   // keep every hi tile in shared memory when it fits, else stream two
   q.resident = zfm_smem(K, s.MM, q.nh) <= avail ? 1 : 0;
+  q.write_w = write_w ? 1 : 0;
   const size_t smem = zfm_smem(K, s.MM, q.resident ? q.nh : 2);
   if (smem > avail) return MB_UNSUPPORTED;
   if (groups == 0) return MB_OK;
