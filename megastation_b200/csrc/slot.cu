@@ -35,7 +35,8 @@ struct mb_slot {
   uint32_t eq_cols;   // tensor-core equalizer columns per CTA (0: 128)
   float2 *precoded;   // [D][M][N]
   cudaStream_t side;
-  cudaEvent_t ev_fork, ev_join;
+  cudaStream_t crit;  // pilot FFT -> ZF: the critical path, at the highest stream priority
+  cudaEvent_t ev_fork, ev_join, ev_crit;
   // captured uplink slots, one per (input, outputs, stream) pointer set,
   // least recently used evicted beyond kGraphCache entries
   struct GraphEntry {
@@ -121,8 +122,10 @@ extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   cudaFree(s->img_w);
   cudaFree(s->precoded);
   if (s->side) cudaStreamDestroy(s->side);
+  if (s->crit) cudaStreamDestroy(s->crit);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->ev_crit) cudaEventDestroy(s->ev_crit);
   delete s;
   return MB_OK;
 }
@@ -178,9 +181,16 @@ static mb_status slot_create(const mb_cell_desc *cell, bool sb_cap_all, mb_slot 
     alloc((void **)&s->y, sizeof(float2) * (size_t)s->sb_cap * c.M * c.S);
   }
   if (st == MB_OK) {
-    cudaError_t e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+    // the uplink FFT batch that overlaps the ZF runs at the lowest priority,
+    // the pilot FFT and ZF it overlaps at the highest (CTAs of the critical
+    // path are scheduled first whenever both are pending)
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, least);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->crit, cudaStreamNonBlocking, greatest);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_crit, cudaEventDisableTiming);
     if (e != cudaSuccess) st = record_error(e);
   }
   if (st == MB_OK && s->csi) {
@@ -234,23 +244,34 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     if (r != MB_OK) return r;
     MB_CUDA_TRY(cudaEventRecord(s->ev_join, s->side));
   }
-  // pilots -> CSI -> W (+ precoder)
+  // pilots -> CSI -> W (+ precoder) on the high-priority stream (the slot
+  // stream itself while timing)
+  cudaStream_t cs = st;
+  if (!mk) {
+    if (!c.U) MB_CUDA_TRY(cudaEventRecord(s->ev_fork, st));
+    MB_CUDA_TRY(cudaStreamWaitEvent(s->crit, s->ev_fork, 0));
+    cs = s->crit;
+  }
   MARK(mk->pilot_b);
-  r = mb_fft_pilot(s->fft, iq, c.iq_dtype, c.P, 0, reinterpret_cast<mb_c32 *>(s->csi), st);
+  r = mb_fft_pilot(s->fft, iq, c.iq_dtype, c.P, 0, reinterpret_cast<mb_c32 *>(s->csi), cs);
   if (r != MB_OK) return r;
   MARK(mk->pilot);
-  r = zf_fill_tail(s->csi, s->G, c.S, c.sg, c.M, c.K, st);
+  r = zf_fill_tail(s->csi, s->G, c.S, c.sg, c.M, c.K, cs);
   if (r != MB_OK) return r;
   float2 *prec = c.D ? s->precoder : nullptr;
   if (mixed) {
     mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, 0};
     // W in FP32 only feeds the downlink precoder; the equalizer reads the image
-    r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, st, prec != nullptr);
-    if (r == MB_OK && prec) r = precoder_launch(s->csi, prec, c.M, c.K, s->G, st);
+    r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr);
+    if (r == MB_OK && prec) r = precoder_launch(s->csi, prec, c.M, c.K, s->G, cs);
   } else {
-    r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, st);
+    r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, cs);
   }
   if (r != MB_OK) return r;
+  if (!mk) {
+    MB_CUDA_TRY(cudaEventRecord(s->ev_crit, s->crit));
+    MB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_crit, 0));
+  }
   MARK(mk->zf);
   if (!c.U) {
     MARK(mk->end);
@@ -322,7 +343,8 @@ extern "C" mb_status mb_slot_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     }
     if (e != cudaSuccess) return record_error(e);
     cudaGraphExec_t exec = nullptr;
-    e = cudaGraphInstantiate(&exec, g, 0);
+    // kernel nodes keep the priority of the stream they were captured on
+    e = cudaGraphInstantiate(&exec, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return record_error(e);
     if (s->graphs.size() >= kGraphCache) {
@@ -506,7 +528,7 @@ static mb_status cells_launch(mb_cells *cs, const void *const *iq, uint16_t *con
       return r != MB_OK ? r : record_error(ce != cudaSuccess ? ce : ee);
     }
     cudaGraphExec_t exec = nullptr;
-    ce = cudaGraphInstantiate(&exec, g, 0);
+    ce = cudaGraphInstantiate(&exec, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (ce != cudaSuccess) return record_error(ce);
     constexpr size_t kGraphCache = 8;
