@@ -37,6 +37,7 @@ struct FftParams {
   uint64_t rows;         // n_sym * M
   uint32_t M, S, start, K, sg, ue_start;
   uint32_t S_pad;        // kUplinkLP row pitch (elements)
+  uint32_t tail_rem;     // kPilot: S % sg when the short last group is filled (0: off)
   int in_dtype, out_dtype;
 };
 
@@ -239,6 +240,10 @@ __device__ __forceinline__ void epilogue(const FftParams &p, const RowCtx &c, ui
         const float2 ps = __ldg(p.pilot + i);
         const float2 e = make_float2(v.x * ps.x + v.y * ps.y, v.x * ps.y - v.y * ps.x);
         reinterpret_cast<float2 *>(p.out)[((uint64_t)g * p.M + c.b) * p.K + u] = e;
+        // a user with no pilot in the short last group takes its estimate
+        // from group G-2 (the slot's tail rule)
+        if (p.tail_rem && g + 2 == (p.S + p.sg - 1) / p.sg && i - g * p.sg >= p.tail_rem)
+          reinterpret_cast<float2 *>(p.out)[((uint64_t)(g + 1) * p.M + c.b) * p.K + u] = e;
       }
     }
   } else {
@@ -519,6 +524,28 @@ extern "C" mb_status mb_fft_pilot(mb_fft *f, const void *iq, int iq_dtype,
   p.ue_start = ue_start;
   p.in_dtype = iq_dtype;
   return launch_fft<kPilot>(f->logn, p, as_stream(stream));
+}
+
+mb_status mb::fft_pilot_fill(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym, mb_c32 *csi,
+                             cudaStream_t st) {
+  if (!f || !iq || !csi || !dtype_ok(iq_dtype)) return MB_BAD_ARG;
+  if (!f->pilot) return MB_BAD_SHAPE;
+  FftParams p{};
+  p.in = iq;
+  p.out = csi;
+  p.tw = f->tw;
+  p.pilot = f->pilot;
+  p.rows = (uint64_t)n_sym * f->d.bs_num;
+  p.M = f->d.bs_num;
+  p.S = f->d.ofdm_num;
+  p.start = f->d.ofdm_start;
+  p.K = f->d.ue_num;
+  p.sg = f->d.sc_group;
+  p.ue_start = 0;
+  const uint32_t G = (p.S + p.sg - 1) / p.sg;
+  p.tail_rem = G >= 2 ? p.S % p.sg : 0;
+  p.in_dtype = iq_dtype;
+  return launch_fft<kPilot>(f->logn, p, st);
 }
 
 extern "C" mb_status mb_ifft_downlink(mb_fft *f, const mb_c32 *in,

@@ -253,11 +253,10 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     cs = s->crit;
   }
   MARK(mk->pilot_b);
-  r = mb_fft_pilot(s->fft, iq, c.iq_dtype, c.P, 0, reinterpret_cast<mb_c32 *>(s->csi), cs);
+  // pilot FFT with the short last group's tail fill in its epilogue
+  r = fft_pilot_fill(s->fft, iq, c.iq_dtype, c.P, reinterpret_cast<mb_c32 *>(s->csi), cs);
   if (r != MB_OK) return r;
   MARK(mk->pilot);
-  r = zf_fill_tail(s->csi, s->G, c.S, c.sg, c.M, c.K, cs);
-  if (r != MB_OK) return r;
   float2 *prec = c.D ? s->precoder : nullptr;
   if (mixed) {
     mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, 0};
