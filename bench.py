@@ -116,6 +116,23 @@ class ClockSampler:
                 "power_w_max": max(power) if power else None}
 
 
+def max_over_ranks(ms, dist, device="cuda"):
+    """The slowest rank's time (every rank takes this collective step at the
+    same point, in warm-up and timing alike); ms itself with one process."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, steps, ms):
+    """Whole-job throughput: every rank ran `steps` slots of its own stream
+    (weak scaling), the job took the slowest rank's `ms`."""
+    return world * steps / (ms / 1e3)
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -694,21 +711,14 @@ def main():
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1e3)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    value = job_value(world, args.steps, ms)
     plain = None
     if args.precision == "mixed" and not args.no_plain:
         pms = time_slots(slot, cfg, "fp32", args.sym_batch, iq_dev, llr, hard, stream, args.steps,
                          args.warmup, dist)
-        if dist:
-            t = torch.tensor([pms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            pms = float(t.item())
-        pv = world * args.steps / (pms / 1e3)
+        pms = max_over_ranks(pms, dist)
+        pv = job_value(world, args.steps, pms)
         plain = {"value": pv, "unit": UNIT, "us_per_slot": 1e3 * pms / args.steps,
                  "speedup_mixed_over_plain": value / pv}
     evm = None if args.no_evm or rank != 0 else evm_report(cfg, d, args.sym_batch)
@@ -778,12 +788,8 @@ def main():
             dist.barrier()
         e2e_steps(args.steps, a0, a1)
         torch.cuda.synchronize()
-        ems = a0.elapsed_time(a1)
-        if dist:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": world * args.steps / (ems / 1e3), "unit": UNIT,
+        ems = max_over_ranks(a0.elapsed_time(a1), dist)
+        e2e = {"value": job_value(world, args.steps, ems), "unit": UNIT,
                "h2d_bytes_per_step": iq_host.numel() * iq_host.element_size(),
                "d2h_bytes_per_step": llr[0].numel() * 2 + hard[0].numel(),
                "pipeline": "double-buffered: H2D of slot k+1 and D2H of slot k-1 overlap slot k"}
