@@ -183,16 +183,19 @@ __global__ void __launch_bounds__(256) precode_kernel(const PcParams p) {
   const uint32_t b_base = blockIdx.z * BT * TB;
   const int tid = threadIdx.x, tc = tid % CT, tb = tid / CT;
   if (g == G) {
-    // guard bins: subcarrier index i in [S, N) maps to bin (i+start+N/2)%N
+    // guard bins: subcarrier indices i in [S, N) map to the bins
+    // (i + start + N/2) % N, one run of N - S bins per row that may wrap
+    // around N: zero the runs of this CTA's rows, a warp per row
     const uint32_t nb = min((uint32_t)(BT * TB), p.M - b_base);
     const uint32_t ng = p.N - p.S;
-    const uint64_t total = (uint64_t)nl * nb * ng;
-    for (uint64_t e = tid; e < total; e += blockDim.x) {
-      uint32_t i = p.S + (uint32_t)(e % ng);
-      uint64_t r = e / ng;
-      uint32_t b = b_base + (uint32_t)(r % nb), l = l0 + (uint32_t)(r / nb);
-      uint32_t k = (i + p.start + p.N / 2) % p.N;
-      p.out[((uint64_t)l * p.M + b) * p.N + k] = make_float2(0.f, 0.f);
+    const uint32_t k0 = (p.S + p.start + p.N / 2) % p.N;
+    const uint32_t n1 = min(ng, p.N - k0);  // bins k0 .. k0 + n1 - 1, then 0 .. ng - n1 - 1
+    const int warp = tid / 32, lane = tid % 32;
+    for (uint32_t r = warp; r < nl * nb; r += blockDim.x / 32) {
+      const uint32_t b = b_base + r % nb, l = l0 + r / nb;
+      float2 *row = p.out + ((uint64_t)l * p.M + b) * p.N;
+      for (uint32_t e = lane; e < n1; e += 32) row[k0 + e] = make_float2(0.f, 0.f);
+      for (uint32_t e = lane; e < ng - n1; e += 32) row[e] = make_float2(0.f, 0.f);
     }
     return;
   }

@@ -206,11 +206,26 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
   }
   const float inv = 1.0f / red[0];
-  for (uint32_t e = threadIdx.x; e < M * K; e += blockDim.x) {
-    uint32_t u = e / M, b = e % M;
-    float2 v = wg[(uint64_t)b * K + u];
-    pg[e] = make_float2(v.x * inv, v.y * inv);
-  }
+  // P[u][b] = W[b][u] * inv through 32 x 32 shared-memory tiles, so both the
+  // reads (along u) and the writes (along b) are coalesced
+  __shared__ float2 tile[32][33];
+  const uint32_t tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 8 rows of 32
+  for (uint32_t b0 = 0; b0 < M; b0 += 32)
+    for (uint32_t u0 = 0; u0 < K; u0 += 32) {
+      __syncthreads();
+      for (uint32_t r = ty; r < 32; r += 8) {
+        const uint32_t b = b0 + r, u = u0 + tx;
+        tile[r][tx] = (b < M && u < K) ? wg[(uint64_t)b * K + u] : make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+      for (uint32_t r = ty; r < 32; r += 8) {
+        const uint32_t u = u0 + r, b = b0 + tx;
+        if (u < K && b < M) {
+          const float2 v = tile[tx][r];
+          pg[(uint64_t)u * M + b] = make_float2(v.x * inv, v.y * inv);
+        }
+      }
+    }
 }
 
 size_t zf_chol_smem(uint32_t M, uint32_t K, bool dbl) {
