@@ -27,6 +27,7 @@ struct mb_slot {
   mb_scrambler *scr;
   float2 *csi;        // [G][M][K]: CSI, then W in place
   float2 *precoder;   // [G][K][M]
+  float *wmax;        // [G] max |W| per group (mixed path with a downlink)
   float2 *y;          // [sym_batch][M][S] uplink FFT output (FP32 path)
   void *y_lp;         // [sym_batch][re|im][M][S_pad] BF16 (mixed path)
   void *img_w;        // detector images for the tensor-core equalizer
@@ -117,6 +118,7 @@ extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   if (s->scr) mb_scrambler_destroy(s->scr);
   cudaFree(s->csi);
   cudaFree(s->precoder);
+  cudaFree(s->wmax);
   cudaFree(s->y);
   cudaFree(s->y_lp);
   cudaFree(s->img_w);
@@ -163,6 +165,7 @@ static mb_status slot_create(const mb_cell_desc *cell, bool sb_cap_all, mb_slot 
   const size_t gmk = (size_t)s->G * c.M * c.K;
   alloc((void **)&s->csi, sizeof(float2) * gmk);
   alloc((void **)&s->precoder, sizeof(float2) * gmk);
+  if (c.D) alloc((void **)&s->wmax, sizeof(float) * s->G);
   alloc((void **)&s->precoded, sizeof(float2) * (size_t)c.D * c.M * c.N);
   const bool mixed = c.zf_precision == MB_ZF_MIXED;
   if (mixed && st == MB_OK && !equalize_tc_supported(c.K, c.sg, s->c.sym_batch))
@@ -261,8 +264,9 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   if (mixed) {
     mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, 0};
     // W in FP32 only feeds the downlink precoder; the equalizer reads the image
-    r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr);
-    if (r == MB_OK && prec) r = precoder_launch(s->csi, prec, c.M, c.K, s->G, cs);
+    r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr,
+                     s->wmax);
+    if (r == MB_OK && prec) r = precoder_scale(s->csi, prec, s->wmax, c.M, c.K, s->G, cs);
   } else {
     r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, cs);
   }

@@ -228,6 +228,32 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// P[g][u][b] = W[g][b][u] / wmax[g]: one CTA per (group, 32 x 32 tile),
+// transposed through shared memory
+__global__ void __launch_bounds__(256)
+    precoder_scale_kernel(const float2 *W, float2 *P, const float *wmax, uint32_t M, uint32_t K,
+                          uint32_t tiles_b) {
+  __shared__ float2 tile[32][33];
+  const uint32_t g = blockIdx.x;
+  const uint32_t b0 = (blockIdx.y % tiles_b) * 32, u0 = (blockIdx.y / tiles_b) * 32;
+  const uint32_t tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  const float2 *wg = W + (uint64_t)g * M * K;
+  float2 *pg = P + (uint64_t)g * M * K;
+  const float inv = 1.0f / wmax[g];  // as precoder_kernel
+  for (uint32_t r = ty; r < 32; r += 8) {
+    const uint32_t b = b0 + r, u = u0 + tx;
+    tile[r][tx] = (b < M && u < K) ? wg[(uint64_t)b * K + u] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  for (uint32_t r = ty; r < 32; r += 8) {
+    const uint32_t u = u0 + r, b = b0 + tx;
+    if (u < K && b < M) {
+      const float2 v = tile[tx][r];
+      pg[(uint64_t)u * M + b] = make_float2(v.x * inv, v.y * inv);
+    }
+  }
+}
+
 size_t zf_chol_smem(uint32_t M, uint32_t K, bool dbl) {
   size_t c = dbl ? 16 : 8;
   return c * ((size_t)K * (M + 1) + (size_t)K * (K + 1)) + 256 * sizeof(float);
@@ -284,6 +310,15 @@ mb_status zf_chol(float2 *csi, float2 *precoder, uint32_t groups, uint32_t M,
     if (s != MB_OK) return s;
     zf_chol_kernel<float><<<groups, 256, smem, st>>>(csi, precoder, M, K, status, cond);
   }
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+mb_status precoder_scale(const float2 *W, float2 *P, const float *wmax, uint32_t M, uint32_t K,
+                         uint32_t groups, cudaStream_t st) {
+  if (groups == 0) return MB_OK;
+  const uint32_t tb = (M + 31) / 32, tu = (K + 31) / 32;
+  precoder_scale_kernel<<<dim3(groups, tb * tu), 256, 0, st>>>(W, P, wmax, M, K, tb);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }

@@ -13,11 +13,15 @@ mb_status zf_chol(float2 *csi, float2 *precoder, uint32_t groups, uint32_t M,
                   cudaStream_t st);
 // mixed precision ZF (zf_mixed.cu): the detector images for the
 // tensor-core equalizer in img_w (zf_mixed_scratch_bytes) and, with write_w,
-// W in place (FP32); without it csi is left as scratch
+// W in place (FP32) and its per-group max |W| in wmax (if not null);
+// without write_w csi is left as scratch
 uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K);
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
                        const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
-                       bool write_w = true);
+                       bool write_w = true, float *wmax = nullptr);
+// precoder P[g][u][b] = W[g][b][u] / wmax[g] from a precomputed per-group max
+mb_status precoder_scale(const float2 *W, float2 *P, const float *wmax, uint32_t M, uint32_t K,
+                         uint32_t groups, cudaStream_t st);
 mb_status precoder_launch(const float2 *W, float2 *P, uint32_t M, uint32_t K,
                           uint32_t groups, cudaStream_t st);
 size_t zf_chol_smem(uint32_t M, uint32_t K, bool dbl);

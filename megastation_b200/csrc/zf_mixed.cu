@@ -43,6 +43,7 @@ struct ZfmParams {
   uint8_t *img_w;     // [G] detector images for the equalizer (BF16)
   int32_t *status;
   float *cond;
+  float *wmax;        // per group max |W| (precoder scaling), or null
   int *err;
   uint32_t M, K, Mp, nkt, ns_iters;
   uint32_t nh;        // plane-0 k tiles: Mp / 64
@@ -352,6 +353,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   // ----------------------------------------- Gram out, inverse, refinement
   float cond_est = INFINITY;
   int st = 0;
+  float wmx = 0.f;  // this thread's max |W| over the values it stored
   if (!fail) {
     // R(G) = A + P A P^T (plane 1 of R(C) is P times plane 0): rows 2u and
     // 2u+1 of A sit in neighbouring TMEM lanes
@@ -537,7 +539,10 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
 #pragma unroll
             for (int e = 0; e < 8; e++) {
               const uint32_t b = kk + e;
-              if (b < M) cg[b * K + u] = make_float2(v[h * 8 + e], nb[h * 8 + e]);
+              if (b < M) {
+                cg[b * K + u] = make_float2(v[h * 8 + e], nb[h * 8 + e]);
+                wmx = fmaxf(wmx, sqrtf(v[h * 8 + e] * v[h * 8 + e] + nb[h * 8 + e] * nb[h * 8 + e]));
+              }
             }
           }
         }
@@ -597,6 +602,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
       for (uint32_t u = 0; u < K; u++) {
         const float2 w = pd ? make_float2((float)z[u].x, (float)z[u].y) : make_float2(0.f, 0.f);
         cg[b * K + u] = w;
+        wmx = fmaxf(wmx, sqrtf(w.x * w.x + w.y * w.y));
         *reinterpret_cast<__nv_bfloat16 *>(imgw + img_off(2 * u, b, MM)) = __float2bfloat16_rn(w.x);
         *reinterpret_cast<__nv_bfloat16 *>(imgw + img_off(2 * u, Mp + b, MM)) = __float2bfloat16_rn(-w.y);
         *reinterpret_cast<__nv_bfloat16 *>(imgw + img_off(2 * u + 1, b, MM)) = __float2bfloat16_rn(w.y);
@@ -605,6 +611,17 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
     }
   }
 
+  if (q.wmax) {
+    // block maximum of |W| for the precoder's scaling (beam_utils.cuh:40-80)
+    __syncthreads();
+    red[tid] = wmx;
+    __syncthreads();
+    for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if (tid < o) red[tid] = fmaxf(red[tid], red[tid + o]);
+      __syncthreads();
+    }
+    if (tid == 0) q.wmax[g] = fail ? 0.f : red[0];
+  }
   if (tid == 0) {
     if (q.status) q.status[g] = fail ? 1 : st;
     if (q.cond) q.cond[g] = cond_est;
@@ -627,7 +644,7 @@ uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K) {
 
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
                        const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
-                       bool write_w) {
+                       bool write_w, float *wmax) {
   if (K == 0 || K > 64) return MB_UNSUPPORTED;
   const TcShape s = tc_shape(M, K);
   const DeviceTables *tab = device_tables();
@@ -637,6 +654,7 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
   q.img_w = reinterpret_cast<uint8_t *>(img_w);
   q.status = status;
   q.cond = cond;
+  q.wmax = write_w ? wmax : nullptr;
   q.err = tab->err;
   q.M = M;
   q.K = K;

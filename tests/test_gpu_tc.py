@@ -159,3 +159,33 @@ def test_zf_mixed_forced_fp64_path(mb):
     assert (status.cpu().numpy() == 2).all(), status.cpu().numpy()
     W = orc.zf(csi, S=G * 16, sg=16)
     np.testing.assert_allclose(d.cpu().numpy(), W, atol=2e-6 * np.abs(W).max())
+
+
+@pytest.mark.parametrize("cond_threshold", [1e4, 0.5], ids=["ns", "fp64"])
+def test_slot_mixed_precoder(mb, cond_threshold):
+    # the mixed slot with a downlink: W from the fused ZF kernel (its FP32
+    # copy) and P = W^T / max|W| per group from the kernel's own max |W|
+    from megastation_b200 import datagen, slot
+    cfg = datagen.CellConfig(M=128, K=32, N=1024, S=600, sg=16, Qm=4, U=2, snr_db=25.0, seed=16)
+    d = datagen.make_slot(cfg)
+    run = slot.UplinkSlot(cfg, precision="mixed", sym_batch=2, use_graph=True, D=2,
+                          cond_threshold=cond_threshold)
+    iq = torch.from_numpy(d["iq"]).cuda()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        run(iq, stream=s)
+    s.synchronize()
+    assert mb.ops.device_error() == 0
+    assert (run.status.cpu().numpy() == (0 if cond_threshold > 1 else 2)).all()
+    W, P = run.buffers()
+    W = W.cpu().numpy()
+    P = P.cpu().numpy()
+    ps = orc.pilot_sign(cfg.S)
+    csi = np.zeros((cfg.G, cfg.M, cfg.K), np.complex64)
+    for p in range(cfg.P):
+        orc.pilot_fft(d["iq"][p], cfg.N, cfg.S, cfg.start, cfg.K, cfg.sg, p * cfg.sg, ps, csi)
+    Wr = orc.zf(csi, S=cfg.S, sg=cfg.sg)
+    assert np.abs(W - Wr).max() <= 0.01 * np.abs(Wr).max()
+    mx = np.abs(W).max(axis=(1, 2))
+    Pr = np.transpose(W, (0, 2, 1)) / mx[:, None, None]
+    np.testing.assert_allclose(P, Pr, rtol=0, atol=1e-6)
