@@ -115,6 +115,18 @@ mb_status mb_fft_destroy(mb_fft *fft);
 mb_status mb_fft_uplink(mb_fft *fft, const void *iq, int iq_dtype,
                         uint32_t n_sym, mb_c32 *out, void *stream);
 
+/* Mixed-precision uplink FFT (no reference counterpart; same transform and
+ * shift gather as mb_fft_uplink): the output is planar BF16 rows
+ * out[n_sym][re|im][M][row_pitch], subcarrier i < S at column i, the layout
+ * the tensor-core equalizer reads.  Columns from S up to S rounded up to a
+ * multiple of 8 may be overwritten with other FFT bins; columns beyond that
+ * are left as they are.  For N = 4096 with row_pitch % 8 == 0 and 16-byte
+ * aligned buffers the butterflies run on the tensor cores (FP16 operands
+ * scaled per row by a power of two, FP32 accumulation); otherwise in FP32. */
+mb_status mb_fft_uplink_bf16(mb_fft *fft, const void *iq, int iq_dtype,
+                             uint32_t n_sym, void *out, uint32_t row_pitch,
+                             void *stream);
+
 /* PilotFFT::operator()(in, out, ue_start) (fft/fft_op.cu:145-165): symbol p
  * of n_sym carries the comb pilots of users ue_start + p*sg + (i % sg); the
  * LS estimate conj(X)*p/|p|^2 of subcarrier i is stored at

@@ -432,6 +432,7 @@ struct mb_fft {
   int device;
   const float2 *tw;
   float2 *pilot;  // device pilot sign table (S entries)
+  FftTcPlan *tc;  // tensor-core FFT operands (N = 4096), else null
 };
 
 extern "C" mb_status mb_fft_create(const mb_fft_desc *desc, mb_fft **out) {
@@ -448,6 +449,7 @@ extern "C" mb_status mb_fft_create(const mb_fft_desc *desc, mb_fft **out) {
   cudaGetDevice(&f->device);
   f->tw = tab->twiddle[f->logn];
   f->pilot = nullptr;
+  f->tc = fft_tc_plan_create(d.ofdm_ca, d.ofdm_start);
   if (d.ue_num > 0 && d.sc_group > 0) {
     mb_c32 *h = new mb_c32[d.ofdm_num];
     mb_pilot_sign(d.ofdm_num, h);
@@ -457,6 +459,7 @@ extern "C" mb_status mb_fft_create(const mb_fft_desc *desc, mb_fft **out) {
     delete[] h;
     if (e != cudaSuccess) {
       if (f->pilot) cudaFree(f->pilot);
+      fft_tc_plan_destroy(f->tc);
       delete f;
       return record_error(e);
     }
@@ -468,6 +471,7 @@ extern "C" mb_status mb_fft_create(const mb_fft_desc *desc, mb_fft **out) {
 extern "C" mb_status mb_fft_destroy(mb_fft *f) {
   if (!f) return MB_BAD_ARG;
   if (f->pilot) cudaFree(f->pilot);
+  fft_tc_plan_destroy(f->tc);
   delete f;
   return MB_OK;
 }
@@ -489,9 +493,19 @@ extern "C" mb_status mb_fft_uplink(mb_fft *f, const void *iq, int iq_dtype,
   return launch_fft<kUplink>(f->logn, p, as_stream(stream));
 }
 
+extern "C" mb_status mb_fft_uplink_bf16(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
+                                        void *out, uint32_t row_pitch, void *stream) {
+  return fft_uplink_lp(f, iq, iq_dtype, n_sym, out, row_pitch, as_stream(stream));
+}
+
 mb_status mb::fft_uplink_lp(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
                             void *y_lp, uint32_t S_pad, cudaStream_t st) {
   if (!f || !iq || !y_lp || !dtype_ok(iq_dtype) || S_pad < f->d.ofdm_num) return MB_BAD_ARG;
+  if (fft_tc_lp_supported(f->tc, iq, S_pad, y_lp)) {
+    const DeviceTables *tab = device_tables();
+    return fft_tc_uplink_lp(f->tc, iq, iq_dtype, n_sym * f->d.bs_num, f->d.bs_num, f->d.ofdm_num, y_lp, S_pad,
+                            tab ? tab->err : nullptr, st);
+  }
   FftParams p{};
   p.in = iq;
   p.out = y_lp;

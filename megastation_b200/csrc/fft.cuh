@@ -14,4 +14,16 @@ mb_status fft_uplink_lp(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
 mb_status fft_pilot_fill(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym, mb_c32 *csi,
                          cudaStream_t st);
 
+// tensor-core FFT for N = 4096 (fft_tc.cu): a plan holds the DFT operands
+// with the FFT shift of `start` folded in; null for other N
+struct FftTcPlan;
+FftTcPlan *fft_tc_plan_create(uint32_t N, uint32_t start);
+void fft_tc_plan_destroy(FftTcPlan *plan);
+bool fft_tc_lp_supported(const FftTcPlan *plan, const void *iq, uint32_t S_pad, const void *y_lp);
+// rows = n_sym * M rows of 4096 samples -> planar BF16 rows as fft_uplink_lp;
+// upc: units of two rows per CTA (0: default)
+mb_status fft_tc_uplink_lp(const FftTcPlan *plan, const void *iq, int iq_dtype, uint32_t rows, uint32_t M,
+                           uint32_t S, void *y_lp, uint32_t S_pad, int *err, cudaStream_t st,
+                           uint32_t upc = 0);
+
 }  // namespace mb

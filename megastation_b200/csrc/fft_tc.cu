@@ -1,0 +1,593 @@
+// fft_tc.cu -- 4096-point OFDM FFT with its butterflies on the tensor cores.
+//
+// Replaces the reference's uplink FFT pipeline for N = 4096 (load kernel ->
+// cuFFT C2C -> FFT-shift gather, fft/fft_op.cu:135-143 with
+// fft_callback.cuh:20-74) in the mixed-precision slot, where the output goes
+// to the tensor-core equalizer as planar BF16 rows.  Cooley-Tukey 64 x 64
+// with n = 64 n1 + n2 and bin k = k1 + 64 k2:
+//
+//   Y[k1][n2]      = sum_n1 x[64 n1 + n2] W64^(n1 k1)     GEMM 1
+//   Z[k1][n2]      = Y[k1][n2] W4096^(n2 k1)               CUDA cores
+//   X[k1 + 64 k2]  = sum_n2 Z[k1][n2] W64^(n2 k2)          GEMM 2
+//
+// and bin k is stored as subcarrier (k - start - N/2) mod N when that is
+// below S (fft_callback.cuh:43-74).  The complex GEMMs run as real ones on
+// the [re; im] embedding (K = 128) with FP16 operands and FP32 accumulation
+// in TMEM (tcgen05.mma kind::f16); both multiply by the same 128 x 128 DFT
+// operand F.  Each row is scaled by a power of two so that its largest
+// component lies in [128, 256): then |Y| and |Z| stay below 2^15.5, inside
+// the FP16 range, and the scale is undone exactly before the BF16 store.
+//
+// One CTA per SM takes `upc` consecutive units of two rows, with 224 KB of
+// shared memory (F, one GEMM operand buffer, an output staging buffer and a
+// two-unit input ring) and 256 TMEM columns (the two GEMM accumulators).
+// Warp 8 is the control warp: one thread streams the units' rows into the
+// ring with 128-byte-swizzled TMA boxes (so the conversion reads are free of
+// bank conflicts), issues both GEMMs and writes the staged output rows back
+// with bulk copies.  Warps 0-7 convert the samples into the GEMM-1 operand,
+// twiddle the GEMM-1 result into the GEMM-2 operand (in the same buffer,
+// which GEMM 1 no longer needs) and stage the GEMM-2 result as BF16 rows.
+// Mbarriers hand each buffer between the roles, so a unit's loads, GEMMs,
+// conversion and stores overlap those of its neighbours.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+#include "tc.cuh"
+
+namespace mb {
+
+struct FftTcPlan {
+  uint8_t *mats;  // F, 128 x 128 FP16 in its shared-memory layout
+  float2 *tw;     // W4096^j, j < 4096
+  uint32_t c;     // (start + N/2) mod N
+};
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kFtCompute = 512;                  // warps 0-15
+constexpr int kFtThreads = kFtCompute + 64;      // + the GEMM and copy warps
+constexpr uint32_t kFtN = 4096;
+constexpr uint32_t kMat = 32768;                 // one 128 x 128 FP16 operand
+constexpr uint32_t kStage = 65536;               // raw samples of one unit (c64)
+// staged output rows (r, plane) at (2 r + plane) * kStgPitch: 8192 B plus 64,
+// so the two planes of a row start on opposite halves of the 32 banks
+constexpr uint32_t kStgPitch = 8192 + 64;
+constexpr uint32_t kFtSmem = 2 * kMat + 2 * kStage + 4 * kStgPitch;  // F, AZ, ring, staging
+
+// byte offset of element (row, kk) of a 128 x 128 K-major operand: 8-row
+// groups 2048 B apart, K core matrices (8 elements, 16 B) 128 B apart
+__host__ __device__ constexpr uint32_t kmaj_off(uint32_t row, uint32_t kk) {
+  return (row / 8) * 2048 + (kk / 8) * 128 + (row % 8) * 16 + (kk % 8) * 2;
+}
+// byte offset of element (mn, kk) of a 128 x 128 MN-major operand: 8-row K
+// groups 2048 B apart, 8-element MN chunks 128 B apart
+__host__ __device__ constexpr uint32_t mnmaj_off(uint32_t mn, uint32_t kk) {
+  return (kk / 8) * 2048 + (mn / 8) * 128 + (kk % 8) * 16 + (mn % 8) * 2;
+}
+
+struct FtParams {
+  uint32_t rows;        // n_sym * M rows of 4096 samples
+  uint32_t M, S, S_pad;
+  __nv_bfloat16 *out;   // [n_sym][re|im][M][S_pad]
+  const uint8_t *mats;
+  const float2 *tw;
+  uint32_t c;
+  uint32_t units;       // ceil(rows / 2)
+  uint32_t upc;         // units per CTA
+  int *err;
+};
+
+template <int DT>
+struct Fmt {
+  static constexpr uint32_t kBytes = DT == MB_IQ_C32 ? 8 : DT == MB_IQ_I8 ? 2 : 4;  // per sample
+  static constexpr uint32_t kBoxes = kBytes / 2;      // 128-byte boxes per 64-sample n1 row
+  static constexpr uint32_t kPPC = kBytes / 2;        // 16-byte pieces per 8-sample chunk
+  static constexpr uint32_t kUnitBytes = 2 * kFtN * kBytes;
+};
+
+// ring offset of the 16-byte piece holding sample n2 (first of its piece)
+// of n1 row n1 of unit row r: box (r, n2 / (128 / bytes)) of 64 n1 rows x
+// 128 B, swizzled by the TMA
+template <int DT>
+__device__ __forceinline__ uint32_t ring_off(uint32_t r, uint32_t n1, uint32_t n2) {
+  using F = Fmt<DT>;
+  const uint32_t byte = n2 * F::kBytes;
+  const uint32_t box = r * F::kBoxes + byte / 128;
+  return box * 8192 + n1 * 128 + ((((byte % 128) / 16) ^ (n1 & 7)) * 16);
+}
+
+template <int DT>
+__device__ __forceinline__ float2 chunk_sample(const uint4 *raw, int j) {
+  if constexpr (DT == MB_IQ_C32) {
+    const uint4 w = raw[j / 2];
+    return (j & 1) ? make_float2(__uint_as_float(w.z), __uint_as_float(w.w))
+                   : make_float2(__uint_as_float(w.x), __uint_as_float(w.y));
+  } else if constexpr (DT == MB_IQ_I16) {
+    const uint4 w = raw[j / 4];
+    const uint32_t v = (j & 3) == 0 ? w.x : (j & 3) == 1 ? w.y : (j & 3) == 2 ? w.z : w.w;
+    return make_float2((float)(int16_t)(v & 0xFFFFu) / 32768.f, (float)(int16_t)(v >> 16) / 32768.f);
+  } else if constexpr (DT == MB_IQ_I8) {
+    const uint4 w = raw[0];
+    const uint32_t v = (j / 2) == 0 ? w.x : (j / 2) == 1 ? w.y : (j / 2) == 2 ? w.z : w.w;
+    const uint32_t h = (j & 1) ? v >> 16 : v & 0xFFFFu;
+    return make_float2((float)(int8_t)(h & 0xFFu) / 128.f, (float)(int8_t)(h >> 8) / 128.f);
+  } else {
+    const uint4 w = raw[j / 4];
+    const uint32_t v = (j & 3) == 0 ? w.x : (j & 3) == 1 ? w.y : (j & 3) == 2 ? w.z : w.w;
+    __half2 h;
+    memcpy(&h, &v, 4);
+    return __half22float2(h);
+  }
+}
+
+__device__ __forceinline__ uint32_t h2_bits(float a, float b) {
+  const __half2 h = __floats2half2_rn(a, b);
+  uint32_t u;
+  memcpy(&u, &h, 4);
+  return u;
+}
+
+__device__ __forceinline__ uint32_t bf2_bits(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  uint32_t u;
+  memcpy(&u, &h, 4);
+  return u;
+}
+
+// Power-of-two scale taking a row maximum with bit pattern mbits (>= 0) to
+// [128, 256), and its inverse.
+__device__ __forceinline__ void row_scale(uint32_t mbits, float &scale, float &inv) {
+  if (mbits == 0) {
+    scale = inv = 1.f;
+    return;
+  }
+  int se = 261 - (int)(mbits >> 23);
+  se = min(max(se, 1), 253);
+  scale = __uint_as_float((uint32_t)se << 23);
+  inv = __uint_as_float((uint32_t)(254 - se) << 23);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
+}
+// named barrier among the compute warps
+__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
+
+// shared -> global bulk copy (16-byte aligned, size a multiple of 16)
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(tc::smem_u32(src)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Bounded wait that also gives up as soon as another thread has failed.
+__device__ __forceinline__ bool ft_wait(uint64_t *bar, uint32_t parity, volatile int *fail) {
+  if (tc::mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = tc::globaltimer();
+  while (!tc::mbar_try_wait(bar, parity)) {
+    if (*fail || tc::globaltimer() - t0 > 1000000000ull) {
+      *fail = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+template <int DT>
+__global__ void __launch_bounds__(kFtThreads, 1)
+    fft_tc_lp_kernel(const __grid_constant__ CUtensorMap in_map, const FtParams p) {
+  extern __shared__ __align__(1024) uint8_t ft_smem[];
+  // F, AZ and the ring start on 1024-byte boundaries (the swizzled TMA boxes
+  // need them); the staging rows follow
+  uint8_t *sF = ft_smem, *sAZ = ft_smem + kMat, *sRing = ft_smem + 2 * kMat;
+  uint8_t *sStg = sRing + 2 * kStage;
+  __shared__ uint64_t bar_mats, full[2], a_ready, z_ready, st_ready, d1_full, d2_full, st_done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ __align__(16) uint32_t s_rmax[16];
+  __shared__ volatile int s_fail;
+  using F = Fmt<DT>;
+
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const uint32_t u_begin = blockIdx.x * p.upc;
+  if (u_begin >= p.units) return;
+  const uint32_t n_units = min(p.upc, p.units - u_begin);
+
+  if (tid == kFtCompute) {
+    tc::mbar_init(&bar_mats, 1);
+    tc::mbar_init(&full[0], 1);
+    tc::mbar_init(&full[1], 1);
+    tc::mbar_init(&a_ready, kFtCompute / 32);
+    tc::mbar_init(&z_ready, kFtCompute / 32);
+    tc::mbar_init(&st_ready, kFtCompute / 32);
+    tc::mbar_init(&d1_full, 1);
+    tc::mbar_init(&d2_full, 1);
+    tc::mbar_init(&st_done, 1);
+    s_fail = 0;
+    tc::fence_mbar_init();
+    tc::prefetch_tmap(&in_map);
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_slot, 256);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_slot;  // D1: columns 0..127, D2: 128..255
+
+  // output rows of unit u: (row, plane) -> global and staging addresses
+  auto out_row = [&](uint32_t u, uint32_t r, uint32_t pl) {
+    const uint32_t row = 2 * u + r, sym = row / p.M, b = row - sym * p.M;
+    return p.out + ((uint64_t)(sym * 2 + pl) * p.M + b) * p.S_pad;
+  };
+  const uint32_t S8 = (p.S + 7) & ~7u;  // columns written by the bulk copies (<= S_pad)
+
+  if (warp == kFtCompute / 32) {
+    // ================================================== GEMM warp
+    if (lane == 0) {
+      const uint32_t fa = tc::smem_u32(sF), az = tc::smem_u32(sAZ);
+      const uint32_t idesc = tc::idesc_f16(128, 128, true, false);  // A MN-major, B K-major
+      // both GEMMs read the operand buffer (MN-major) and F (K-major)
+      uint64_t da[8], db[8];
+#pragma unroll
+      for (int ks = 0; ks < 8; ks++) {
+        da[ks] = tc::smem_desc(az + ks * 4096, 2048, 128);
+        db[ks] = tc::smem_desc(fa + ks * 256, 128, 2048);
+      }
+      uint32_t n_d1 = 0, n_d2 = 0;
+      bool ok = ft_wait(&bar_mats, 0, &s_fail);
+      for (uint32_t i = 0; i < n_units && ok; i++) {
+        // GEMM 1: D1 (128 (r, n2) x 128 (p', k1)) = A (samples) x F
+        if (!ft_wait(&a_ready, i & 1, &s_fail)) break;
+        tc::fence_after_sync();
+#pragma unroll
+        for (int ks = 0; ks < 8; ks++) tc::mma_f16(tmem, da[ks], db[ks], idesc, ks > 0);
+        tc::mma_commit(&d1_full);
+        n_d1++;
+        // GEMM 2: D2 (128 (r, k1) x 128 (p', k2)) = Z x F
+        if (!ft_wait(&z_ready, i & 1, &s_fail)) break;
+        tc::fence_after_sync();
+#pragma unroll
+        for (int ks = 0; ks < 8; ks++) tc::mma_f16(tmem + 128, da[ks], db[ks], idesc, ks > 0);
+        tc::mma_commit(&d2_full);
+        n_d2++;
+      }
+      if (s_fail) {
+        // a wait ran out: let the issued GEMMs drain (bounded)
+        if (n_d1) tc::mbar_wait(&d1_full, (n_d1 - 1) & 1, 100000000ull);
+        if (n_d2) tc::mbar_wait(&d2_full, (n_d2 - 1) & 1, 100000000ull);
+      }
+    }
+  } else if (warp == kFtCompute / 32 + 1) {
+    // ================================================== copy warp
+    if (lane == 0) {
+      uint32_t loads[2] = {0, 0};
+      auto issue_load = [&](uint32_t i) {
+        if (i >= n_units) return;
+        const uint32_t u = u_begin + i;
+        loads[i & 1]++;
+        uint8_t *slot = sRing + (i & 1) * kStage;
+        tc::mbar_arrive_expect_tx(&full[i & 1], F::kUnitBytes);
+#pragma unroll
+        for (uint32_t r = 0; r < 2; r++)
+#pragma unroll
+          for (uint32_t bx = 0; bx < F::kBoxes; bx++)
+            tc::tma_load_2d(slot + (r * F::kBoxes + bx) * 8192, &in_map, (int32_t)(bx * 128),
+                            (int32_t)((2 * u + r) * 64), &full[i & 1]);
+      };
+      // staged rows hold all 4096 bins in subcarrier order; the first
+      // S rounded up to 8 go out by bulk copy (within the row pitch)
+      auto issue_stores = [&](uint32_t i) {
+        const uint32_t u = u_begin + i;
+        for (uint32_t r = 0; r < 2; r++) {
+          if (2 * u + r >= p.rows) break;
+          for (uint32_t pl = 0; pl < 2; pl++) bulk_s2g(out_row(u, r, pl), sStg + (2 * r + pl) * kStgPitch, S8 * 2);
+        }
+        bulk_commit();
+      };
+      tc::mbar_arrive_expect_tx(&bar_mats, kMat);
+      tc::bulk_g2s(sF, p.mats, kMat, &bar_mats);
+      issue_load(0);
+      issue_load(1);
+      for (uint32_t i = 0; i < n_units; i++) {
+        // the ring slot of unit i takes unit i + 2 once unit i is converted
+        if (!ft_wait(&a_ready, i & 1, &s_fail)) break;
+        issue_load(i + 2);
+        if (i > 0) {
+          if (!ft_wait(&st_ready, (i - 1) & 1, &s_fail)) break;
+          issue_stores(i - 1);
+          bulk_wait_read();
+          mbar_arrive(&st_done);
+        }
+      }
+      if (!s_fail && ft_wait(&st_ready, (n_units - 1) & 1, &s_fail)) issue_stores(n_units - 1);
+      bulk_wait_all();
+      if (s_fail) {
+        // a wait ran out: record it and let the loads in flight land (bounded)
+        if (p.err) atomicOr(p.err, tc::kErrTimeout);
+        for (int sl = 0; sl < 2; sl++)
+          if (loads[sl]) tc::mbar_wait(&full[sl], (loads[sl] - 1) & 1, 100000000ull);
+        tc::mbar_wait(&bar_mats, 0, 100000000ull);
+      }
+    }
+  } else {
+    // ================================================== compute warps
+    bool ok = true;  // warp-uniform: every compute thread runs the same barriers
+    auto wait_ok = [&](uint64_t *bar, uint32_t parity) {
+      if (ok) ok = ft_wait(bar, parity, &s_fail);
+      ok = __all_sync(0xffffffffu, ok);
+    };
+    auto arrive = [&](uint64_t *bar) {
+      tc::fence_proxy_async_smem();
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar);
+    };
+    // Conversion: thread -> row rh of the unit, 2 chunks of 8 samples (n1,
+    // n2 .. n2 + 7); a warp covers 8 consecutive n1 x 4 chunks, so its
+    // 16-byte operand stores fill whole core matrices.  Offsets are the same
+    // for every unit.
+    const uint32_t rh = tid >> 8, wq = (tid >> 5) & 7;
+    uint32_t r_off[2][F::kPPC], a_off[2];
+#pragma unroll
+    for (int c2 = 0; c2 < 2; c2++) {
+      const uint32_t q = wq * 2 + c2, n1 = 8 * (q >> 1) + (lane & 7), n2b = 4 * (q & 1) + (lane >> 3);
+#pragma unroll
+      for (int w = 0; w < (int)F::kPPC; w++) r_off[c2][w] = ring_off<DT>(rh, n1, 8 * n2b + w * (16 / F::kBytes));
+      a_off[c2] = mnmaj_off(64 * rh + 8 * n2b, n1);  // imaginary parts 8 K groups (16 KB) further
+    }
+    // GEMM-1 epilogue: TMEM lane (r, n2), k1 in [16 part, 16 part + 16)
+    const uint32_t quad = warp & 3, part = warp >> 2;
+    const uint32_t lane_row = quad * 32 + lane;
+    const uint32_t tl = tmem + ((quad * 32) << 16);
+    const uint32_t e_n2 = lane_row & 63, e_r = lane_row >> 6;
+    float2 tw[16];  // W4096^(n2 k1)
+#pragma unroll
+    for (int j = 0; j < 16; j++) tw[j] = __ldg(p.tw + ((e_n2 * (16 * part + j)) & (kFtN - 1)));
+    const uint32_t z_off = mnmaj_off(64 * e_r + 16 * part, e_n2);
+    // GEMM-2 epilogue: TMEM lane (r, k1), k2 in [16 part, 16 part + 16); bin
+    // k1 + 64 k2 is subcarrier (k1 + 64 k2 - c) mod N.  With c even the even
+    // lane's subcarrier is even: lane pairs swap one packed BF16 pair, then
+    // the even lane writes the real pair (sc, sc + 1) and the odd lane the
+    // imaginary pair (sc - 1, sc), two 64-byte runs in disjoint banks.
+    const uint32_t s_r = lane_row >> 6, s_k1 = lane_row & 63;
+    const uint32_t s_base = (s_k1 + kFtN - p.c + 1024 * part) & (kFtN - 1);
+    const bool odd = lane & 1, pairs = (p.c & 1) == 0;
+    const uint32_t perm = odd ? 0x3276u : 0x5410u;
+    uint8_t *stg_mine = sStg + (2 * s_r + (odd ? 1 : 0)) * kStgPitch;
+    __nv_bfloat16 *stg_re = reinterpret_cast<__nv_bfloat16 *>(sStg + 2 * s_r * kStgPitch);
+    __nv_bfloat16 *stg_im = reinterpret_cast<__nv_bfloat16 *>(sStg + (2 * s_r + 1) * kStgPitch);
+    __shared__ float s_inv[2][2];  // [unit parity][row] inverse row scales
+
+    auto store_unit = [&](uint32_t i) {
+      const float inv = s_inv[i & 1][s_r];
+      float vr[16], vi[16];
+      tc::tmem_ld16(tl + 128 + 16 * part, vr);
+      tc::tmem_ld16(tl + 192 + 16 * part, vi);
+      if (pairs) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const uint32_t own = bf2_bits(vr[j] * inv, vi[j] * inv);
+          const uint32_t other = __shfl_xor_sync(0xffffffffu, own, 1);
+          const uint32_t s0 = (s_base + 64 * j) & (kFtN - 2);
+          *reinterpret_cast<uint32_t *>(stg_mine + 2 * s0) = __byte_perm(own, other, perm);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const uint32_t sc = (s_base + 64 * j) & (kFtN - 1);
+          stg_re[sc] = __float2bfloat16_rn(vr[j] * inv);
+          stg_im[sc] = __float2bfloat16_rn(vi[j] * inv);
+        }
+      }
+      arrive(&st_ready);
+    };
+
+    for (uint32_t i = 0; i < n_units; i++) {
+      const uint8_t *slot = sRing + (i & 1) * kStage;
+      // (a) conversion: row maximum, power-of-two scale, FP16 operand A
+      wait_ok(&full[i & 1], (i >> 1) & 1);
+      uint4 re[2], im[2];
+      {
+        uint4 raw[2][F::kPPC];
+#pragma unroll
+        for (int c2 = 0; c2 < 2; c2++)
+#pragma unroll
+          for (int w = 0; w < (int)F::kPPC; w++) raw[c2][w] = *reinterpret_cast<const uint4 *>(slot + r_off[c2][w]);
+        float m = 0.f;
+#pragma unroll
+        for (int c2 = 0; c2 < 2; c2++)
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const float2 v = chunk_sample<DT>(raw[c2], j);
+            m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+          }
+        const uint32_t mb = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+        if (lane == 0) s_rmax[warp] = mb;
+        compute_sync();
+        const uint4 m0 = *reinterpret_cast<const uint4 *>(&s_rmax[rh * 8]);
+        const uint4 m1 = *reinterpret_cast<const uint4 *>(&s_rmax[rh * 8 + 4]);
+        const uint32_t rmax = max(max(max(m0.x, m0.y), max(m0.z, m0.w)), max(max(m1.x, m1.y), max(m1.z, m1.w)));
+        float scale, inv;
+        row_scale(rmax, scale, inv);
+        if ((tid & 255) == 0) s_inv[i & 1][rh] = inv;
+#pragma unroll
+        for (int c2 = 0; c2 < 2; c2++) {
+          float2 v[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) v[j] = chunk_sample<DT>(raw[c2], j);
+          re[c2] = make_uint4(h2_bits(v[0].x * scale, v[1].x * scale), h2_bits(v[2].x * scale, v[3].x * scale),
+                              h2_bits(v[4].x * scale, v[5].x * scale), h2_bits(v[6].x * scale, v[7].x * scale));
+          im[c2] = make_uint4(h2_bits(v[0].y * scale, v[1].y * scale), h2_bits(v[2].y * scale, v[3].y * scale),
+                              h2_bits(v[4].y * scale, v[5].y * scale), h2_bits(v[6].y * scale, v[7].y * scale));
+        }
+      }
+      // the operand buffer holds Z of the previous unit until GEMM 2 has read it
+      if (i > 0) wait_ok(&d2_full, (i - 1) & 1);
+      tc::fence_after_sync();
+      if (ok) {
+#pragma unroll
+        for (int c2 = 0; c2 < 2; c2++) {
+          *reinterpret_cast<uint4 *>(sAZ + a_off[c2]) = re[c2];
+          *reinterpret_cast<uint4 *>(sAZ + a_off[c2] + 16384) = im[c2];
+        }
+      }
+      arrive(&a_ready);
+      // (b) GEMM-2 epilogue of the previous unit into the staging rows,
+      // once the bulk copies of the unit before it have read them
+      if (i > 0) {
+        if (i > 1) wait_ok(&st_done, (i - 2) & 1);
+        if (ok) store_unit(i - 1);
+        else arrive(&st_ready);
+      }
+      // (c) GEMM-1 epilogue: twiddle into the GEMM-2 operand Z
+      wait_ok(&d1_full, i & 1);
+      tc::fence_after_sync();
+      if (ok) {
+        float yr[16], yi[16];
+        tc::tmem_ld16(tl + 16 * part, yr);
+        tc::tmem_ld16(tl + 64 + 16 * part, yi);
+#pragma unroll
+        for (int g = 0; g < 2; g++) {
+          float zr[8], zi[8];
+#pragma unroll
+          for (int b = 0; b < 8; b++) {
+            const float2 w = tw[8 * g + b];
+            const float xr = yr[8 * g + b], xi = yi[8 * g + b];
+            zr[b] = xr * w.x - xi * w.y;
+            zi[b] = xr * w.y + xi * w.x;
+          }
+          *reinterpret_cast<uint4 *>(sAZ + z_off + g * 128) =
+              make_uint4(h2_bits(zr[0], zr[1]), h2_bits(zr[2], zr[3]), h2_bits(zr[4], zr[5]), h2_bits(zr[6], zr[7]));
+          *reinterpret_cast<uint4 *>(sAZ + z_off + g * 128 + 16384) =
+              make_uint4(h2_bits(zi[0], zi[1]), h2_bits(zi[2], zi[3]), h2_bits(zi[4], zi[5]), h2_bits(zi[6], zi[7]));
+        }
+      }
+      arrive(&z_ready);
+    }
+    // the last unit's inverse scales were written after the last barrier
+    compute_sync();
+    wait_ok(&d2_full, (n_units - 1) & 1);
+    tc::fence_after_sync();
+    if (n_units > 1) wait_ok(&st_done, (n_units - 2) & 1);
+    if (ok) store_unit(n_units - 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 256);
+}
+
+using FtKernel = void (*)(const CUtensorMap, const FtParams);
+FtKernel fft_tc_kernel_of(int dt) {
+  switch (dt) {
+    case MB_IQ_C32: return fft_tc_lp_kernel<MB_IQ_C32>;
+    case MB_IQ_I16: return fft_tc_lp_kernel<MB_IQ_I16>;
+    case MB_IQ_I8: return fft_tc_lp_kernel<MB_IQ_I8>;
+    default: return fft_tc_lp_kernel<MB_IQ_F16>;
+  }
+}
+
+mb_status fft_tc_configure(int dt, int dev) {
+  static std::atomic<uint64_t> configured[4] = {};
+  const int which = dt == MB_IQ_C32 ? 0 : dt == MB_IQ_I16 ? 1 : dt == MB_IQ_I8 ? 2 : 3;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (configured[which].load() & bit) return MB_OK;
+  MB_CUDA_TRY(cudaFuncSetAttribute(fft_tc_kernel_of(dt), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kFtSmem));
+  configured[which].fetch_or(bit);
+  return MB_OK;
+}
+
+}  // namespace
+
+FftTcPlan *fft_tc_plan_create(uint32_t N, uint32_t start) {
+  if (N != kFtN) return nullptr;
+  const uint32_t c = (start + N / 2) % N;
+  // F[(p', k)][(p, n)]: real embedding of W64^(n k).  Row (p', k) weighs the
+  // (re, im) inputs by (Re W, -Im W) for the real output p' = 0 and by
+  // (Im W, Re W) for p' = 1.
+  std::vector<uint16_t> mats(kMat / 2, 0);
+  for (uint32_t k = 0; k < 64; k++)
+    for (uint32_t n = 0; n < 64; n++) {
+      const double ang = 2.0 * kPi * (double)((n * k) % 64) / 64.0;
+      const float wr = (float)std::cos(ang), wi = (float)-std::sin(ang);
+      const float v[2][2] = {{wr, -wi}, {wi, wr}};  // [p'][p]
+      for (int pp = 0; pp < 2; pp++)
+        for (int pi = 0; pi < 2; pi++) {
+          const __half h = __float2half_rn(v[pp][pi]);
+          uint16_t bits;
+          memcpy(&bits, &h, 2);
+          mats[kmaj_off(64 * pp + k, 64 * pi + n) / 2] = bits;
+        }
+    }
+  std::vector<float2> tw(kFtN);
+  for (uint32_t j = 0; j < kFtN; j++) {
+    const double ang = 2.0 * kPi * (double)j / (double)kFtN;
+    tw[j] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+  }
+  FftTcPlan *pl = new FftTcPlan{nullptr, nullptr, c};
+  cudaError_t e = cudaMalloc(&pl->mats, kMat);
+  if (e == cudaSuccess) e = cudaMalloc(&pl->tw, sizeof(float2) * kFtN);
+  if (e == cudaSuccess) e = cudaMemcpy(pl->mats, mats.data(), kMat, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(pl->tw, tw.data(), sizeof(float2) * kFtN, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    record_error(e);
+    fft_tc_plan_destroy(pl);
+    return nullptr;
+  }
+  return pl;
+}
+
+void fft_tc_plan_destroy(FftTcPlan *pl) {
+  if (!pl) return;
+  cudaFree(pl->mats);
+  cudaFree(pl->tw);
+  delete pl;
+}
+
+bool fft_tc_lp_supported(const FftTcPlan *pl, const void *iq, uint32_t S_pad, const void *y_lp) {
+  return pl && S_pad % 8 == 0 && (reinterpret_cast<uintptr_t>(iq) & 15) == 0 &&
+         (reinterpret_cast<uintptr_t>(y_lp) & 15) == 0;
+}
+
+mb_status fft_tc_uplink_lp(const FftTcPlan *pl, const void *iq, int iq_dtype, uint32_t rows, uint32_t M,
+                           uint32_t S, void *y_lp, uint32_t S_pad, int *err, cudaStream_t st,
+                           uint32_t upc) {
+  if (!fft_tc_lp_supported(pl, iq, S_pad, y_lp) || S > kFtN || S > S_pad) return MB_BAD_ARG;
+  if (rows == 0) return MB_OK;
+  int dev = 0;
+  MB_CUDA_TRY(cudaGetDevice(&dev));
+  mb_status r = fft_tc_configure(iq_dtype, dev);
+  if (r != MB_OK) return r;
+  const uint32_t bytes = iq_dtype == MB_IQ_C32 ? 8 : iq_dtype == MB_IQ_I8 ? 2 : 4;
+  // the rows as 64-sample n1 rows of 64 * bytes bytes, read in 128-byte boxes
+  CUtensorMap map;
+  r = make_tmap_2d_u8_sw128(&map, iq, 64ull * bytes, (uint64_t)rows * 64, 64ull * bytes, 64);
+  if (r != MB_OK) return r;
+  FtParams p{};
+  p.rows = rows;
+  p.M = M;
+  p.S = S;
+  p.S_pad = S_pad;
+  p.out = reinterpret_cast<__nv_bfloat16 *>(y_lp);
+  p.mats = pl->mats;
+  p.tw = pl->tw;
+  p.c = pl->c;
+  p.units = (rows + 1) / 2;
+  p.upc = upc ? upc : 11;
+  p.err = err;
+  const uint32_t grid = (p.units + p.upc - 1) / p.upc;
+  fft_tc_kernel_of(iq_dtype)<<<grid, kFtThreads, kFtSmem, st>>>(map, p);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
+
+}  // namespace mb

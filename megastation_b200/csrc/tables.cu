@@ -140,6 +140,35 @@ mb_status make_tmap_2d_bf16(CUtensorMap *map, const void *base, uint64_t width, 
   return r == CUDA_SUCCESS ? MB_OK : MB_BAD_ARG;
 }
 
+// Host: a 2-D byte tensor map over `rows` rows of `width` bytes (row pitch
+// `pitch` bytes, a multiple of 16), box = 128 bytes by box_y rows, stored
+// in shared memory with the 128-byte swizzle (16-byte chunk c of box row y
+// at chunk c ^ (y % 8); boxes 1024-byte aligned).
+mb_status make_tmap_2d_u8_sw128(CUtensorMap *map, const void *base, uint64_t width, uint64_t rows,
+                                uint64_t pitch, uint32_t box_y) {
+  static EncodeTiledFn fn = nullptr;
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!fn) {
+      void *p = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      MB_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+      if (q != cudaDriverEntryPointSuccess || !p) return MB_CUDA_ERROR;
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+  }
+  if (pitch % 16 || (reinterpret_cast<uintptr_t>(base) % 16)) return MB_BAD_ARG;
+  cuuint64_t dims[2] = {width, rows};
+  cuuint64_t strides[1] = {pitch};
+  cuuint32_t box[2] = {128, box_y};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? MB_OK : MB_BAD_ARG;
+}
+
 }  // namespace mb
 
 using namespace mb;

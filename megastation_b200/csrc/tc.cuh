@@ -143,6 +143,16 @@ __host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N, bool a
          | ((M >> 4) << 24);                // M / 16
 }
 
+// Instruction descriptor, kind::f16: FP32 accumulate, FP16 A and B.
+__host__ __device__ constexpr uint32_t idesc_f16(uint32_t M, uint32_t N, bool a_mn_major,
+                                                 bool b_mn_major) {
+  return (1u << 4)                          // D format F32; A, B format F16 (0)
+         | ((a_mn_major ? 1u : 0u) << 15)   // A major
+         | ((b_mn_major ? 1u : 0u) << 16)   // B major
+         | ((N >> 3) << 17)                 // N / 8
+         | ((M >> 4) << 24);                // M / 16
+}
+
 }  // namespace tc
 }  // namespace mb
 
@@ -187,5 +197,9 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
 // a multiple of 16 bytes), box = box_x elements by box_y rows, no swizzle.
 mb_status make_tmap_2d_bf16(CUtensorMap *map, const void *base, uint64_t width, uint64_t rows,
                             uint64_t pitch_elems, uint32_t box_x, uint32_t box_y);
+// Host: a 2-D byte tensor map, 128-byte boxes of box_y rows, 128-byte
+// swizzle in shared memory.
+mb_status make_tmap_2d_u8_sw128(CUtensorMap *map, const void *base, uint64_t width, uint64_t rows,
+                                uint64_t pitch, uint32_t box_y);
 
 }  // namespace mb

@@ -95,39 +95,45 @@ __device__ bool chol_smem(C *A, uint32_t K, uint32_t lda, int *flag) {
   return *flag == 0;
 }
 
-// In-place inverse of the K x K Hermitian positive definite matrix G (leading
-// dim ld) into X by Gauss-Jordan on [G | I] without pivoting: every pivot of
-// a positive definite matrix is real and positive.  The matrix is padded to
-// KP x KP with an identity block.  Thread t holds row t / TPR of [G | I] in
+// Inverse of the K x K Hermitian positive definite matrix G (leading dim ld)
+// into X by in-place Gauss-Jordan without pivoting (every pivot of a
+// positive definite matrix is real and positive): at pivot k the pivot row
+// becomes a_kj / a_kk with a_kk <- 1 / a_kk, and every other row i becomes
+// a_ij - a_ik a_kj' with a_ik <- -a_ik / a_kk, so column k of G is replaced
+// by column k of the inverse and no identity half is carried.  The matrix is
+// padded to KP x KP with an identity block.  Thread t holds row t / TPR in
 // registers, columns t % TPR + TPR m; the pivot row goes through shared
-// memory (prow, two buffers of 2 KP), so each pivot costs one barrier.
+// memory (prow, two buffers of KP), so each pivot costs one barrier.  The
+// register row is rotated by one slot after every TPR pivots, so the pivot
+// column always sits in slot 0 and the loop body indexes registers
+// statically without being unrolled over the row (a short body: the
+// unrolled form stalled on instruction fetch at KP = 64).
 // Returns false when a pivot is not positive (the output is then garbage).
 template <int KP>
 __device__ __forceinline__ bool gj_inverse(const float2 *G, float2 *X, uint32_t K, uint32_t ld,
                                            float2 *prow, int *bad) {
-  constexpr int TPR = kThreads / KP, NC = 2 * KP / TPR;
+  constexpr int TPR = kThreads / KP, NC = KP / TPR;
   const uint32_t i = threadIdx.x / TPR, sub = threadIdx.x % TPR;
+  // v[m] holds column sub + TPR ((m + r) % NC) after r rotations
   float2 v[NC];
 #pragma unroll
   for (int m = 0; m < NC; m++) {
     const uint32_t c = sub + TPR * m;
-    if (m < NC / 2)
-      v[m] = (i < K && c < K) ? G[i * ld + c] : make_float2(i == c ? 1.f : 0.f, 0.f);
-    else
-      v[m] = make_float2(c - KP == i ? 1.f : 0.f, 0.f);
+    v[m] = (i < K && c < K) ? G[i * ld + c] : make_float2(i == c ? 1.f : 0.f, 0.f);
   }
-#pragma unroll
-  for (int mk = 0; mk < NC / 2; mk++) {
 #pragma unroll 1
-    for (uint32_t s = 0; s < (uint32_t)TPR; s++) {
-      const uint32_t k = mk * TPR + s;
+  for (uint32_t r = 0; r < (uint32_t)NC; r++) {
+#pragma unroll
+    for (int s = 0; s < TPR; s++) {
+      const uint32_t k = r * TPR + s;
       float2 f;  // this row's entry in column k
-      f.x = __shfl_sync(0xffffffffu, v[mk].x, s, TPR);
-      f.y = __shfl_sync(0xffffffffu, v[mk].y, s, TPR);
-      float2 *pr = prow + (k & 1) * 2 * KP;
+      f.x = __shfl_sync(0xffffffffu, v[0].x, s, TPR);
+      f.y = __shfl_sync(0xffffffffu, v[0].y, s, TPR);
+      float2 *pr = prow + (k & 1) * KP;
       if (i == k) {
         if (!(f.x > 0.f)) *bad = 1;
         const float inv = __frcp_rn(f.x);
+        if (sub == (uint32_t)s) v[0] = make_float2(1.f, 0.f);
 #pragma unroll
         for (int m = 0; m < NC; m++) {
           v[m].x *= inv;
@@ -137,21 +143,26 @@ __device__ __forceinline__ bool gj_inverse(const float2 *G, float2 *X, uint32_t 
       }
       __syncthreads();
       if (i != k) {
+        if (sub == (uint32_t)s) v[0] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int m = 0; m < NC; m++) {
-          const float2 r = pr[sub + TPR * m];
-          v[m].x -= f.x * r.x - f.y * r.y;
-          v[m].y -= f.x * r.y + f.y * r.x;
+          const float2 w = pr[sub + TPR * m];
+          v[m].x -= f.x * w.x - f.y * w.y;
+          v[m].y -= f.x * w.y + f.y * w.x;
         }
       }
     }
+    const float2 t = v[0];
+#pragma unroll
+    for (int m = 0; m < NC - 1; m++) v[m] = v[m + 1];
+    v[NC - 1] = t;
   }
   __syncthreads();
   const bool ok = *bad == 0;
   if (i < K) {
 #pragma unroll
-    for (int m = NC / 2; m < NC; m++) {
-      const uint32_t c = sub + TPR * m - KP;
+    for (int m = 0; m < NC; m++) {
+      const uint32_t c = sub + TPR * m;
       if (c < K) X[i * ld + c] = v[m];
     }
   }
@@ -162,8 +173,10 @@ __device__ __forceinline__ bool gj_inverse(const float2 *G, float2 *X, uint32_t 
 // C = A B for K x K complex matrices in shared memory (leading dims given);
 // out(i, j, c) receives each entry.  Thread t owns the outputs
 // (t / 16 + 16a, t % 16 + 16b), a, b < T: T*T independent accumulators that
-// share each A and B load.  Needs 256 threads and K <= 16 T.
-template <int T, typename Out>
+// share each A and B load.  Needs 256 threads and K <= 16 T.  HERM: C is
+// known to be Hermitian, so only the 16 x 16 blocks a <= b are computed and
+// the blocks below the diagonal are written as their conjugate transposes.
+template <int T, bool HERM, typename Out>
 __device__ __forceinline__ void cmatmul(const float2 *A, uint32_t lda, const float2 *B, uint32_t ldb,
                                         uint32_t K, Out out) {
   const uint32_t ti = threadIdx.x / 16, tj = threadIdx.x % 16;
@@ -189,6 +202,7 @@ __device__ __forceinline__ void cmatmul(const float2 *A, uint32_t lda, const flo
     for (int a = 0; a < T; a++)
 #pragma unroll
       for (int b = 0; b < T; b++) {
+        if (HERM && a > b) continue;
         acc[a][b].x = fmaf(av[a].x, bv[b].x, fmaf(-av[a].y, bv[b].y, acc[a][b].x));
         acc[a][b].y = fmaf(av[a].x, bv[b].y, fmaf(av[a].y, bv[b].x, acc[a][b].y));
       }
@@ -197,25 +211,29 @@ __device__ __forceinline__ void cmatmul(const float2 *A, uint32_t lda, const flo
   for (int a = 0; a < T; a++)
 #pragma unroll
     for (int b = 0; b < T; b++) {
+      if (HERM && a > b) continue;
       const uint32_t i = ti + 16 * a, j = tj + 16 * b;
-      if (i < K && j < K) out(i, j, acc[a][b]);
+      if (i < K && j < K) {
+        out(i, j, acc[a][b]);
+        if (HERM && a < b) out(j, i, make_float2(acc[a][b].x, -acc[a][b].y));
+      }
     }
 }
 
 // K <= MM / 2: MM = 64 covers K <= 32, MM = 128 covers K <= 64
-template <int MM, typename Out>
+template <int MM, bool HERM = false, typename Out>
 __device__ __forceinline__ void cmatmul_any(const float2 *A, uint32_t lda, const float2 *B, uint32_t ldb,
                                             uint32_t K, Out out) {
   if (MM == 64) {
     if (K <= 16)
-      cmatmul<1>(A, lda, B, ldb, K, out);
+      cmatmul<1, HERM>(A, lda, B, ldb, K, out);
     else
-      cmatmul<2>(A, lda, B, ldb, K, out);
+      cmatmul<2, HERM>(A, lda, B, ldb, K, out);
   } else {
     if (K <= 48)
-      cmatmul<3>(A, lda, B, ldb, K, out);
+      cmatmul<3, HERM>(A, lda, B, ldb, K, out);
     else
-      cmatmul<4>(A, lda, B, ldb, K, out);
+      cmatmul<4, HERM>(A, lda, B, ldb, K, out);
   }
 }
 }  // namespace
@@ -228,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   __shared__ uint32_t tmem_slot;
   __shared__ int flag, fail, piv_bad;
   __shared__ float red[kThreads], red2[kThreads];
-  __shared__ float2 prow[2 * MM];  // Gauss-Jordan pivot rows, two buffers of 2 KP <= MM
+  __shared__ float2 prow[MM];  // Gauss-Jordan pivot rows, two buffers of KP <= MM / 2
 
   constexpr uint32_t tile_bytes = MM * kKT * 2;
   constexpr uint32_t TC = 256;             // TMEM columns: the Gram (MM) or TCH W tiles
@@ -391,7 +409,9 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
           Ts[i * K + j] = make_float2((i == j ? 2.f : 0.f) - s.x, -s.y);
         });
         __syncthreads();
-        cmatmul_any<MM>(xc, ldc, Ts, K, K, [&](uint32_t i, uint32_t j, float2 s) { xn[i * ldn + j] = s; });
+        // X T = 2X - X G X is Hermitian for Hermitian X: upper blocks only
+        cmatmul_any<MM, true>(xc, ldc, Ts, K, K,
+                              [&](uint32_t i, uint32_t j, float2 s) { xn[i * ldn + j] = s; });
         __syncthreads();
         float2 *t = xc;
         xc = xn;

@@ -86,6 +86,14 @@ class UplinkFFT(_FFTBase):
         check(LIB.mb_fft_uplink(self._h, p, code, n_sym, _dev(out, "out"), _stream(stream)),
               "UplinkFFT")
 
+    def uplink_bf16(self, inp, out, row_pitch, stream=None):
+        """Planar BF16 rows out[n_sym][re|im][M][row_pitch] (mb_fft_uplink_bf16)."""
+        p, code, n_sym = _iq(inp, "in", self.bs_num, self.ofdm_ca)
+        if out.dtype != torch.bfloat16 or out.numel() < n_sym * 2 * self.bs_num * row_pitch:
+            raise ValueError("out must hold [n_sym, 2, M, row_pitch] bfloat16")
+        check(LIB.mb_fft_uplink_bf16(self._h, p, code, n_sym, _dev(out, "out"), row_pitch, _stream(stream)),
+              "UplinkFFT.uplink_bf16")
+
 
 class PilotFFT(_FFTBase):
     """fft/fft_op.h:93-110: forward FFT + LS pilot estimate into CSI [G, M, K]."""

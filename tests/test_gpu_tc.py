@@ -109,10 +109,13 @@ CASES = [
     dict(M=32, K=8, N=256, S=200, sg=8, Qm=2, U=3, snr_db=12.0, seed=13, iq_dtype="int16"),
     # antenna tiles streamed through shared memory in the mixed ZF
     dict(M=384, K=64, N=512, S=300, sg=16, Qm=4, U=3, snr_db=30.0, seed=14),
+    # N = 4096: the uplink FFT on the tensor cores
+    dict(M=64, K=16, N=4096, S=3276, sg=16, Qm=6, U=3, snr_db=25.0, seed=17, iq_dtype="int16"),
+    dict(M=32, K=8, N=4096, S=3276, sg=16, Qm=8, U=2, snr_db=32.0, seed=18),
 ]
 
 
-@pytest.mark.parametrize("case", CASES, ids=[f"{c['M']}x{c['K']}Q{c['Qm']}" for c in CASES])
+@pytest.mark.parametrize("case", CASES, ids=[f"{c['M']}x{c['K']}Q{c['Qm']}N{c['N']}" for c in CASES])
 def test_slot_uplink_mixed_vs_oracle(mb, case):
     from megastation_b200 import datagen, slot
     cfg = datagen.CellConfig(**case)
