@@ -135,6 +135,14 @@ mb_status mb_fft_pilot(mb_fft *fft, const void *iq, int iq_dtype,
                        uint32_t n_sym, uint32_t ue_start, mb_c32 *csi,
                        void *stream);
 
+/* Mixed-precision pilot FFT (no reference counterpart): the contract of
+ * mb_fft_pilot; for N = 4096 with a 16-byte aligned input the butterflies
+ * run on the tensor cores (FP16 operands scaled per row by a power of two,
+ * FP32 accumulation), otherwise it is mb_fft_pilot. */
+mb_status mb_fft_pilot_mixed(mb_fft *fft, const void *iq, int iq_dtype,
+                             uint32_t n_sym, uint32_t ue_start, mb_c32 *csi,
+                             void *stream);
+
 /* DownlinkIFFT::operator() (fft/fft_op.cu:167-174, ifft_callback.cuh:21-59):
  * unnormalised inverse FFT of each [M][N] row, then for int16/int8 outputs
  * q = saturate(rint(x * (max+1) / N)); for MB_IQ_F16 / MB_IQ_C32 outputs

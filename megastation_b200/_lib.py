@@ -90,6 +90,7 @@ def _load():
         "mb_fft_uplink": (ST, [VP, VP, I32, U32, VP, VP]),
         "mb_fft_uplink_bf16": (ST, [VP, VP, I32, U32, VP, U32, VP]),
         "mb_fft_pilot": (ST, [VP, VP, I32, U32, U32, VP, VP]),
+        "mb_fft_pilot_mixed": (ST, [VP, VP, I32, U32, U32, VP, VP]),
         "mb_ifft_downlink": (ST, [VP, VP, U32, VP, I32, VP]),
         "mb_zf_create": (ST, [U32, U32, U32, ctypes.POINTER(VP)]),
         "mb_zf_destroy": (ST, [VP]),

@@ -540,10 +540,27 @@ extern "C" mb_status mb_fft_pilot(mb_fft *f, const void *iq, int iq_dtype,
   return launch_fft<kPilot>(f->logn, p, as_stream(stream));
 }
 
-mb_status mb::fft_pilot_fill(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym, mb_c32 *csi,
-                             cudaStream_t st) {
+extern "C" mb_status mb_fft_pilot_mixed(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
+                                        uint32_t ue_start, mb_c32 *csi, void *stream) {
   if (!f || !iq || !csi || !dtype_ok(iq_dtype)) return MB_BAD_ARG;
   if (!f->pilot) return MB_BAD_SHAPE;
+  if (!fft_tc_pilot_supported(f->tc, iq)) return mb_fft_pilot(f, iq, iq_dtype, n_sym, ue_start, csi, stream);
+  const DeviceTables *tab = device_tables();
+  return fft_tc_pilot(f->tc, iq, iq_dtype, n_sym, f->d.bs_num, f->d.ofdm_num, f->d.ue_num, f->d.sc_group,
+                      ue_start, 0, f->pilot, reinterpret_cast<float2 *>(csi), tab ? tab->err : nullptr,
+                      as_stream(stream));
+}
+
+mb_status mb::fft_pilot_fill(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym, mb_c32 *csi,
+                             cudaStream_t st, bool tensor) {
+  if (!f || !iq || !csi || !dtype_ok(iq_dtype)) return MB_BAD_ARG;
+  if (!f->pilot) return MB_BAD_SHAPE;
+  if (tensor && fft_tc_pilot_supported(f->tc, iq)) {
+    const uint32_t S = f->d.ofdm_num, sg = f->d.sc_group, G = (S + sg - 1) / sg;
+    const DeviceTables *tab = device_tables();
+    return fft_tc_pilot(f->tc, iq, iq_dtype, n_sym, f->d.bs_num, S, f->d.ue_num, sg, 0, G >= 2 ? S % sg : 0,
+                        f->pilot, reinterpret_cast<float2 *>(csi), tab ? tab->err : nullptr, st);
+  }
   FftParams p{};
   p.in = iq;
   p.out = csi;

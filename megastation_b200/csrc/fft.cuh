@@ -10,9 +10,10 @@ mb_status fft_uplink_lp(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
                         void *y_lp, uint32_t S_pad, cudaStream_t st);
 
 // pilot FFT of n_sym comb-pilot symbols (ue_start 0) that also fills the
-// short last group's users without a pilot from group G-2 (zf_fill_tail)
+// short last group's users without a pilot from group G-2 (zf_fill_tail);
+// tensor: the FP16 tensor-core FFT where it applies (mixed precision)
 mb_status fft_pilot_fill(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym, mb_c32 *csi,
-                         cudaStream_t st);
+                         cudaStream_t st, bool tensor = false);
 
 // tensor-core FFT for N = 4096 (fft_tc.cu): a plan holds the DFT operands
 // with the FFT shift of `start` folded in; null for other N
@@ -25,5 +26,11 @@ bool fft_tc_lp_supported(const FftTcPlan *plan, const void *iq, uint32_t S_pad, 
 mb_status fft_tc_uplink_lp(const FftTcPlan *plan, const void *iq, int iq_dtype, uint32_t rows, uint32_t M,
                            uint32_t S, void *y_lp, uint32_t S_pad, int *err, cudaStream_t st,
                            uint32_t upc = 0);
+// pilot FFT of n_sym comb-pilot symbols into csi [G][M][K] as mb_fft_pilot,
+// with the short-last-group fill when tail_rem != 0 (fft_pilot_fill)
+bool fft_tc_pilot_supported(const FftTcPlan *plan, const void *iq);
+mb_status fft_tc_pilot(const FftTcPlan *plan, const void *iq, int iq_dtype, uint32_t n_sym, uint32_t M, uint32_t S,
+                       uint32_t K, uint32_t sg, uint32_t ue_start, uint32_t tail_rem, const float2 *pilot,
+                       float2 *csi, int *err, cudaStream_t st, uint32_t upc = 0);
 
 }  // namespace mb

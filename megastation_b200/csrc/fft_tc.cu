@@ -73,10 +73,16 @@ __host__ __device__ constexpr uint32_t mnmaj_off(uint32_t mn, uint32_t kk) {
   return (kk / 8) * 2048 + (mn / 8) * 128 + (kk % 8) * 16 + (mn % 8) * 2;
 }
 
+enum FtMode { kFtUplinkLP = 0, kFtPilot = 1 };
+
 struct FtParams {
   uint32_t rows;        // n_sym * M rows of 4096 samples
   uint32_t M, S, S_pad;
-  __nv_bfloat16 *out;   // [n_sym][re|im][M][S_pad]
+  __nv_bfloat16 *out;   // uplink: [n_sym][re|im][M][S_pad]
+  float2 *csi;          // pilot: [G][M][K]
+  const float2 *pilot;  // pilot: sign of each subcarrier
+  uint32_t K, sg, ue_start, tail_rem, G;
+  uint32_t sg_magic;    // floor(i / sg) = umulhi(i, sg_magic) for i < 2^13
   const uint8_t *mats;
   const float2 *tw;
   uint32_t c;
@@ -184,9 +190,9 @@ __device__ __forceinline__ bool ft_wait(uint64_t *bar, uint32_t parity, volatile
   return true;
 }
 
-template <int DT>
+template <int DT, int MODE>
 __global__ void __launch_bounds__(kFtThreads, 1)
-    fft_tc_lp_kernel(const __grid_constant__ CUtensorMap in_map, const FtParams p) {
+    fft_tc_kernel(const __grid_constant__ CUtensorMap in_map, const FtParams p) {
   extern __shared__ __align__(1024) uint8_t ft_smem[];
   // F, AZ and the ring start on 1024-byte boundaries (the swizzled TMA boxes
   // need them); the staging rows follow
@@ -301,14 +307,15 @@ __global__ void __launch_bounds__(kFtThreads, 1)
         // the ring slot of unit i takes unit i + 2 once unit i is converted
         if (!ft_wait(&a_ready, i & 1, &s_fail)) break;
         issue_load(i + 2);
-        if (i > 0) {
+        if (MODE == kFtUplinkLP && i > 0) {
           if (!ft_wait(&st_ready, (i - 1) & 1, &s_fail)) break;
           issue_stores(i - 1);
           bulk_wait_read();
           mbar_arrive(&st_done);
         }
       }
-      if (!s_fail && ft_wait(&st_ready, (n_units - 1) & 1, &s_fail)) issue_stores(n_units - 1);
+      if (MODE == kFtUplinkLP && !s_fail && ft_wait(&st_ready, (n_units - 1) & 1, &s_fail))
+        issue_stores(n_units - 1);
       bulk_wait_all();
       if (s_fail) {
         // a wait ran out: record it and let the loads in flight land (bounded)
@@ -372,6 +379,28 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       float vr[16], vi[16];
       tc::tmem_ld16(tl + 128 + 16 * part, vr);
       tc::tmem_ld16(tl + 192 + 16 * part, vi);
+      if constexpr (MODE == kFtPilot) {
+        // LS estimate conj(X) p of subcarrier sc for user u0 + sc % sg into
+        // csi[sc / sg][b][u] (fft_callback.cuh:76-108); a user with no pilot
+        // in the short last group takes its estimate from group G-2
+        const uint32_t row = 2 * (u_begin + i) + s_r;
+        if (row < p.rows) {
+          const uint32_t sym = row / p.M, b = row - sym * p.M, u0 = p.ue_start + sym * p.sg;
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const uint32_t sc = (s_base + 64 * j) & (kFtN - 1);
+            if (sc >= p.S) continue;
+            const uint32_t g = __umulhi(sc, p.sg_magic), sl = sc - g * p.sg, uu = u0 + sl;
+            if (uu >= p.K) continue;
+            const float2 ps = __ldg(p.pilot + sc);
+            const float x = vr[j] * inv, y = vi[j] * inv;
+            const float2 e = make_float2(x * ps.x + y * ps.y, x * ps.y - y * ps.x);
+            p.csi[((uint64_t)g * p.M + b) * p.K + uu] = e;
+            if (p.tail_rem && g + 2 == p.G && sl >= p.tail_rem) p.csi[((uint64_t)(g + 1) * p.M + b) * p.K + uu] = e;
+          }
+        }
+        return;
+      }
       if (pairs) {
 #pragma unroll
         for (int j = 0; j < 16; j++) {
@@ -444,9 +473,9 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       // (b) GEMM-2 epilogue of the previous unit into the staging rows,
       // once the bulk copies of the unit before it have read them
       if (i > 0) {
-        if (i > 1) wait_ok(&st_done, (i - 2) & 1);
+        if (MODE == kFtUplinkLP && i > 1) wait_ok(&st_done, (i - 2) & 1);
         if (ok) store_unit(i - 1);
-        else arrive(&st_ready);
+        else if (MODE == kFtUplinkLP) arrive(&st_ready);
       }
       // (c) GEMM-1 epilogue: twiddle into the GEMM-2 operand Z
       wait_ok(&d1_full, i & 1);
@@ -477,7 +506,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     compute_sync();
     wait_ok(&d2_full, (n_units - 1) & 1);
     tc::fence_after_sync();
-    if (n_units > 1) wait_ok(&st_done, (n_units - 2) & 1);
+    if (MODE == kFtUplinkLP && n_units > 1) wait_ok(&st_done, (n_units - 2) & 1);
     if (ok) store_unit(n_units - 1);
   }
   tc::fence_before_sync();
@@ -486,23 +515,56 @@ __global__ void __launch_bounds__(kFtThreads, 1)
 }
 
 using FtKernel = void (*)(const CUtensorMap, const FtParams);
+template <int MODE>
 FtKernel fft_tc_kernel_of(int dt) {
   switch (dt) {
-    case MB_IQ_C32: return fft_tc_lp_kernel<MB_IQ_C32>;
-    case MB_IQ_I16: return fft_tc_lp_kernel<MB_IQ_I16>;
-    case MB_IQ_I8: return fft_tc_lp_kernel<MB_IQ_I8>;
-    default: return fft_tc_lp_kernel<MB_IQ_F16>;
+    case MB_IQ_C32: return fft_tc_kernel<MB_IQ_C32, MODE>;
+    case MB_IQ_I16: return fft_tc_kernel<MB_IQ_I16, MODE>;
+    case MB_IQ_I8: return fft_tc_kernel<MB_IQ_I8, MODE>;
+    default: return fft_tc_kernel<MB_IQ_F16, MODE>;
   }
 }
 
-mb_status fft_tc_configure(int dt, int dev) {
-  static std::atomic<uint64_t> configured[4] = {};
-  const int which = dt == MB_IQ_C32 ? 0 : dt == MB_IQ_I16 ? 1 : dt == MB_IQ_I8 ? 2 : 3;
+// raises the dynamic shared memory limit of a (type, mode) kernel once per
+// device, and returns the device's SM count
+mb_status fft_tc_configure(int dt, int mode, int dev, int *sms) {
+  static std::atomic<uint64_t> configured[8] = {};
+  static std::atomic<int> sm_count[64] = {};
+  const int which = (dt == MB_IQ_C32 ? 0 : dt == MB_IQ_I16 ? 1 : dt == MB_IQ_I8 ? 2 : 3) + 4 * mode;
   const uint64_t bit = 1ull << (dev & 63);
-  if (configured[which].load() & bit) return MB_OK;
-  MB_CUDA_TRY(cudaFuncSetAttribute(fft_tc_kernel_of(dt), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kFtSmem));
-  configured[which].fetch_or(bit);
+  if (!(configured[which].load() & bit)) {
+    const FtKernel k = mode == kFtPilot ? fft_tc_kernel_of<kFtPilot>(dt) : fft_tc_kernel_of<kFtUplinkLP>(dt);
+    MB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFtSmem));
+    int n = 0;
+    MB_CUDA_TRY(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    sm_count[dev & 63].store(n);
+    configured[which].fetch_or(bit);
+  }
+  *sms = sm_count[dev & 63].load();
+  return MB_OK;
+}
+
+// one wave: units spread evenly over at most one CTA per SM
+mb_status fft_tc_launch(int mode, const FftTcPlan *pl, const void *iq, int iq_dtype, FtParams &p,
+                        cudaStream_t st, uint32_t upc) {
+  int dev = 0, sms = 0;
+  MB_CUDA_TRY(cudaGetDevice(&dev));
+  mb_status r = fft_tc_configure(iq_dtype, mode, dev, &sms);
+  if (r != MB_OK) return r;
+  const uint32_t bytes = iq_dtype == MB_IQ_C32 ? 8 : iq_dtype == MB_IQ_I8 ? 2 : 4;
+  // the rows as 64-sample n1 rows of 64 * bytes bytes, read in 128-byte boxes
+  CUtensorMap map;
+  r = make_tmap_2d_u8_sw128(&map, iq, 64ull * bytes, (uint64_t)p.rows * 64, 64ull * bytes, 64);
+  if (r != MB_OK) return r;
+  p.mats = pl->mats;
+  p.tw = pl->tw;
+  p.c = pl->c;
+  p.units = (p.rows + 1) / 2;
+  p.upc = upc ? upc : (p.units + (uint32_t)max(sms, 1) - 1) / (uint32_t)max(sms, 1);
+  const uint32_t grid = (p.units + p.upc - 1) / p.upc;
+  const FtKernel k = mode == kFtPilot ? fft_tc_kernel_of<kFtPilot>(iq_dtype) : fft_tc_kernel_of<kFtUplinkLP>(iq_dtype);
+  k<<<grid, kFtThreads, kFtSmem, st>>>(map, p);
+  MB_LAUNCH_CHECK();
   return MB_OK;
 }
 
@@ -563,31 +625,39 @@ mb_status fft_tc_uplink_lp(const FftTcPlan *pl, const void *iq, int iq_dtype, ui
                            uint32_t upc) {
   if (!fft_tc_lp_supported(pl, iq, S_pad, y_lp) || S > kFtN || S > S_pad) return MB_BAD_ARG;
   if (rows == 0) return MB_OK;
-  int dev = 0;
-  MB_CUDA_TRY(cudaGetDevice(&dev));
-  mb_status r = fft_tc_configure(iq_dtype, dev);
-  if (r != MB_OK) return r;
-  const uint32_t bytes = iq_dtype == MB_IQ_C32 ? 8 : iq_dtype == MB_IQ_I8 ? 2 : 4;
-  // the rows as 64-sample n1 rows of 64 * bytes bytes, read in 128-byte boxes
-  CUtensorMap map;
-  r = make_tmap_2d_u8_sw128(&map, iq, 64ull * bytes, (uint64_t)rows * 64, 64ull * bytes, 64);
-  if (r != MB_OK) return r;
   FtParams p{};
   p.rows = rows;
   p.M = M;
   p.S = S;
   p.S_pad = S_pad;
   p.out = reinterpret_cast<__nv_bfloat16 *>(y_lp);
-  p.mats = pl->mats;
-  p.tw = pl->tw;
-  p.c = pl->c;
-  p.units = (rows + 1) / 2;
-  p.upc = upc ? upc : 11;
   p.err = err;
-  const uint32_t grid = (p.units + p.upc - 1) / p.upc;
-  fft_tc_kernel_of(iq_dtype)<<<grid, kFtThreads, kFtSmem, st>>>(map, p);
-  MB_LAUNCH_CHECK();
-  return MB_OK;
+  return fft_tc_launch(kFtUplinkLP, pl, iq, iq_dtype, p, st, upc);
+}
+
+bool fft_tc_pilot_supported(const FftTcPlan *pl, const void *iq) {
+  return pl && (reinterpret_cast<uintptr_t>(iq) & 15) == 0;
+}
+
+mb_status fft_tc_pilot(const FftTcPlan *pl, const void *iq, int iq_dtype, uint32_t n_sym, uint32_t M, uint32_t S,
+                       uint32_t K, uint32_t sg, uint32_t ue_start, uint32_t tail_rem, const float2 *pilot,
+                       float2 *csi, int *err, cudaStream_t st, uint32_t upc) {
+  if (!fft_tc_pilot_supported(pl, iq) || S > kFtN || sg == 0 || sg >= kFtN || !pilot || !csi) return MB_BAD_ARG;
+  if (n_sym == 0 || M == 0) return MB_OK;
+  FtParams p{};
+  p.rows = n_sym * M;
+  p.M = M;
+  p.S = S;
+  p.csi = csi;
+  p.pilot = pilot;
+  p.K = K;
+  p.sg = sg;
+  p.ue_start = ue_start;
+  p.tail_rem = tail_rem;
+  p.G = (S + sg - 1) / sg;
+  p.sg_magic = (uint32_t)((0x100000000ull + sg - 1) / sg);
+  p.err = err;
+  return fft_tc_launch(kFtPilot, pl, iq, iq_dtype, p, st, upc);
 }
 
 }  // namespace mb

@@ -109,6 +109,15 @@ class PilotFFT(_FFTBase):
         check(LIB.mb_fft_pilot(self._h, p, code, n_sym, ue_start, _dev(out, "out"), _stream(stream)),
               "PilotFFT")
 
+    def mixed(self, inp, out, ue_start=0, stream=None):
+        """The same estimate with the tensor-core FFT (mb_fft_pilot_mixed)."""
+        p, code, n_sym = _iq(inp, "in", self.bs_num, self.ofdm_ca)
+        G = (self.ofdm_num + self.sc_group - 1) // self.sc_group
+        if out.dtype != torch.complex64 or out.numel() < G * self.bs_num * self.ue_num:
+            raise ValueError("out must hold CSI [G, M, K] complex64")
+        check(LIB.mb_fft_pilot_mixed(self._h, p, code, n_sym, ue_start, _dev(out, "out"), _stream(stream)),
+              "PilotFFT.mixed")
+
 
 class DownlinkIFFT(_FFTBase):
     """fft/fft_op.h:112-120: inverse FFT + quantise, [..., M, N] c64 -> [..., M, N, 2]."""

@@ -98,3 +98,27 @@ def test_fft_bf16_fp32_kernel(mb, N, S, pitch):
     got, o, start = run_bf16(mb, x, N, S, 3, 2, pitch)
     check_rows(got, x, N, S, start)
     assert (o[..., S:] == 7.0).all()
+
+
+@pytest.mark.parametrize("dtype,M,K,sg", [("c64", 4, 20, 16), ("int16", 5, 32, 16), ("c64", 3, 8, 8)])
+def test_pilot_fft_mixed_vs_oracle(mb, dtype, M, K, sg):
+    # LS pilot estimates from the tensor-core FFT: within 2e-3 of the RMS
+    # estimate (FP16 operands) of the FP64 oracle
+    N, S = 4096, 3276
+    rng = np.random.default_rng(K + M)
+    P = (K + sg - 1) // sg
+    x = (rng.standard_normal((P, M, N)) + 1j * rng.standard_normal((P, M, N))) * 0.1
+    iq = make_iq(x, dtype)
+    start = (N - S) // 2
+    G = (S + sg - 1) // sg
+    csi = torch.zeros(G, M, K, dtype=torch.complex64, device="cuda")
+    mb.PilotFFT(start, N, S, M, K, sg).mixed(torch.from_numpy(np.ascontiguousarray(iq)).cuda(), csi)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    ref = np.zeros((G, M, K), np.complex64)
+    ps = orc.pilot_sign(S)
+    for p in range(P):
+        orc.pilot_fft(iq[p], N, S, start, K, sg, p * sg, ps, ref)
+    got = csi.cpu().numpy()
+    scale = np.sqrt(np.mean(np.abs(ref) ** 2))
+    assert np.abs(got - ref).max() <= 2e-3 * scale
