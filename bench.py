@@ -183,11 +183,14 @@ def roofline(cfg, args, st, n_valid, hrow):
                      "bytes": (cfg.G * img_group if mixed else cfg.G * cfg.M * cfg.K * 8)
                      + syms * (cfg.M * cfg.S * out_b + cfg.K * (n_valid * 2 + hrow))},
     }
-    names = {"fft_uplink": "fft_kernel<12, uplink LP>" if mixed else "fft_kernel<12, uplink>",
+    tc_fft = mixed and cfg.N == 4096  # the tensor-core FFT takes the mixed uplink at N = 4096
+    names = {"fft_uplink": ("fft_tc_kernel<uplink LP>" if tc_fft else "fft_kernel<12, uplink LP>") if mixed
+             else "fft_kernel<12, uplink>",
              "fft_pilot": "fft_kernel<12, pilot>",
              "zf": "zf_mixed_kernel<64>" if mixed else "zf_chol_kernel<float>",
              "equalize": "equalize_tc_kernel<64, 6>" if mixed else "equalize_fp32_kernel"}
-    profiles = {"fft_uplink": "fft_uplink_lp_4096x256", "equalize": "equalize_tc_256x32",
+    profiles = {"fft_uplink": "fft_tc_uplink_4096x256" if tc_fft else "fft_uplink_lp_4096x256",
+                "equalize": "equalize_tc_256x32",
                 "zf": "zf_mixed_256x32", "fft_pilot": "fft_uplink_lp_4096x256"}
     for key, v in k.items():
         sec = v["ms"] / 1e3
