@@ -168,10 +168,14 @@ def roofline(cfg, args, st, n_valid, hrow):
     out_b = 4 if mixed else 8                          # BF16 planar or c32 per subcarrier
     tc = {"MM": 64 if 2 * cfg.K <= 64 else 128, "Mp": (cfg.M + 63) // 64 * 64}
     img_group = 2 * tc["Mp"] * tc["MM"] * 2
+    tc_fft = mixed and cfg.N == 4096  # the tensor-core FFT takes the mixed uplink at N = 4096 ...
+    # ... and, in the slot, the pilot rows too (one launch with the first batch)
+    pilot_rows = cfg.P * cfg.M * calls / n_fft if tc_fft else 0
     k = {
         "fft_uplink": {"ms": st["uplink_fft"] / n_fft, "per_slot_ms": st["uplink_fft"] / calls,
-                       "bound": "hbm", "units": rows, "unit_name": "antenna row",
-                       "bytes": rows * (cfg.N * 8 + cfg.S * out_b)},
+                       "bound": "hbm", "units": rows + pilot_rows, "unit_name": "antenna row",
+                       "bytes": rows * (cfg.N * 8 + cfg.S * out_b)
+                       + pilot_rows * cfg.N * 8 + (cfg.G * cfg.M * cfg.K * 8 * calls / n_fft if tc_fft else 0)},
         "fft_pilot": {"ms": st["pilot_fft"] / calls, "per_slot_ms": st["pilot_fft"] / calls,
                       "bound": "hbm", "units": cfg.P * cfg.M, "unit_name": "pilot row",
                       "bytes": cfg.P * cfg.M * (cfg.N * 8) + cfg.G * cfg.M * cfg.K * 8},
@@ -183,7 +187,8 @@ def roofline(cfg, args, st, n_valid, hrow):
                      "bytes": (cfg.G * img_group if mixed else cfg.G * cfg.M * cfg.K * 8)
                      + syms * (cfg.M * cfg.S * out_b + cfg.K * (n_valid * 2 + hrow))},
     }
-    tc_fft = mixed and cfg.N == 4096  # the tensor-core FFT takes the mixed uplink at N = 4096
+    if tc_fft:
+        del k["fft_pilot"]  # the pilot rows go through the uplink FFT launch
     names = {"fft_uplink": ("fft_tc_kernel<uplink LP>" if tc_fft else "fft_kernel<12, uplink LP>") if mixed
              else "fft_kernel<12, uplink>",
              "fft_pilot": "fft_kernel<12, pilot>",

@@ -540,6 +540,19 @@ extern "C" mb_status mb_fft_pilot(mb_fft *f, const void *iq, int iq_dtype,
   return launch_fft<kPilot>(f->logn, p, as_stream(stream));
 }
 
+bool mb::fft_slot_tc_ok(mb_fft *f, const void *iq, uint32_t S_pad, const void *y_lp) {
+  return f && f->pilot && fft_tc_lp_supported(f->tc, iq, S_pad, y_lp);
+}
+
+mb_status mb::fft_slot_tc(mb_fft *f, const void *iq, int iq_dtype, uint32_t P, uint32_t U, mb_c32 *csi,
+                          void *y_lp, uint32_t S_pad, cudaStream_t st) {
+  if (!fft_slot_tc_ok(f, iq, S_pad, y_lp) || !dtype_ok(iq_dtype) || !csi) return MB_BAD_ARG;
+  const uint32_t S = f->d.ofdm_num, sg = f->d.sc_group, G = (S + sg - 1) / sg;
+  const DeviceTables *tab = device_tables();
+  return fft_tc_slot(f->tc, iq, iq_dtype, P, U, f->d.bs_num, S, f->d.ue_num, sg, G >= 2 ? S % sg : 0, f->pilot,
+                     reinterpret_cast<float2 *>(csi), y_lp, S_pad, tab ? tab->err : nullptr, st);
+}
+
 extern "C" mb_status mb_fft_pilot_mixed(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
                                         uint32_t ue_start, mb_c32 *csi, void *stream) {
   if (!f || !iq || !csi || !dtype_ok(iq_dtype)) return MB_BAD_ARG;

@@ -15,6 +15,13 @@ mb_status fft_uplink_lp(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
 mb_status fft_pilot_fill(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym, mb_c32 *csi,
                          cudaStream_t st, bool tensor = false);
 
+// the slot's P pilot symbols and first U uplink symbols (adjacent rows of
+// iq) in one tensor-core launch: CSI with the tail fill, and planar BF16
+// rows; fft_slot_tc_ok tells whether it applies (N = 4096, alignment)
+bool fft_slot_tc_ok(mb_fft *f, const void *iq, uint32_t S_pad, const void *y_lp);
+mb_status fft_slot_tc(mb_fft *f, const void *iq, int iq_dtype, uint32_t P, uint32_t U, mb_c32 *csi, void *y_lp,
+                      uint32_t S_pad, cudaStream_t st);
+
 // tensor-core FFT for N = 4096 (fft_tc.cu): a plan holds the DFT operands
 // with the FFT shift of `start` folded in; null for other N
 struct FftTcPlan;
@@ -32,5 +39,10 @@ bool fft_tc_pilot_supported(const FftTcPlan *plan, const void *iq);
 mb_status fft_tc_pilot(const FftTcPlan *plan, const void *iq, int iq_dtype, uint32_t n_sym, uint32_t M, uint32_t S,
                        uint32_t K, uint32_t sg, uint32_t ue_start, uint32_t tail_rem, const float2 *pilot,
                        float2 *csi, int *err, cudaStream_t st, uint32_t upc = 0);
+// one launch for a slot's P comb-pilot symbols (CSI out, tail fill with
+// tail_rem) followed by U uplink symbols (planar BF16 rows out)
+mb_status fft_tc_slot(const FftTcPlan *plan, const void *iq, int iq_dtype, uint32_t P, uint32_t U, uint32_t M,
+                      uint32_t S, uint32_t K, uint32_t sg, uint32_t tail_rem, const float2 *pilot, float2 *csi,
+                      void *y_lp, uint32_t S_pad, int *err, cudaStream_t st);
 
 }  // namespace mb

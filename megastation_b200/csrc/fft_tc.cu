@@ -18,7 +18,7 @@
 // component lies in [128, 256): then |Y| and |Z| stay below 2^15.5, inside
 // the FP16 range, and the scale is undone exactly before the BF16 store.
 //
-// One CTA per SM takes `upc` consecutive units of two rows, with 224 KB of
+// One CTA per SM takes every gridDim-th unit of two rows, with 224 KB of
 // shared memory (F, one GEMM operand buffer, an output staging buffer and a
 // two-unit input ring) and 256 TMEM columns (the two GEMM accumulators).
 // Warp 8 is the control warp: one thread streams the units' rows into the
@@ -73,12 +73,12 @@ __host__ __device__ constexpr uint32_t mnmaj_off(uint32_t mn, uint32_t kk) {
   return (kk / 8) * 2048 + (mn / 8) * 128 + (kk % 8) * 16 + (mn % 8) * 2;
 }
 
-enum FtMode { kFtUplinkLP = 0, kFtPilot = 1 };
-
 struct FtParams {
-  uint32_t rows;        // n_sym * M rows of 4096 samples
+  uint32_t rows;        // rows of 4096 samples, [symbol][M]
+  uint32_t pilot_rows;  // the first pilot_rows are comb-pilot rows (CSI out),
+                        // the others uplink rows (planar BF16 out)
   uint32_t M, S, S_pad;
-  __nv_bfloat16 *out;   // uplink: [n_sym][re|im][M][S_pad]
+  __nv_bfloat16 *out;   // uplink: [n_sym][re|im][M][S_pad], row (row - pilot_rows)
   float2 *csi;          // pilot: [G][M][K]
   const float2 *pilot;  // pilot: sign of each subcarrier
   uint32_t K, sg, ue_start, tail_rem, G;
@@ -190,7 +190,7 @@ __device__ __forceinline__ bool ft_wait(uint64_t *bar, uint32_t parity, volatile
   return true;
 }
 
-template <int DT, int MODE>
+template <int DT>
 __global__ void __launch_bounds__(kFtThreads, 1)
     fft_tc_kernel(const __grid_constant__ CUtensorMap in_map, const FtParams p) {
   extern __shared__ __align__(1024) uint8_t ft_smem[];
@@ -205,9 +205,11 @@ __global__ void __launch_bounds__(kFtThreads, 1)
   using F = Fmt<DT>;
 
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
-  const uint32_t u_begin = blockIdx.x * p.upc;
-  if (u_begin >= p.units) return;
-  const uint32_t n_units = min(p.upc, p.units - u_begin);
+  // this CTA's units: blockIdx.x, blockIdx.x + gridDim.x, ... (strided, so
+  // the pilot rows at the front spread over all CTAs)
+  if (blockIdx.x >= p.units) return;
+  const uint32_t n_units = (p.units - blockIdx.x + gridDim.x - 1) / gridDim.x;
+  auto unit_of = [&](uint32_t i) { return blockIdx.x + i * gridDim.x; };
 
   if (tid == kFtCompute) {
     tc::mbar_init(&bar_mats, 1);
@@ -229,9 +231,10 @@ __global__ void __launch_bounds__(kFtThreads, 1)
   tc::fence_after_sync();
   const uint32_t tmem = tmem_slot;  // D1: columns 0..127, D2: 128..255
 
-  // output rows of unit u: (row, plane) -> global and staging addresses
-  auto out_row = [&](uint32_t u, uint32_t r, uint32_t pl) {
-    const uint32_t row = 2 * u + r, sym = row / p.M, b = row - sym * p.M;
+  // planar BF16 output row of uplink row lrow (rows counted after the
+  // pilot rows), plane pl
+  auto out_row = [&](uint32_t lrow, uint32_t pl) {
+    const uint32_t sym = lrow / p.M, b = lrow - sym * p.M;
     return p.out + ((uint64_t)(sym * 2 + pl) * p.M + b) * p.S_pad;
   };
   const uint32_t S8 = (p.S + 7) & ~7u;  // columns written by the bulk copies (<= S_pad)
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       uint32_t loads[2] = {0, 0};
       auto issue_load = [&](uint32_t i) {
         if (i >= n_units) return;
-        const uint32_t u = u_begin + i;
+        const uint32_t u = unit_of(i);
         loads[i & 1]++;
         uint8_t *slot = sRing + (i & 1) * kStage;
         tc::mbar_arrive_expect_tx(&full[i & 1], F::kUnitBytes);
@@ -292,10 +295,13 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       // staged rows hold all 4096 bins in subcarrier order; the first
       // S rounded up to 8 go out by bulk copy (within the row pitch)
       auto issue_stores = [&](uint32_t i) {
-        const uint32_t u = u_begin + i;
+        const uint32_t u = unit_of(i);
         for (uint32_t r = 0; r < 2; r++) {
-          if (2 * u + r >= p.rows) break;
-          for (uint32_t pl = 0; pl < 2; pl++) bulk_s2g(out_row(u, r, pl), sStg + (2 * r + pl) * kStgPitch, S8 * 2);
+          const uint32_t row = 2 * u + r;
+          if (row >= p.rows) break;
+          if (row < p.pilot_rows) continue;
+          for (uint32_t pl = 0; pl < 2; pl++)
+            bulk_s2g(out_row(row - p.pilot_rows, pl), sStg + (2 * r + pl) * kStgPitch, S8 * 2);
         }
         bulk_commit();
       };
@@ -307,15 +313,14 @@ __global__ void __launch_bounds__(kFtThreads, 1)
         // the ring slot of unit i takes unit i + 2 once unit i is converted
         if (!ft_wait(&a_ready, i & 1, &s_fail)) break;
         issue_load(i + 2);
-        if (MODE == kFtUplinkLP && i > 0) {
+        if (i > 0) {
           if (!ft_wait(&st_ready, (i - 1) & 1, &s_fail)) break;
           issue_stores(i - 1);
           bulk_wait_read();
           mbar_arrive(&st_done);
         }
       }
-      if (MODE == kFtUplinkLP && !s_fail && ft_wait(&st_ready, (n_units - 1) & 1, &s_fail))
-        issue_stores(n_units - 1);
+      if (!s_fail && ft_wait(&st_ready, (n_units - 1) & 1, &s_fail)) issue_stores(n_units - 1);
       bulk_wait_all();
       if (s_fail) {
         // a wait ran out: record it and let the loads in flight land (bounded)
@@ -379,29 +384,33 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       float vr[16], vi[16];
       tc::tmem_ld16(tl + 128 + 16 * part, vr);
       tc::tmem_ld16(tl + 192 + 16 * part, vi);
-      if constexpr (MODE == kFtPilot) {
+      const uint32_t row = 2 * unit_of(i) + s_r;  // the same for the whole warp
+      if (row < p.pilot_rows) {
         // LS estimate conj(X) p of subcarrier sc for user u0 + sc % sg into
         // csi[sc / sg][b][u] (fft_callback.cuh:76-108); a user with no pilot
-        // in the short last group takes its estimate from group G-2
-        const uint32_t row = 2 * (u_begin + i) + s_r;
-        if (row < p.rows) {
-          const uint32_t sym = row / p.M, b = row - sym * p.M, u0 = p.ue_start + sym * p.sg;
+        // in the short last group takes its estimate from group G-2.  The
+        // pilot signs are all loaded before any branch, so their latencies
+        // overlap.
+        const uint32_t sym = row / p.M, b = row - sym * p.M, u0 = p.ue_start + sym * p.sg;
 #pragma unroll
-          for (int j = 0; j < 16; j++) {
-            const uint32_t sc = (s_base + 64 * j) & (kFtN - 1);
-            if (sc >= p.S) continue;
+        for (int jb = 0; jb < 16; jb += 8) {
+          float2 ps[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) ps[j] = __ldg(p.pilot + min((s_base + 64 * (jb + j)) & (kFtN - 1), p.S - 1));
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const uint32_t sc = (s_base + 64 * (jb + j)) & (kFtN - 1);
             const uint32_t g = __umulhi(sc, p.sg_magic), sl = sc - g * p.sg, uu = u0 + sl;
-            if (uu >= p.K) continue;
-            const float2 ps = __ldg(p.pilot + sc);
-            const float x = vr[j] * inv, y = vi[j] * inv;
-            const float2 e = make_float2(x * ps.x + y * ps.y, x * ps.y - y * ps.x);
-            p.csi[((uint64_t)g * p.M + b) * p.K + uu] = e;
-            if (p.tail_rem && g + 2 == p.G && sl >= p.tail_rem) p.csi[((uint64_t)(g + 1) * p.M + b) * p.K + uu] = e;
+            const float x = vr[jb + j] * inv, y = vi[jb + j] * inv;
+            const float2 e = make_float2(x * ps[j].x + y * ps[j].y, x * ps[j].y - y * ps[j].x);
+            if (sc < p.S && uu < p.K) {
+              float2 *d = p.csi + ((uint64_t)g * p.M + b) * p.K + uu;
+              *d = e;
+              if (p.tail_rem && g + 2 == p.G && sl >= p.tail_rem) d[(uint64_t)p.M * p.K] = e;
+            }
           }
         }
-        return;
-      }
-      if (pairs) {
+      } else if (pairs) {
 #pragma unroll
         for (int j = 0; j < 16; j++) {
           const uint32_t own = bf2_bits(vr[j] * inv, vi[j] * inv);
@@ -473,9 +482,9 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       // (b) GEMM-2 epilogue of the previous unit into the staging rows,
       // once the bulk copies of the unit before it have read them
       if (i > 0) {
-        if (MODE == kFtUplinkLP && i > 1) wait_ok(&st_done, (i - 2) & 1);
+        if (i > 1) wait_ok(&st_done, (i - 2) & 1);
         if (ok) store_unit(i - 1);
-        else if (MODE == kFtUplinkLP) arrive(&st_ready);
+        else arrive(&st_ready);
       }
       // (c) GEMM-1 epilogue: twiddle into the GEMM-2 operand Z
       wait_ok(&d1_full, i & 1);
@@ -506,7 +515,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     compute_sync();
     wait_ok(&d2_full, (n_units - 1) & 1);
     tc::fence_after_sync();
-    if (MODE == kFtUplinkLP && n_units > 1) wait_ok(&st_done, (n_units - 2) & 1);
+    if (n_units > 1) wait_ok(&st_done, (n_units - 2) & 1);
     if (ok) store_unit(n_units - 1);
   }
   tc::fence_before_sync();
@@ -515,26 +524,25 @@ __global__ void __launch_bounds__(kFtThreads, 1)
 }
 
 using FtKernel = void (*)(const CUtensorMap, const FtParams);
-template <int MODE>
 FtKernel fft_tc_kernel_of(int dt) {
   switch (dt) {
-    case MB_IQ_C32: return fft_tc_kernel<MB_IQ_C32, MODE>;
-    case MB_IQ_I16: return fft_tc_kernel<MB_IQ_I16, MODE>;
-    case MB_IQ_I8: return fft_tc_kernel<MB_IQ_I8, MODE>;
-    default: return fft_tc_kernel<MB_IQ_F16, MODE>;
+    case MB_IQ_C32: return fft_tc_kernel<MB_IQ_C32>;
+    case MB_IQ_I16: return fft_tc_kernel<MB_IQ_I16>;
+    case MB_IQ_I8: return fft_tc_kernel<MB_IQ_I8>;
+    default: return fft_tc_kernel<MB_IQ_F16>;
   }
 }
 
-// raises the dynamic shared memory limit of a (type, mode) kernel once per
+// raises the dynamic shared memory limit of a sample type's kernel once per
 // device, and returns the device's SM count
-mb_status fft_tc_configure(int dt, int mode, int dev, int *sms) {
-  static std::atomic<uint64_t> configured[8] = {};
+mb_status fft_tc_configure(int dt, int dev, int *sms) {
+  static std::atomic<uint64_t> configured[4] = {};
   static std::atomic<int> sm_count[64] = {};
-  const int which = (dt == MB_IQ_C32 ? 0 : dt == MB_IQ_I16 ? 1 : dt == MB_IQ_I8 ? 2 : 3) + 4 * mode;
+  const int which = dt == MB_IQ_C32 ? 0 : dt == MB_IQ_I16 ? 1 : dt == MB_IQ_I8 ? 2 : 3;
   const uint64_t bit = 1ull << (dev & 63);
   if (!(configured[which].load() & bit)) {
-    const FtKernel k = mode == kFtPilot ? fft_tc_kernel_of<kFtPilot>(dt) : fft_tc_kernel_of<kFtUplinkLP>(dt);
-    MB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFtSmem));
+    MB_CUDA_TRY(cudaFuncSetAttribute(fft_tc_kernel_of(dt), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kFtSmem));
     int n = 0;
     MB_CUDA_TRY(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
     sm_count[dev & 63].store(n);
@@ -545,11 +553,11 @@ mb_status fft_tc_configure(int dt, int mode, int dev, int *sms) {
 }
 
 // one wave: units spread evenly over at most one CTA per SM
-mb_status fft_tc_launch(int mode, const FftTcPlan *pl, const void *iq, int iq_dtype, FtParams &p,
-                        cudaStream_t st, uint32_t upc) {
+mb_status fft_tc_launch(const FftTcPlan *pl, const void *iq, int iq_dtype, FtParams &p, cudaStream_t st,
+                        uint32_t upc) {
   int dev = 0, sms = 0;
   MB_CUDA_TRY(cudaGetDevice(&dev));
-  mb_status r = fft_tc_configure(iq_dtype, mode, dev, &sms);
+  mb_status r = fft_tc_configure(iq_dtype, dev, &sms);
   if (r != MB_OK) return r;
   const uint32_t bytes = iq_dtype == MB_IQ_C32 ? 8 : iq_dtype == MB_IQ_I8 ? 2 : 4;
   // the rows as 64-sample n1 rows of 64 * bytes bytes, read in 128-byte boxes
@@ -562,8 +570,7 @@ mb_status fft_tc_launch(int mode, const FftTcPlan *pl, const void *iq, int iq_dt
   p.units = (p.rows + 1) / 2;
   p.upc = upc ? upc : (p.units + (uint32_t)max(sms, 1) - 1) / (uint32_t)max(sms, 1);
   const uint32_t grid = (p.units + p.upc - 1) / p.upc;
-  const FtKernel k = mode == kFtPilot ? fft_tc_kernel_of<kFtPilot>(iq_dtype) : fft_tc_kernel_of<kFtUplinkLP>(iq_dtype);
-  k<<<grid, kFtThreads, kFtSmem, st>>>(map, p);
+  fft_tc_kernel_of(iq_dtype)<<<grid, kFtThreads, kFtSmem, st>>>(map, p);
   MB_LAUNCH_CHECK();
   return MB_OK;
 }
@@ -632,7 +639,8 @@ mb_status fft_tc_uplink_lp(const FftTcPlan *pl, const void *iq, int iq_dtype, ui
   p.S_pad = S_pad;
   p.out = reinterpret_cast<__nv_bfloat16 *>(y_lp);
   p.err = err;
-  return fft_tc_launch(kFtUplinkLP, pl, iq, iq_dtype, p, st, upc);
+  p.pilot_rows = 0;
+  return fft_tc_launch(pl, iq, iq_dtype, p, st, upc);
 }
 
 bool fft_tc_pilot_supported(const FftTcPlan *pl, const void *iq) {
@@ -657,7 +665,34 @@ mb_status fft_tc_pilot(const FftTcPlan *pl, const void *iq, int iq_dtype, uint32
   p.G = (S + sg - 1) / sg;
   p.sg_magic = (uint32_t)((0x100000000ull + sg - 1) / sg);
   p.err = err;
-  return fft_tc_launch(kFtPilot, pl, iq, iq_dtype, p, st, upc);
+  p.pilot_rows = p.rows;
+  return fft_tc_launch(pl, iq, iq_dtype, p, st, upc);
+}
+
+mb_status fft_tc_slot(const FftTcPlan *pl, const void *iq, int iq_dtype, uint32_t P, uint32_t U, uint32_t M,
+                      uint32_t S, uint32_t K, uint32_t sg, uint32_t tail_rem, const float2 *pilot, float2 *csi,
+                      void *y_lp, uint32_t S_pad, int *err, cudaStream_t st) {
+  if (!fft_tc_lp_supported(pl, iq, S_pad, y_lp) || S > kFtN || S > S_pad || sg == 0 || sg >= kFtN || !pilot ||
+      !csi)
+    return MB_BAD_ARG;
+  FtParams p{};
+  p.rows = (P + U) * M;
+  p.pilot_rows = P * M;
+  if (p.rows == 0) return MB_OK;
+  p.M = M;
+  p.S = S;
+  p.S_pad = S_pad;
+  p.out = reinterpret_cast<__nv_bfloat16 *>(y_lp);
+  p.csi = csi;
+  p.pilot = pilot;
+  p.K = K;
+  p.sg = sg;
+  p.ue_start = 0;
+  p.tail_rem = tail_rem;
+  p.G = (S + sg - 1) / sg;
+  p.sg_magic = (uint32_t)((0x100000000ull + sg - 1) / sg);
+  p.err = err;
+  return fft_tc_launch(pl, iq, iq_dtype, p, st, 0);
 }
 
 }  // namespace mb

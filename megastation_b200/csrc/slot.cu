@@ -232,15 +232,22 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     return mixed ? fft_uplink_lp(s->fft, src, c.iq_dtype, nb, s->y_lp, s->S_pad, fs)
                  : mb_fft_uplink(s->fft, src, c.iq_dtype, nb, reinterpret_cast<mb_c32 *>(s->y), fs);
   };
-  // fork: the first uplink FFT batch only needs the samples (serialised
-  // and timed on the slot stream when timing is on)
+  // Mixed precision at N = 4096: the pilot symbols and the first uplink
+  // batch are adjacent rows of iq and go through ONE tensor-core FFT launch
+  // on the critical stream (CSI and planar BF16 rows).  That kernel holds a
+  // whole SM per CTA, so nothing would run beside a separate pilot launch
+  // anyway, and the pilots ride in its pipeline instead of paying a
+  // latency-bound launch of their own.
   const uint32_t nb0 = std::min(c.sym_batch, c.U);
-  if (c.U && mk) {
+  const bool combined = mixed && c.U && fft_slot_tc_ok(s->fft, iq, s->S_pad, s->y_lp);
+  // otherwise fork: the first uplink FFT batch only needs the samples
+  // (serialised and timed on the slot stream when timing is on)
+  if (!combined && c.U && mk) {
     MARK(mk->fft_b[0]);
     r = fft_batch(0, nb0, st);
     if (r != MB_OK) return r;
     MARK(mk->fft_e[0]);
-  } else if (c.U) {
+  } else if (!combined && c.U) {
     MB_CUDA_TRY(cudaEventRecord(s->ev_fork, st));
     MB_CUDA_TRY(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
     r = fft_batch(0, nb0, s->side);
@@ -251,17 +258,25 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   // stream itself while timing)
   cudaStream_t cs = st;
   if (!mk) {
-    if (!c.U) MB_CUDA_TRY(cudaEventRecord(s->ev_fork, st));
+    if (!c.U || combined) MB_CUDA_TRY(cudaEventRecord(s->ev_fork, st));
     MB_CUDA_TRY(cudaStreamWaitEvent(s->crit, s->ev_fork, 0));
     cs = s->crit;
+  }
+  if (combined) {
+    MARK(mk->fft_b[0]);
+    r = fft_slot_tc(s->fft, iq, c.iq_dtype, c.P, nb0, reinterpret_cast<mb_c32 *>(s->csi), s->y_lp, s->S_pad, cs);
+    if (r != MB_OK) return r;
+    MARK(mk->fft_e[0]);
   }
   MARK(mk->pilot_b);
   // pilot FFT with the short last group's tail fill in its epilogue.  The
   // FP32 kernel's many small CTAs finish a few pilot symbols sooner than
   // the tensor-core kernel's one-CTA-per-SM pipeline (18 vs 22 us for 512
   // rows of 4096), so the pilots stay on it in both precisions.
-  r = fft_pilot_fill(s->fft, iq, c.iq_dtype, c.P, reinterpret_cast<mb_c32 *>(s->csi), cs);
-  if (r != MB_OK) return r;
+  if (!combined) {
+    r = fft_pilot_fill(s->fft, iq, c.iq_dtype, c.P, reinterpret_cast<mb_c32 *>(s->csi), cs);
+    if (r != MB_OK) return r;
+  }
   MARK(mk->pilot);
   float2 *prec = c.D ? s->precoder : nullptr;
   if (mixed) {
@@ -283,7 +298,7 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     MARK(mk->end);
     return MB_OK;
   }
-  if (!mk) MB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
+  if (!mk && !combined) MB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
   const uint64_t llr_sym = (uint64_t)c.K * c.cb_stride;
   const uint64_t hard_sym = (uint64_t)c.K * s->hrow;
   uint32_t bi = 0;
