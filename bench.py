@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed"])
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 path")
     ap.add_argument("--no-evm", action="store_true")
+    ap.add_argument("--ns-iters", type=int, default=1, help="Newton-Schulz steps of the mixed ZF")
     ap.add_argument("--sym-batch", type=int, default=12)
     ap.add_argument("--rotate", type=int, default=4, help="distinct input slots cycled (L2 flush)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -153,6 +154,16 @@ def profile_traffic(name, unit_name, units):
     with open(path) as f:
         m = re.search(r"dram bytes per " + re.escape(unit_name) + r": *([0-9.eE+]+)", f.read())
     return float(m.group(1)) * units if m else None
+
+
+def slot_launches(cfg, sym_batch, mixed, downlink=False):
+    """Kernels one uplink slot launches: the pilot FFT (inside the first
+    uplink FFT launch in the mixed path at N = 4096), the ZF, one uplink FFT
+    and one equalize per symbol batch; with a downlink also the precoder
+    scaling, the precode and the IFFT."""
+    batches = max(1, -(-cfg.U // max(sym_batch, 1)))
+    n = (0 if mixed and cfg.N == 4096 else 1) + 1 + 2 * batches
+    return n + (3 if downlink else 0)
 
 
 def roofline(cfg, args, st, n_valid, hrow):
@@ -341,9 +352,11 @@ def time_slots(slot_mod, cfg, precision, sym_batch, iq_dev, llr, hard, stream, s
     return e0.elapsed_time(e1)
 
 
-def evm_report(cfg, d, sym_batch):
+def evm_report(cfg, d, sym_batch, ns_iters=1):
     """EVM (dB) of the equalized symbols against the transmitted ones for the
-    plain FP32 path, the mixed path and an FP64-ZF variant, on one slot."""
+    plain FP32 path, the mixed path and an FP64-ZF variant, on one slot.  The
+    mixed row follows the mixed slot's arithmetic: the mixed-precision pilot
+    and uplink FFTs (tensor cores at N = 4096) and their BF16 rows."""
     import torch
     import megastation_b200 as mb
     iq = torch.from_numpy(d["iq"]).cuda()
@@ -351,10 +364,19 @@ def evm_report(cfg, d, sym_batch):
     out = {}
     for name, prec in (("fp64_zf", 2), ("plain_fp32", 0), ("mixed", 1)):
         csi = torch.zeros(cfg.G, cfg.M, cfg.K, dtype=torch.complex64, device="cuda")
-        mb.PilotFFT(cfg.start, cfg.N, cfg.S, cfg.M, cfg.K, cfg.sg)(iq[:cfg.P], csi)
-        mb.Beamform(cfg.M, cfg.K, cfg.G, precision=prec).beamform_uplink(csi, S=cfg.S, sc_group=cfg.sg)
-        y = torch.zeros(cfg.U, cfg.M, cfg.S, dtype=torch.complex64, device="cuda")
-        mb.UplinkFFT(cfg.start, cfg.N, cfg.S, cfg.M)(iq[cfg.P:], y)
+        pf = mb.PilotFFT(cfg.start, cfg.N, cfg.S, cfg.M, cfg.K, cfg.sg)
+        (pf.mixed if prec == 1 else pf)(iq[:cfg.P], csi)
+        mb.Beamform(cfg.M, cfg.K, cfg.G, precision=prec, ns_iters=ns_iters).beamform_uplink(
+            csi, S=cfg.S, sc_group=cfg.sg)
+        uf = mb.UplinkFFT(cfg.start, cfg.N, cfg.S, cfg.M)
+        if prec == 1:
+            pitch = (cfg.S + 7) // 8 * 8
+            ylp = torch.zeros(cfg.U, 2, cfg.M, pitch, dtype=torch.bfloat16, device="cuda")
+            uf.uplink_bf16(iq[cfg.P:], ylp, pitch)
+            y = torch.complex(ylp[:, 0, :, :cfg.S].float(), ylp[:, 1, :, :cfg.S].float()).contiguous()
+        else:
+            y = torch.zeros(cfg.U, cfg.M, cfg.S, dtype=torch.complex64, device="cuda")
+            uf(iq[cfg.P:], y)
         llr = torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda")
         x = torch.zeros(cfg.U, cfg.K, cfg.S, dtype=torch.complex64, device="cuda")
         eq = mb.Equalize.equalize_tc if prec == 1 else mb.Equalize.equalize
@@ -372,7 +394,7 @@ def workload_config(cfg, args):
     return {"workload": "uplink slot 256x32, N=4096, S=3276, 2 pilot + 12 data symbols, 64-QAM, "
                         "8-tap exp-PDP rho=0.5, 25 dB, c64 samples",
             "M": cfg.M, "K": cfg.K, "N": cfg.N, "S": cfg.S, "sg": cfg.sg, "Qm": cfg.Qm, "P": cfg.P,
-            "U": cfg.U, "precision": args.precision, "sym_batch": args.sym_batch,
+            "U": cfg.U, "precision": args.precision, "sym_batch": args.sym_batch, "ns_iters": args.ns_iters,
             "l2": f"inputs {cfg.symbols * cfg.M * cfg.N * 8 / 1e6:.0f} MB per slot, {args.rotate} "
                   "slots rotated (larger than the 126 MB L2)",
             "seed": cfg.seed}
@@ -458,7 +480,7 @@ def run_full(args):
             "latency_us": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max()), "mean": float(lat.mean())},
             "uplink_evm_db": evm, "clocks": clk,
-            "gpu_launches": n * (2 + (1 if cfg.S % cfg.sg else 0) + 1 + 2 + 2),
+            "gpu_launches": n * slot_launches(cfg, cfg.U, args.precision == "mixed", downlink=True),
             "note": "learned initialiser not applied: the per-subcarrier path supports K <= 32"}
     print(json.dumps(line), flush=True)
 
@@ -636,7 +658,7 @@ def run_cells(args):
     f1.record(stream)
     f1.synchronize()
     ms_seq = f0.elapsed_time(f1)
-    launches = sum(2 + (1 if c.S % c.sg else 0) + 2 for c in cfgs)
+    launches = sum(slot_launches(c, max(c.U, 1), args.precision == "mixed") for c in cfgs)
     line = {"metric": "batched slots/s (32 uneven cells)", "value": args.steps / (ms / 1e3),
             "unit": "slots/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -687,7 +709,8 @@ def main():
     iq_host = torch.from_numpy(d["iq"]).pin_memory()
     iq_dev = [iq_host.cuda() for _ in range(R)]
     stream = torch.cuda.Stream()
-    run = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=True)
+    run = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=True,
+                          ns_iters=args.ns_iters)
     llr = [torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda") for _ in range(2)]
     hard = [torch.zeros(cfg.U, cfg.K, hrow, dtype=torch.uint8, device="cuda") for _ in range(2)]
 
@@ -729,8 +752,8 @@ def main():
         pv = job_value(world, args.steps, pms)
         plain = {"value": pv, "unit": UNIT, "us_per_slot": 1e3 * pms / args.steps,
                  "speedup_mixed_over_plain": value / pv}
-    evm = None if args.no_evm or rank != 0 else evm_report(cfg, d, args.sym_batch)
-    launches_per_slot = 2 + (1 if cfg.S % cfg.sg else 0) + 2 * ((cfg.U + args.sym_batch - 1) // args.sym_batch)
+    evm = None if args.no_evm or rank != 0 else evm_report(cfg, d, args.sym_batch, args.ns_iters)
+    launches_per_slot = slot_launches(cfg, args.sym_batch, args.precision == "mixed")
 
     # ---- roofline pass: the same slots with every kernel alone on the slot
     # stream (timing mode serialises the side-stream FFT) and CUDA events at
