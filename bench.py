@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed"])
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 path")
     ap.add_argument("--no-evm", action="store_true")
-    ap.add_argument("--ns-iters", type=int, default=1, help="Newton-Schulz steps of the mixed ZF")
+    ap.add_argument("--ns-iters", type=int, default=2, help="Newton-Schulz steps of the mixed ZF (config 2 names 2)")
     ap.add_argument("--sym-batch", type=int, default=12)
     ap.add_argument("--rotate", type=int, default=4, help="distinct input slots cycled (L2 flush)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -352,7 +352,7 @@ def time_slots(slot_mod, cfg, precision, sym_batch, iq_dev, llr, hard, stream, s
     return e0.elapsed_time(e1)
 
 
-def evm_report(cfg, d, sym_batch, ns_iters=1):
+def evm_report(cfg, d, sym_batch, ns_iters=2):
     """EVM (dB) of the equalized symbols against the transmitted ones for the
     plain FP32 path, the mixed path and an FP64-ZF variant, on one slot.  The
     mixed row follows the mixed slot's arithmetic: the mixed-precision pilot

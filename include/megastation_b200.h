@@ -165,7 +165,7 @@ typedef enum {
 
 typedef struct {
   uint32_t precision;     /* mb_zf_precision */
-  uint32_t ns_iters;      /* Newton-Schulz refinements (MIXED), e.g. 1 */
+  uint32_t ns_iters;      /* Newton-Schulz refinements (MIXED), e.g. 2 */
   float cond_threshold;   /* FP64 fallback above this estimate, e.g. 1e4 */
   uint32_t reserved;
 } mb_zf_opts;

@@ -21,7 +21,7 @@ def _ptrs(tensors):
 class Cells:
     """cfgs: datagen.CellConfig per cell (shapes may all differ)."""
 
-    def __init__(self, cfgs, precision="mixed", ns_iters=1, cond_threshold=1e4):
+    def __init__(self, cfgs, precision="mixed", ns_iters=2, cond_threshold=1e4):
         self.cfgs = list(cfgs)
         descs = (_lib.MbCellDesc * len(self.cfgs))()
         self.llr, self.hard, self.status = [], [], []

@@ -142,7 +142,7 @@ class DownlinkIFFT(_FFTBase):
 class Beamform:
     """beamform/beamform.h:27-84: zero-forcing detector and precoder."""
 
-    def __init__(self, num_bs, num_ue, batch_count, precision=_lib.MB_ZF_FP32, ns_iters=1,
+    def __init__(self, num_bs, num_ue, batch_count, precision=_lib.MB_ZF_FP32, ns_iters=2,
                  cond_threshold=1e4):
         h = ctypes.c_void_p()
         check(LIB.mb_zf_create(num_bs, num_ue, batch_count, ctypes.byref(h)), "Beamform")

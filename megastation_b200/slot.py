@@ -19,7 +19,7 @@ class UplinkSlot:
     with the same fields)."""
 
     def __init__(self, cfg, precision="fp32", sym_batch=4, use_graph=False, D=0, out_dtype="f16",
-                 ns_iters=1, cond_threshold=1e4):
+                 ns_iters=2, cond_threshold=1e4):
         cb, zeros, stride = cfg.ldpc()
         self.cfg = cfg
         self.cb_size, self.zeros, self.cb_stride = cb, zeros, stride
