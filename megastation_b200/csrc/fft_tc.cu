@@ -198,7 +198,12 @@ __global__ void __launch_bounds__(kFtThreads, 1)
   // need them); the staging rows follow
   uint8_t *sF = ft_smem, *sAZ = ft_smem + kMat, *sRing = ft_smem + 2 * kMat;
   uint8_t *sStg = sRing + 2 * kStage;
-  __shared__ uint64_t bar_mats, full[2], a_ready, z_ready, st_ready, d1_full, d2_full, st_done;
+  // Each barrier completes once per unit.  a_ready comes as a pair per ring
+  // slot, waited with parity (i >> 1) & 1: the copy warp may trail the
+  // compute warps by two units (while it drains a bulk store), and a plain
+  // parity wait would then alias a later phase.  full is per slot anyway;
+  // every other barrier's waiters are at most one phase behind.
+  __shared__ uint64_t bar_mats, full[2], a_ready[2], z_ready, st_ready, d1_full, d2_full, st_done;
   __shared__ uint32_t tmem_slot;
   __shared__ __align__(16) uint32_t s_rmax[16];
   __shared__ volatile int s_fail;
@@ -215,7 +220,8 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     tc::mbar_init(&bar_mats, 1);
     tc::mbar_init(&full[0], 1);
     tc::mbar_init(&full[1], 1);
-    tc::mbar_init(&a_ready, kFtCompute / 32);
+    tc::mbar_init(&a_ready[0], kFtCompute / 32);
+    tc::mbar_init(&a_ready[1], kFtCompute / 32);
     tc::mbar_init(&z_ready, kFtCompute / 32);
     tc::mbar_init(&st_ready, kFtCompute / 32);
     tc::mbar_init(&d1_full, 1);
@@ -255,7 +261,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       bool ok = ft_wait(&bar_mats, 0, &s_fail);
       for (uint32_t i = 0; i < n_units && ok; i++) {
         // GEMM 1: D1 (128 (r, n2) x 128 (p', k1)) = A (samples) x F
-        if (!ft_wait(&a_ready, i & 1, &s_fail)) break;
+        if (!ft_wait(&a_ready[i & 1], (i >> 1) & 1, &s_fail)) break;
         tc::fence_after_sync();
 #pragma unroll
         for (int ks = 0; ks < 8; ks++) tc::mma_f16(tmem, da[ks], db[ks], idesc, ks > 0);
@@ -311,7 +317,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       issue_load(1);
       for (uint32_t i = 0; i < n_units; i++) {
         // the ring slot of unit i takes unit i + 2 once unit i is converted
-        if (!ft_wait(&a_ready, i & 1, &s_fail)) break;
+        if (!ft_wait(&a_ready[i & 1], (i >> 1) & 1, &s_fail)) break;
         issue_load(i + 2);
         if (i > 0) {
           if (!ft_wait(&st_ready, (i - 1) & 1, &s_fail)) break;
@@ -478,7 +484,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
           *reinterpret_cast<uint4 *>(sAZ + a_off[c2] + 16384) = im[c2];
         }
       }
-      arrive(&a_ready);
+      arrive(&a_ready[i & 1]);
       // (b) GEMM-2 epilogue of the previous unit into the staging rows,
       // once the bulk copies of the unit before it have read them
       if (i > 0) {

@@ -122,3 +122,41 @@ def test_pilot_fft_mixed_vs_oracle(mb, dtype, M, K, sg):
     got = csi.cpu().numpy()
     scale = np.sqrt(np.mean(np.abs(ref) ** 2))
     assert np.abs(got - ref).max() <= 2e-3 * scale
+
+
+def test_fft_tc_many_units_per_cta(mb):
+    # the bench's launch size: 12 symbols x 256 antennas = 1536 two-row units,
+    # about 11 per CTA, so every ring slot and barrier of the pipeline turns
+    # over many times (a barrier phase mix-up shows as a device error)
+    N, S, M, n_sym = 4096, 3276, 256, 12
+    rng = np.random.default_rng(99)
+    # rows 2^-8 .. 2^8 apart, so a row scaled with another row's factor shows
+    row_gain = 2.0 ** rng.integers(-8, 9, size=(n_sym, M, 1))
+    x = ((rng.standard_normal((n_sym, M, N)) + 1j * rng.standard_normal((n_sym, M, N))) * row_gain).astype(np.complex64)
+    got, _, start = run_bf16(mb, x, N, S, M, n_sym, (S + 7) // 8 * 8)
+    check_rows(got[::5], x[::5], N, S, start)
+
+
+def test_pilot_fft_mixed_many_units(mb):
+    N, S, M, K, sg = 4096, 3276, 256, 64, 16
+    P = K // sg
+    rng = np.random.default_rng(7)
+    row_gain = 2.0 ** rng.integers(-4, 5, size=(P, M, 1))
+    x = ((rng.standard_normal((P, M, N)) + 1j * rng.standard_normal((P, M, N))) * row_gain).astype(np.complex64)
+    start = (N - S) // 2
+    G = (S + sg - 1) // sg
+    csi = torch.zeros(G, M, K, dtype=torch.complex64, device="cuda")
+    mb.PilotFFT(start, N, S, M, K, sg).mixed(torch.from_numpy(x).cuda(), csi)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    ref = np.zeros((G, M, K), np.complex64)
+    ps = orc.pilot_sign(S)
+    for p in range(P):
+        orc.pilot_fft(x[p], N, S, start, K, sg, p * sg, ps, ref)
+    # per (antenna, pilot symbol): each row has its own gain; user u's
+    # estimate comes from pilot symbol u // sg
+    got = csi.cpu().numpy().reshape(G, M, P, sg)
+    r = ref.reshape(G, M, P, sg)
+    scale = np.sqrt(np.mean(np.abs(r) ** 2, axis=(0, 3), keepdims=True))
+    ratio = np.abs(got - r) / (2e-3 * scale)
+    assert ratio.max() <= 1.0, (ratio.max(), np.unravel_index(ratio.argmax(), ratio.shape))

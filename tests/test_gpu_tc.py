@@ -112,6 +112,10 @@ CASES = [
     # N = 4096: the uplink FFT on the tensor cores
     dict(M=64, K=16, N=4096, S=3276, sg=16, Qm=6, U=3, snr_db=25.0, seed=17, iq_dtype="int16"),
     dict(M=32, K=8, N=4096, S=3276, sg=16, Qm=8, U=2, snr_db=32.0, seed=18),
+    # the bench's slot shape: the combined pilot + uplink FFT launch with
+    # about 13 units per CTA
+    dict(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=12, snr_db=25.0, seed=19, channel="tdl", rho=0.5,
+         n_taps=8, tap_decay=2.0),
 ]
 
 
@@ -120,7 +124,7 @@ def test_slot_uplink_mixed_vs_oracle(mb, case):
     from megastation_b200 import datagen, slot
     cfg = datagen.CellConfig(**case)
     d = datagen.make_slot(cfg)
-    run = slot.UplinkSlot(cfg, precision="mixed", sym_batch=4, use_graph=True)
+    run = slot.UplinkSlot(cfg, precision="mixed", sym_batch=12 if cfg.U == 12 else 4, use_graph=True)
     iq = torch.from_numpy(d["iq"]).cuda()
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
