@@ -26,7 +26,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=12, snr_db=25.0, channel="tdl",
-                n_taps=8, tap_decay=2.0, rho=0.5, iq_dtype="c64", seed=2024)
+                n_taps=8, tap_decay=2.0, rho=0.5, iq_dtype="int16", seed=2024)
+# bytes per IQ sample of each input format
+IQ_BYTES = {"c64": 8, "int16": 4, "int8": 2, "f16": 4}
 METRIC = "slots/s"
 UNIT = "slots/s"
 
@@ -177,6 +179,7 @@ def roofline(cfg, args, st, n_valid, hrow):
     rows = cfg.U * cfg.M * calls / n_fft               # antenna rows per uplink FFT launch
     syms = cfg.U * calls / n_eq                        # symbols per equalize launch
     out_b = 4 if mixed else 8                          # BF16 planar or c32 per subcarrier
+    bps = IQ_BYTES[cfg.iq_dtype]                       # bytes per input sample
     tc = {"MM": 64 if 2 * cfg.K <= 64 else 128, "Mp": (cfg.M + 63) // 64 * 64}
     img_group = 2 * tc["Mp"] * tc["MM"] * 2
     tc_fft = mixed and cfg.N == 4096  # the tensor-core FFT takes the mixed uplink at N = 4096 ...
@@ -185,11 +188,11 @@ def roofline(cfg, args, st, n_valid, hrow):
     k = {
         "fft_uplink": {"ms": st["uplink_fft"] / n_fft, "per_slot_ms": st["uplink_fft"] / calls,
                        "bound": "hbm", "units": rows + pilot_rows, "unit_name": "antenna row",
-                       "bytes": rows * (cfg.N * 8 + cfg.S * out_b)
-                       + pilot_rows * cfg.N * 8 + (cfg.G * cfg.M * cfg.K * 8 * calls / n_fft if tc_fft else 0)},
+                       "bytes": rows * (cfg.N * bps + cfg.S * out_b)
+                       + pilot_rows * cfg.N * bps + (cfg.G * cfg.M * cfg.K * 8 * calls / n_fft if tc_fft else 0)},
         "fft_pilot": {"ms": st["pilot_fft"] / calls, "per_slot_ms": st["pilot_fft"] / calls,
                       "bound": "hbm", "units": cfg.P * cfg.M, "unit_name": "pilot row",
-                      "bytes": cfg.P * cfg.M * (cfg.N * 8) + cfg.G * cfg.M * cfg.K * 8},
+                      "bytes": cfg.P * cfg.M * (cfg.N * bps) + cfg.G * cfg.M * cfg.K * 8},
         "zf": {"ms": st["zf"] / calls, "per_slot_ms": st["zf"] / calls, "bound": "tensor",
                "units": cfg.G, "unit_name": "subcarrier group",
                "flops": cfg.G * (16.0 * cfg.K ** 2 * cfg.M + 40.0 * cfg.K ** 3)},
@@ -392,10 +395,10 @@ def evm_report(cfg, d, sym_batch, ns_iters=2):
 
 def workload_config(cfg, args):
     return {"workload": "uplink slot 256x32, N=4096, S=3276, 2 pilot + 12 data symbols, 64-QAM, "
-                        "8-tap exp-PDP rho=0.5, 25 dB, c64 samples",
+                        f"8-tap exp-PDP rho=0.5, 25 dB, {cfg.iq_dtype} samples",
             "M": cfg.M, "K": cfg.K, "N": cfg.N, "S": cfg.S, "sg": cfg.sg, "Qm": cfg.Qm, "P": cfg.P,
             "U": cfg.U, "precision": args.precision, "sym_batch": args.sym_batch, "ns_iters": args.ns_iters,
-            "l2": f"inputs {cfg.symbols * cfg.M * cfg.N * 8 / 1e6:.0f} MB per slot, {args.rotate} "
+            "l2": f"inputs {cfg.symbols * cfg.M * cfg.N * IQ_BYTES[cfg.iq_dtype] / 1e6:.0f} MB per slot, {args.rotate} "
                   "slots rotated (larger than the 126 MB L2)",
             "seed": cfg.seed}
 

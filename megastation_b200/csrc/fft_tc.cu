@@ -99,6 +99,10 @@ struct Fmt {
   static constexpr uint32_t kUnitBytes = 2 * kFtN * kBytes;
 };
 
+// integer samples have a known range: a fixed scale instead of the row maximum
+template <int DT>
+constexpr bool kFixedScale = DT == MB_IQ_I16 || DT == MB_IQ_I8;
+
 // ring offset of the 16-byte piece holding sample n2 (first of its piece)
 // of n1 row n1 of unit row r: box (r, n2 / (128 / bytes)) of 64 n1 rows x
 // 128 B, swizzled by the TMA
@@ -386,7 +390,9 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     __shared__ float s_inv[2][2];  // [unit parity][row] inverse row scales
 
     auto store_unit = [&](uint32_t i) {
-      const float inv = s_inv[i & 1][s_r];
+      // integer samples: the FFT of q * 2^-8 (int16) or of q (int8) is the
+      // FFT of the normalised samples q / 2^15 or q / 2^7 times 2^7
+      const float inv = kFixedScale<DT> ? 1.0f / 128.0f : s_inv[i & 1][s_r];
       float vr[16], vi[16];
       tc::tmem_ld16(tl + 128 + 16 * part, vr);
       tc::tmem_ld16(tl + 192 + 16 * part, vi);
@@ -446,32 +452,66 @@ __global__ void __launch_bounds__(kFtThreads, 1)
         for (int c2 = 0; c2 < 2; c2++)
 #pragma unroll
           for (int w = 0; w < (int)F::kPPC; w++) raw[c2][w] = *reinterpret_cast<const uint4 *>(slot + r_off[c2][w]);
-        float m = 0.f;
+        if constexpr (kFixedScale<DT>) {
+          // integer samples: |q| <= 2^15 (int16) or 2^7 (int8) converts to
+          // FP16 and a fixed power of two takes it below 2^7 (exact), so no
+          // row maximum is needed
+          const __half2 sc2 = __float2half2_rn(DT == MB_IQ_I16 ? 1.0f / 256.0f : 1.0f);
 #pragma unroll
-        for (int c2 = 0; c2 < 2; c2++)
+          for (int c2 = 0; c2 < 2; c2++) {
+            uint32_t rw[4], iw[4];
 #pragma unroll
-          for (int j = 0; j < 8; j++) {
-            const float2 v = chunk_sample<DT>(raw[c2], j);
-            m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+            for (int t = 0; t < 4; t++) {
+              __half2 hr, hi;
+              if constexpr (DT == MB_IQ_I16) {
+                const uint4 w = raw[c2][t / 2];
+                const uint32_t a = (t & 1) ? w.z : w.x, b = (t & 1) ? w.w : w.y;  // samples 2t, 2t+1
+                hr = __halves2half2(__short2half_rn((short)(a & 0xFFFFu)), __short2half_rn((short)(b & 0xFFFFu)));
+                hi = __halves2half2(__short2half_rn((short)(a >> 16)), __short2half_rn((short)(b >> 16)));
+              } else {
+                const uint4 w = raw[c2][0];
+                const uint32_t v = t == 0 ? w.x : t == 1 ? w.y : t == 2 ? w.z : w.w;  // samples 2t, 2t+1
+                hr = __halves2half2(__short2half_rn((short)(int8_t)(v & 0xFFu)),
+                                    __short2half_rn((short)(int8_t)((v >> 16) & 0xFFu)));
+                hi = __halves2half2(__short2half_rn((short)(int8_t)((v >> 8) & 0xFFu)),
+                                    __short2half_rn((short)(int8_t)(v >> 24)));
+              }
+              hr = __hmul2(hr, sc2);
+              hi = __hmul2(hi, sc2);
+              memcpy(&rw[t], &hr, 4);
+              memcpy(&iw[t], &hi, 4);
+            }
+            re[c2] = make_uint4(rw[0], rw[1], rw[2], rw[3]);
+            im[c2] = make_uint4(iw[0], iw[1], iw[2], iw[3]);
           }
-        const uint32_t mb = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
-        if (lane == 0) s_rmax[warp] = mb;
-        compute_sync();
-        const uint4 m0 = *reinterpret_cast<const uint4 *>(&s_rmax[rh * 8]);
-        const uint4 m1 = *reinterpret_cast<const uint4 *>(&s_rmax[rh * 8 + 4]);
-        const uint32_t rmax = max(max(max(m0.x, m0.y), max(m0.z, m0.w)), max(max(m1.x, m1.y), max(m1.z, m1.w)));
-        float scale, inv;
-        row_scale(rmax, scale, inv);
-        if ((tid & 255) == 0) s_inv[i & 1][rh] = inv;
+        } else {
+          float m = 0.f;
 #pragma unroll
-        for (int c2 = 0; c2 < 2; c2++) {
-          float2 v[8];
+          for (int c2 = 0; c2 < 2; c2++)
 #pragma unroll
-          for (int j = 0; j < 8; j++) v[j] = chunk_sample<DT>(raw[c2], j);
-          re[c2] = make_uint4(h2_bits(v[0].x * scale, v[1].x * scale), h2_bits(v[2].x * scale, v[3].x * scale),
-                              h2_bits(v[4].x * scale, v[5].x * scale), h2_bits(v[6].x * scale, v[7].x * scale));
-          im[c2] = make_uint4(h2_bits(v[0].y * scale, v[1].y * scale), h2_bits(v[2].y * scale, v[3].y * scale),
-                              h2_bits(v[4].y * scale, v[5].y * scale), h2_bits(v[6].y * scale, v[7].y * scale));
+            for (int j = 0; j < 8; j++) {
+              const float2 v = chunk_sample<DT>(raw[c2], j);
+              m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+            }
+          const uint32_t mb = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+          if (lane == 0) s_rmax[warp] = mb;
+          compute_sync();
+          const uint4 m0 = *reinterpret_cast<const uint4 *>(&s_rmax[rh * 8]);
+          const uint4 m1 = *reinterpret_cast<const uint4 *>(&s_rmax[rh * 8 + 4]);
+          const uint32_t rmax = max(max(max(m0.x, m0.y), max(m0.z, m0.w)), max(max(m1.x, m1.y), max(m1.z, m1.w)));
+          float scale, inv;
+          row_scale(rmax, scale, inv);
+          if ((tid & 255) == 0) s_inv[i & 1][rh] = inv;
+#pragma unroll
+          for (int c2 = 0; c2 < 2; c2++) {
+            float2 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) v[j] = chunk_sample<DT>(raw[c2], j);
+            re[c2] = make_uint4(h2_bits(v[0].x * scale, v[1].x * scale), h2_bits(v[2].x * scale, v[3].x * scale),
+                                h2_bits(v[4].x * scale, v[5].x * scale), h2_bits(v[6].x * scale, v[7].x * scale));
+            im[c2] = make_uint4(h2_bits(v[0].y * scale, v[1].y * scale), h2_bits(v[2].y * scale, v[3].y * scale),
+                                h2_bits(v[4].y * scale, v[5].y * scale), h2_bits(v[6].y * scale, v[7].y * scale));
+          }
         }
       }
       // the operand buffer holds Z of the previous unit until GEMM 2 has read it
@@ -518,7 +558,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       arrive(&z_ready);
     }
     // the last unit's inverse scales were written after the last barrier
-    compute_sync();
+    if constexpr (!kFixedScale<DT>) compute_sync();
     wait_ok(&d2_full, (n_units - 1) & 1);
     tc::fence_after_sync();
     if (n_units > 1) wait_ok(&st_done, (n_units - 2) & 1);
