@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-inflight", action="store_true", help="skip timing two slots in flight")
     return ap.parse_args()
 
 
@@ -203,7 +204,7 @@ def roofline(cfg, args, st, n_valid, hrow):
     }
     if tc_fft:
         del k["fft_pilot"]  # the pilot rows go through the uplink FFT launch
-    names = {"fft_uplink": ("fft_tc_kernel<uplink LP>" if tc_fft else "fft_kernel<12, uplink LP>") if mixed
+    names = {"fft_uplink": ("fft_tc_kernel<pilot + uplink rows>" if tc_fft else "fft_kernel<12, uplink LP>") if mixed
              else "fft_kernel<12, uplink>",
              "fft_pilot": "fft_kernel<12, pilot>",
              "zf": "zf_mixed_kernel<64>" if mixed else "zf_chol_kernel<float>",
@@ -353,6 +354,44 @@ def time_slots(slot_mod, cfg, precision, sym_batch, iq_dev, llr, hard, stream, s
     e1.record(stream)
     e1.synchronize()
     return e0.elapsed_time(e1)
+
+
+def time_in_flight(slot_mod, cfg, args, iq_dev, stride, hrow, dist, D=2):
+    """The same slots with D of them in flight: D slot runners, each a
+    captured graph on its own stream, taking every D-th slot; reported beside
+    the headline (one slot at a time), not instead of it."""
+    import torch
+    R = len(iq_dev)
+    streams = [torch.cuda.Stream() for _ in range(D)]
+    runs = [slot_mod.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=True,
+                                ns_iters=args.ns_iters) for _ in range(D)]
+    llr = [torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda") for _ in range(2 * D)]
+    hard = [torch.zeros(cfg.U, cfg.K, hrow, dtype=torch.uint8, device="cuda") for _ in range(2 * D)]
+
+    def step(k):
+        i = k % D
+        o = (k // D) % 2 * D + i
+        runs[i](iq_dev[k % R], llr[o], hard[o], stream=streams[i])
+
+    for k in range(max(args.warmup, 2 * R * D)):
+        step(k)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    master = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(master)
+    for s in streams:
+        s.wait_stream(master)
+    for k in range(args.steps):
+        step(k)
+    for s in streams:
+        master.wait_stream(s)
+    e1.record(master)
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    return {"slots_in_flight": D, "value": job_value(1 if not dist else dist.get_world_size(), args.steps, ms),
+            "unit": UNIT, "us_per_slot": 1e3 * ms / args.steps}
 
 
 def evm_report(cfg, d, sym_batch, ns_iters=2):
@@ -756,6 +795,7 @@ def main():
         plain = {"value": pv, "unit": UNIT, "us_per_slot": 1e3 * pms / args.steps,
                  "speedup_mixed_over_plain": value / pv}
     evm = None if args.no_evm or rank != 0 else evm_report(cfg, d, args.sym_batch, args.ns_iters)
+    inflight = None if args.no_inflight else time_in_flight(slot, cfg, args, iq_dev, stride, hrow, dist)
     launches_per_slot = slot_launches(cfg, args.sym_batch, args.precision == "mixed")
 
     # ---- roofline pass: the same slots with every kernel alone on the slot
@@ -844,7 +884,7 @@ def main():
             "data": "synthetic (seeded generator, megastation_b200.datagen)",
             "config": workload_config(cfg, args), "clocks": clk, "e2e": e2e,
             "gpu_launches": launches_per_slot * args.steps, "roofline": roof, "cpu_baseline": cpu,
-            "plain_fp32": plain, "evm_db": evm,
+            "plain_fp32": plain, "evm_db": evm, "in_flight": inflight,
             "parallelism": f"replicas x{world}"}
     print(json.dumps(line), flush=True)
 
