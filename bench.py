@@ -816,57 +816,28 @@ def main():
     roof["slot"] = {"bytes": slot_bytes, "GB_s": slot_bytes * value / world / 1e9,
                     "frac_of_hbm": slot_bytes * value / world / 1e9 / hbm_peak}
 
-    # ---- e2e: public API with host buffers, H2D of each slot and D2H of LLRs+bits
+    # ---- e2e: the public slot pipeline (mb_pipe_*) from host buffers: H2D of
+    # each slot's samples, the slot, D2H of its LLRs and hard bits, timed on
+    # the device by the pipeline's own events
     e2e = None
     if not args.no_e2e:
-        cp_s, d2h_s = torch.cuda.Stream(), torch.cuda.Stream()
-        dev_in = [torch.empty_like(iq_dev[0]) for _ in range(2)]
-        host_llr = [torch.empty(llr[0].shape, dtype=llr[0].dtype).pin_memory() for _ in range(2)]
-        host_hard = [torch.empty(hard[0].shape, dtype=hard[0].dtype).pin_memory() for _ in range(2)]
-        ev_in = [torch.cuda.Event() for _ in range(2)]
-        ev_done = [torch.cuda.Event() for _ in range(2)]
-        ev_free = [torch.cuda.Event() for _ in range(2)]
-        ev_out = [torch.cuda.Event() for _ in range(2)]
-        run_e = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=True)
-
-        def e2e_steps(n, t_start=None, t_end=None):
-            for k in range(n):
-                b = k % 2
-                with torch.cuda.stream(cp_s):
-                    if k >= 2:
-                        cp_s.wait_event(ev_free[b])
-                    if k == 0 and t_start is not None:
-                        t_start.record(cp_s)
-                    dev_in[b].copy_(iq_host, non_blocking=True)
-                    ev_in[b].record(cp_s)
-                stream.wait_event(ev_in[b])
-                if k >= 2:
-                    stream.wait_event(ev_out[b])
-                run_e(dev_in[b], llr[b], hard[b], stream=stream)
-                ev_done[b].record(stream)
-                ev_free[b].record(stream)
-                with torch.cuda.stream(d2h_s):
-                    d2h_s.wait_event(ev_done[b])
-                    host_llr[b].copy_(llr[b], non_blocking=True)
-                    host_hard[b].copy_(hard[b], non_blocking=True)
-                    ev_out[b].record(d2h_s)
-            if t_end is not None:
-                for b in range(2):
-                    stream.wait_event(ev_out[b])
-                t_end.record(stream)
-
-        e2e_steps(4)
-        torch.cuda.synchronize()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        pipe = slot.SlotPipeline(cfg, precision=args.precision, sym_batch=args.sym_batch, depth=2,
+                                 ns_iters=args.ns_iters)
+        outs = [pipe.host_outputs() for _ in range(2)]
+        for k in range(4):
+            t = pipe.submit(iq_host, *outs[k % 2])
+        pipe.wait(t)
         if dist:
             dist.barrier()
-        e2e_steps(args.steps, a0, a1)
-        torch.cuda.synchronize()
-        ems = max_over_ranks(a0.elapsed_time(a1), dist)
+        pipe.timer_start()
+        for k in range(args.steps):
+            t = pipe.submit(iq_host, *outs[k % 2])
+        pipe.wait(t)
+        ems = max_over_ranks(pipe.timer_ms(), dist)
         e2e = {"value": job_value(world, args.steps, ems), "unit": UNIT,
-               "h2d_bytes_per_step": iq_host.numel() * iq_host.element_size(),
-               "d2h_bytes_per_step": llr[0].numel() * 2 + hard[0].numel(),
-               "pipeline": "double-buffered: H2D of slot k+1 and D2H of slot k-1 overlap slot k"}
+               "h2d_bytes_per_step": pipe.iq_bytes, "d2h_bytes_per_step": pipe.llr_bytes + pipe.hard_bytes,
+               "pipeline": "mb_pipe (depth 2): H2D of slot k+1 and D2H of slot k-1 overlap slot k"}
+        del pipe
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -333,6 +333,33 @@ mb_status mb_slot_uplink(mb_slot *slot, const void *iq, uint16_t *llr,
 mb_status mb_slot_downlink(mb_slot *slot, const mb_c32 *symbols, void *out,
                            void *stream);
 
+/* Single-GPU slot pipeline over host buffers (scheduler/gpu_engine.cc:77-437
+ * and cpu_buffer.cc:5-49 for one GPU): each submitted slot's samples are
+ * copied to a ring of `depth` device buffers, the slot runs (an mb_slot
+ * with this cell description), and its FP16 LLRs and hard bits are copied
+ * back, on three streams ordered by events, so the samples of slot k+1
+ * cross PCIe while slot k computes and slot k-1's results come back.
+ * mb_pipe_submit does not block; the host buffers of a slot must stay valid
+ * (and unmodified, for the samples) until mb_pipe_wait(ticket) returns MB_OK.
+ * Pinned host memory (cudaHostAlloc) lets the copies overlap; pageable
+ * memory works but copies synchronously.  Sizes: mb_pipe_io_bytes.
+ * mb_pipe_wait gives up after timeout_ms (UINT32_MAX: no limit) with
+ * MB_TIMEOUT; the slot's work stays queued. */
+typedef struct mb_pipe mb_pipe;
+mb_status mb_pipe_create(const mb_cell_desc *cell, uint32_t depth, mb_pipe **out);
+mb_status mb_pipe_destroy(mb_pipe *pipe);
+mb_status mb_pipe_io_bytes(const mb_pipe *pipe, uint64_t *iq_bytes,
+                           uint64_t *llr_bytes, uint64_t *hard_bytes);
+mb_status mb_pipe_submit(mb_pipe *pipe, const void *iq_host, uint16_t *llr_host,
+                         uint8_t *hard_host, uint64_t *ticket);
+mb_status mb_pipe_wait(mb_pipe *pipe, uint64_t ticket, uint32_t timeout_ms);
+/* Device timer: after mb_pipe_timer_start, the next submitted slot records
+ * a start event before its sample copy and every slot after it an end
+ * event after its result copies; mb_pipe_timer_ms waits for the last end
+ * event and returns the device time between the two (CUDA events). */
+mb_status mb_pipe_timer_start(mb_pipe *pipe);
+mb_status mb_pipe_timer_ms(mb_pipe *pipe, double *ms);
+
 /* Stage timing.  mb_slot_timing(slot, n) makes the next n slot calls record
  * CUDA events around each stage on the launching stream (0 disables);
  * mb_slot_stage_ms waits for those events and returns, summed over the

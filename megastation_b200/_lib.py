@@ -85,6 +85,13 @@ def _load():
         "mb_dmrs_table": (ST, [U64, U64, VP]),
         "mb_ldpc_sizes": (ST, [U64, U32, ctypes.c_double, U32, U64, I32,
                                ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64)]),
+        "mb_pipe_create": (ST, [ctypes.POINTER(MbCellDesc), U32, ctypes.POINTER(VP)]),
+        "mb_pipe_destroy": (ST, [VP]),
+        "mb_pipe_io_bytes": (ST, [VP, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64)]),
+        "mb_pipe_submit": (ST, [VP, VP, VP, VP, ctypes.POINTER(U64)]),
+        "mb_pipe_wait": (ST, [VP, U64, U32]),
+        "mb_pipe_timer_start": (ST, [VP]),
+        "mb_pipe_timer_ms": (ST, [VP, ctypes.POINTER(ctypes.c_double)]),
         "mb_fft_create": (ST, [ctypes.POINTER(MbFftDesc), ctypes.POINTER(VP)]),
         "mb_fft_destroy": (ST, [VP]),
         "mb_fft_uplink": (ST, [VP, VP, I32, U32, VP, VP]),

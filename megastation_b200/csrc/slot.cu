@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "slot.cuh"
 #include "sgemv.cuh"
 #include "eq_tc.cuh"
 #include "fft.cuh"
@@ -208,6 +209,15 @@ static mb_status slot_create(const mb_cell_desc *cell, bool sb_cap_all, mb_slot 
   }
   *out = s;
   return MB_OK;
+}
+
+// bytes of one slot's samples, LLRs and hard bits (the pipeline sizes its
+// device rings with them)
+void mb::slot_io_bytes(const mb_slot *s, uint64_t *iq, uint64_t *llr, uint64_t *hard) {
+  const mb_cell_desc &c = s->c;
+  *iq = (uint64_t)(c.P + c.U) * iq_elem_bytes(c.iq_dtype) * c.M * c.N;
+  *llr = (uint64_t)c.U * c.K * c.cb_stride * 2;
+  *hard = (uint64_t)c.U * c.K * s->hrow;
 }
 
 extern "C" mb_status mb_slot_create(const mb_cell_desc *cell, mb_slot **out) {

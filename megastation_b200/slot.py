@@ -84,3 +84,72 @@ def _wrap(ptr, n):
     h = _Holder()
     h.__cuda_array_interface__ = {"shape": (n,), "typestr": "<c8", "data": (ptr, False), "version": 3}
     return torch.as_tensor(h, device="cuda")
+
+
+class SlotPipeline:
+    """Slots from host buffers through the single-GPU pipeline (mb_pipe_*):
+    submit() queues one slot (samples in, LLRs and hard bits out, all host
+    tensors, pinned for overlap) and returns a ticket; wait(ticket) returns
+    once that slot's results are in host memory.  depth slots are in flight:
+    the copies of neighbouring slots overlap each slot's kernels."""
+
+    def __init__(self, cfg, precision="mixed", sym_batch=12, depth=2, ns_iters=2, cond_threshold=1e4,
+                 use_graph=True):
+        cb, zeros, stride = cfg.ldpc()
+        self.cfg = cfg
+        self.cb_size, self.zeros, self.cb_stride = cb, zeros, stride
+        self.hrow = (min(cfg.S * cfg.Qm, cb) + 7) // 8
+        d = _lib.MbCellDesc(cfg.M, cfg.K, cfg.N, cfg.S, cfg.sg, cfg.Qm, cfg.P, cfg.U, 0,
+                            _IQ[cfg.iq_dtype], cb, stride, zeros, _PREC[precision], ns_iters,
+                            cond_threshold, _SCR[cfg.scrambler], cfg.c_init, _IQ["f16"],
+                            sym_batch, int(use_graph))
+        h = ctypes.c_void_p()
+        check(LIB.mb_pipe_create(ctypes.byref(d), depth, ctypes.byref(h)), "mb_pipe_create")
+        self._h = h
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        check(LIB.mb_pipe_io_bytes(h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "mb_pipe_io_bytes")
+        self.iq_bytes, self.llr_bytes, self.hard_bytes = a.value, b.value, c.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            LIB.mb_pipe_destroy(h)
+            self._h = None
+
+    def host_outputs(self):
+        """Pinned host tensors for one slot's LLRs and hard bits."""
+        cfg = self.cfg
+        llr = torch.empty(cfg.U, cfg.K, self.cb_stride, dtype=torch.float16).pin_memory()
+        hard = torch.empty(cfg.U, cfg.K, self.hrow, dtype=torch.uint8).pin_memory()
+        return llr, hard
+
+    def submit(self, iq, llr, hard=None):
+        for t, name, n in ((iq, "iq", self.iq_bytes), (llr, "llr", self.llr_bytes),
+                           (hard, "hard", self.hard_bytes)):
+            if t is None and name == "hard":
+                continue
+            if t.is_cuda or not t.is_contiguous() or t.numel() * t.element_size() != n:
+                raise ValueError(f"{name} must be a contiguous host tensor of {n} bytes")
+        ticket = ctypes.c_uint64()
+        check(LIB.mb_pipe_submit(self._h, ctypes.c_void_p(iq.data_ptr()), ctypes.c_void_p(llr.data_ptr()),
+                                 ctypes.c_void_p(hard.data_ptr()) if hard is not None else None,
+                                 ctypes.byref(ticket)), "mb_pipe_submit")
+        return ticket.value
+
+    def wait(self, ticket, timeout_ms=None):
+        """True once slot `ticket` is done; False if timeout_ms ran out first."""
+        r = LIB.mb_pipe_wait(self._h, ticket, 0xFFFFFFFF if timeout_ms is None else int(timeout_ms))
+        if r == _lib.MB_TIMEOUT:
+            return False
+        check(r, "mb_pipe_wait")
+        return True
+
+    def timer_start(self):
+        """Device timer from the next submitted slot's sample copy on."""
+        check(LIB.mb_pipe_timer_start(self._h), "mb_pipe_timer_start")
+
+    def timer_ms(self):
+        """Device ms from the timer's start to the last submitted slot's results."""
+        ms = ctypes.c_double()
+        check(LIB.mb_pipe_timer_ms(self._h, ctypes.byref(ms)), "mb_pipe_timer_ms")
+        return ms.value
