@@ -85,6 +85,10 @@ extern "C" mb_status mb_pipe_create(const mb_cell_desc *cell, uint32_t depth, mb
     e = cudaMalloc(&p->iq[b], p->iq_bytes);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&p->llr[b]), p->llr_bytes);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&p->hard[b]), p->hard_bytes);
+    // the slot never writes an LLR row's punctured and padding positions:
+    // they stay zero, as in a caller's zeroed buffer
+    if (e == cudaSuccess) e = cudaMemset(p->llr[b], 0, p->llr_bytes);
+    if (e == cudaSuccess) e = cudaMemset(p->hard[b], 0, p->hard_bytes);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&p->status[b]), sizeof(int32_t) * G);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_in[b], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_done[b], cudaEventDisableTiming);
