@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-evm", action="store_true")
     ap.add_argument("--ns-iters", type=int, default=2, help="Newton-Schulz steps of the mixed ZF (config 2 names 2)")
     ap.add_argument("--sym-batch", type=int, default=12)
+    ap.add_argument("--iq", default="int8", choices=["int8", "int16", "c64", "f16"],
+                    help="sample format of the cell256x32 workload: int8 is the reference's production "
+                         "QuanT (utils/types.h:26), int16 the other integer format its FFT takes")
     ap.add_argument("--rotate", type=int, default=4, help="distinct input slots cycled (L2 flush)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -57,9 +60,11 @@ def parse():
     return ap.parse_args()
 
 
-def algorithmic_bytes(cfg, b_in=8):
-    """Compulsory bytes of one uplink slot: samples in, FP16 LLRs and packed
+def algorithmic_bytes(cfg, b_in=None):
+    """Compulsory bytes of one uplink slot: samples in (b_in bytes each, by
+    default those of the workload's sample format), FP16 LLRs and packed
     hard bits out (intermediates excluded)."""
+    b_in = IQ_BYTES[cfg.iq_dtype] if b_in is None else b_in
     cb, zeros, stride = cfg.ldpc()
     n_valid = min(cfg.S * cfg.Qm, cb)
     return (cfg.P + cfg.U) * cfg.M * cfg.N * b_in + cfg.U * cfg.K * n_valid * 2 + \
@@ -209,7 +214,10 @@ def roofline(cfg, args, st, n_valid, hrow):
              "fft_pilot": "fft_kernel<12, pilot>",
              "zf": "zf_mixed_kernel<64>" if mixed else "zf_chol_kernel<float>",
              "equalize": "equalize_tc_kernel<64, 6>" if mixed else "equalize_fp32_kernel"}
-    profiles = {"fft_uplink": "fft_tc_uplink_4096x256" if tc_fft else "fft_uplink_lp_4096x256",
+    # the tensor-core FFT's traffic depends on the sample format: int8
+    # workloads read the int8 capture, the others the int16 one
+    fft_tc_prof = "fft_tc_uplink_4096x256" + ("_int8" if cfg.iq_dtype == "int8" else "")
+    profiles = {"fft_uplink": fft_tc_prof if tc_fft else "fft_uplink_lp_4096x256",
                 "equalize": "equalize_tc_256x32",
                 "zf": "zf_mixed_256x32", "fft_pilot": "fft_uplink_lp_4096x256"}
     for key, v in k.items():
@@ -269,18 +277,21 @@ def run_reference(args, rank, world):
     from megastation_b200 import datagen
     if rank != 0:
         return
-    cfg = datagen.CellConfig(**WORKLOAD)
+    cfg = datagen.CellConfig(**{**WORKLOAD, "iq_dtype": args.iq})
     from oracle import ref_ops
     cb, zeros, stride = cfg.ldpc()
     if ref_ops.available():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        c16 = datagen.CellConfig(**{**cfg.__dict__, "iq_dtype": "int16"})
-        R = max(2, args.rotate)
-        iqs = [torch.from_numpy(datagen.make_slot(datagen.CellConfig(**{**c16.__dict__, "seed": c16.seed + r}))["iq"]
+        # the reference FFT takes integer samples only (fft_op.cu:194-200)
+        iq_ref = args.iq if args.iq in ("int8", "int16") else "int16"
+        cfg = datagen.CellConfig(**{**cfg.__dict__, "iq_dtype": iq_ref})
+        R = rotation(cfg, args)
+        iqs = [torch.from_numpy(datagen.make_slot(datagen.CellConfig(**{**cfg.__dict__, "seed": cfg.seed + r}))["iq"]
                                 ).cuda() for r in range(R)]
         llr = [torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda") for _ in range(2)]
-        ref = ref_ops.RefSlot(cfg.M, cfg.K, cfg.N, cfg.S, cfg.sg, cfg.Qm, cfg.P, cfg.U, cb, zeros, stride)
+        ref = ref_ops.RefSlot(cfg.M, cfg.K, cfg.N, cfg.S, cfg.sg, cfg.Qm, cfg.P, cfg.U, cb, zeros, stride,
+                              iq=iq_ref)
         stream = torch.cuda.Stream()
         for k in range(max(args.warmup, 3)):
             ref.uplink(iqs[k % R].data_ptr(), llr[k % 2].data_ptr(), stream.cuda_stream)
@@ -300,8 +311,8 @@ def run_reference(args, rank, world):
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded, megastation_b200.datagen), int16 samples",
-                "config": {**workload_config(cfg, args), "iq_dtype": "int16 (the reference FFT takes integer IQ)"},
+                "data": f"synthetic (seeded, megastation_b200.datagen), {iq_ref} samples",
+                "config": {**workload_config(cfg, args, R), "iq_dtype": iq_ref},
                 "clocks": clk,
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": 0, "kind": "reference",
                                  "sample": f"{args.steps} slots through the reference's own CUDA operators "
@@ -432,12 +443,22 @@ def evm_report(cfg, d, sym_batch, ns_iters=2):
     return out
 
 
-def workload_config(cfg, args):
+def rotation(cfg, args):
+    """Distinct input slots cycled through the timed steps: at least
+    --rotate, and enough that the rotated samples alone exceed 1.25x the
+    126 MB L2, so every step reads its samples from HBM."""
+    slot_bytes = cfg.symbols * cfg.M * cfg.N * IQ_BYTES[cfg.iq_dtype]
+    return max(2, args.rotate, -(-int(1.25 * 126e6) // slot_bytes))
+
+
+def workload_config(cfg, args, R=None):
+    R = rotation(cfg, args) if R is None else R
     return {"workload": "uplink slot 256x32, N=4096, S=3276, 2 pilot + 12 data symbols, 64-QAM, "
                         f"8-tap exp-PDP rho=0.5, 25 dB, {cfg.iq_dtype} samples",
             "M": cfg.M, "K": cfg.K, "N": cfg.N, "S": cfg.S, "sg": cfg.sg, "Qm": cfg.Qm, "P": cfg.P,
-            "U": cfg.U, "precision": args.precision, "sym_batch": args.sym_batch, "ns_iters": args.ns_iters,
-            "l2": f"inputs {cfg.symbols * cfg.M * cfg.N * IQ_BYTES[cfg.iq_dtype] / 1e6:.0f} MB per slot, {args.rotate} "
+            "U": cfg.U, "iq_dtype": cfg.iq_dtype, "precision": args.precision, "sym_batch": args.sym_batch,
+            "ns_iters": args.ns_iters,
+            "l2": f"inputs {cfg.symbols * cfg.M * cfg.N * IQ_BYTES[cfg.iq_dtype] / 1e6:.1f} MB per slot, {R} "
                   "slots rotated (larger than the 126 MB L2)",
             "seed": cfg.seed}
 
@@ -741,13 +762,13 @@ def main():
 
     import megastation_b200 as mb
     from megastation_b200 import datagen, slot
-    cfg = datagen.CellConfig(**WORKLOAD)
+    cfg = datagen.CellConfig(**{**WORKLOAD, "iq_dtype": args.iq})
     d = datagen.make_slot(cfg)
     cb, zeros, stride = cfg.ldpc()
     n_valid = min(cfg.S * cfg.Qm, cb)
     hrow = (n_valid + 7) // 8
 
-    R = max(2, args.rotate)
+    R = rotation(cfg, args)
     iq_host = torch.from_numpy(d["iq"]).pin_memory()
     iq_dev = [iq_host.cuda() for _ in range(R)]
     stream = torch.cuda.Stream()

@@ -26,6 +26,8 @@ def lib():
         VP, U32, U64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
         L.ref_slot_create.restype = VP
         L.ref_slot_create.argtypes = [U32] * 8 + [U64] * 3
+        L.ref_slot_create_iq.restype = VP
+        L.ref_slot_create_iq.argtypes = [U32] * 8 + [U64] * 3 + [U32]
         L.ref_slot_destroy.argtypes = [VP]
         L.ref_slot_uplink.restype = ctypes.c_int
         L.ref_slot_uplink.argtypes = [VP, VP, VP, VP]
@@ -36,10 +38,14 @@ def lib():
 
 
 class RefSlot:
-    """One cell's uplink slot through the reference operators (int16 IQ)."""
+    """One cell's uplink slot through the reference operators: int16 IQ, or
+    int8 IQ (the reference's production sample type) with iq="int8"."""
 
-    def __init__(self, M, K, N, S, sg, Qm, P, U, cb_size, zeros, cb_stride):
-        self._h = lib().ref_slot_create(M, K, N, S, sg, Qm, P, U, cb_size, zeros, cb_stride)
+    def __init__(self, M, K, N, S, sg, Qm, P, U, cb_size, zeros, cb_stride, iq="int16"):
+        if iq not in ("int16", "int8"):
+            raise ValueError("the reference FFT takes int16 or int8 samples")
+        self._h = lib().ref_slot_create_iq(M, K, N, S, sg, Qm, P, U, cb_size, zeros, cb_stride,
+                                           1 if iq == "int8" else 0)
         if not self._h:
             raise RuntimeError("ref_slot_create failed")
 

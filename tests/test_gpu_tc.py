@@ -116,10 +116,14 @@ CASES = [
     # about 13 units per CTA
     dict(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=12, snr_db=25.0, seed=19, channel="tdl", rho=0.5,
          n_taps=8, tap_decay=2.0),
+    # the same shape on int8 samples, the reference's production format
+    dict(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=12, snr_db=25.0, seed=20, channel="tdl", rho=0.5,
+         n_taps=8, tap_decay=2.0, iq_dtype="int8"),
 ]
 
 
-@pytest.mark.parametrize("case", CASES, ids=[f"{c['M']}x{c['K']}Q{c['Qm']}N{c['N']}" for c in CASES])
+@pytest.mark.parametrize("case", CASES, ids=[f"{c['M']}x{c['K']}Q{c['Qm']}N{c['N']}{c.get('iq_dtype', '')}"
+                                             for c in CASES])
 def test_slot_uplink_mixed_vs_oracle(mb, case):
     from megastation_b200 import datagen, slot
     cfg = datagen.CellConfig(**case)
