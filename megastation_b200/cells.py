@@ -41,7 +41,7 @@ class Cells:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
             LIB.mb_cells_destroy(h)
             self._h = None
 

@@ -43,7 +43,7 @@ class MLP:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
             LIB.mb_mlp_destroy(h)
             self._h = None
 
@@ -103,7 +103,7 @@ class LearnedZF:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
             LIB.mb_lzf_destroy(h)
             self._h = None
 

@@ -68,7 +68,7 @@ class _FFTBase:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
             LIB.mb_fft_destroy(h)
             self._h = None
 
@@ -152,7 +152,7 @@ class Beamform:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
             LIB.mb_zf_destroy(h)
             self._h = None
 
@@ -204,7 +204,7 @@ class Scrambler:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
             LIB.mb_scrambler_destroy(h)
             self._h = None
 

@@ -39,7 +39,7 @@ class UplinkSlot:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
             LIB.mb_slot_destroy(h)
             self._h = None
 
@@ -112,7 +112,7 @@ class SlotPipeline:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
             LIB.mb_pipe_destroy(h)
             self._h = None
 
