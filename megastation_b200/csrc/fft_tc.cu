@@ -371,9 +371,12 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     const uint32_t lane_row = quad * 32 + lane;
     const uint32_t tl = tmem + ((quad * 32) << 16);
     const uint32_t e_n2 = lane_row & 63, e_r = lane_row >> 6;
-    float2 tw[16];  // W4096^(n2 k1)
-#pragma unroll
-    for (int j = 0; j < 16; j++) tw[j] = __ldg(p.tw + ((e_n2 * (16 * part + j)) & (kFtN - 1)));
+    // W4096^(n2 k1) for k1 = 16 part + j is tw0 tws^j, formed by recurrence in
+    // the twiddle phase (15 FP32 complex products: about 2e-6 relative, far
+    // below the FP16 rounding of the result); holding all 16 twiddles for the
+    // whole kernel cost 32 registers and made the threads spill
+    const float2 tw0 = __ldg(p.tw + ((e_n2 * 16 * part) & (kFtN - 1)));
+    const float2 tws = __ldg(p.tw + e_n2);
     const uint32_t z_off = mnmaj_off(64 * e_r + 16 * part, e_n2);
     // GEMM-2 epilogue: TMEM lane (r, k1), k2 in [16 part, 16 part + 16); bin
     // k1 + 64 k2 is subcarrier (k1 + 64 k2 - c) mod N.  With c even the even
@@ -393,27 +396,27 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       // integer samples: the FFT of q * 2^-8 (int16) or of q (int8) is the
       // FFT of the normalised samples q / 2^15 or q / 2^7 times 2^7
       const float inv = kFixedScale<DT> ? 1.0f / 128.0f : s_inv[i & 1][s_r];
-      float vr[16], vi[16];
-      tc::tmem_ld16(tl + 128 + 16 * part, vr);
-      tc::tmem_ld16(tl + 192 + 16 * part, vi);
       const uint32_t row = 2 * unit_of(i) + s_r;  // the same for the whole warp
       if (row < p.pilot_rows) {
         // LS estimate conj(X) p of subcarrier sc for user u0 + sc % sg into
         // csi[sc / sg][b][u] (fft_callback.cuh:76-108); a user with no pilot
-        // in the short last group takes its estimate from group G-2.  The
-        // pilot signs are all loaded before any branch, so their latencies
-        // overlap.
+        // in the short last group takes its estimate from group G-2.  Eight
+        // bins at a time (half the accumulator registers live at once, which
+        // keeps this branch from spilling); their pilot signs are loaded
+        // before any branch, so the latencies overlap.
         const uint32_t sym = row / p.M, b = row - sym * p.M, u0 = p.ue_start + sym * p.sg;
 #pragma unroll
         for (int jb = 0; jb < 16; jb += 8) {
           float2 ps[8];
 #pragma unroll
           for (int j = 0; j < 8; j++) ps[j] = __ldg(p.pilot + min((s_base + 64 * (jb + j)) & (kFtN - 1), p.S - 1));
+          float vr[8], vi[8];
+          tc::tmem_ld8x2(tl + 128 + 16 * part + jb, vr, tl + 192 + 16 * part + jb, vi);
 #pragma unroll
           for (int j = 0; j < 8; j++) {
             const uint32_t sc = (s_base + 64 * (jb + j)) & (kFtN - 1);
             const uint32_t g = __umulhi(sc, p.sg_magic), sl = sc - g * p.sg, uu = u0 + sl;
-            const float x = vr[jb + j] * inv, y = vi[jb + j] * inv;
+            const float x = vr[j] * inv, y = vi[j] * inv;
             const float2 e = make_float2(x * ps[j].x + y * ps[j].y, x * ps[j].y - y * ps[j].x);
             if (sc < p.S && uu < p.K) {
               float2 *d = p.csi + ((uint64_t)g * p.M + b) * p.K + uu;
@@ -422,7 +425,13 @@ __global__ void __launch_bounds__(kFtThreads, 1)
             }
           }
         }
-      } else if (pairs) {
+        arrive(&st_ready);
+        return;
+      }
+      float vr[16], vi[16];
+      tc::tmem_ld16(tl + 128 + 16 * part, vr);
+      tc::tmem_ld16(tl + 192 + 16 * part, vi);
+      if (pairs) {
 #pragma unroll
         for (int j = 0; j < 16; j++) {
           const uint32_t own = bf2_bits(vr[j] * inv, vi[j] * inv);
@@ -536,18 +545,19 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       wait_ok(&d1_full, i & 1);
       tc::fence_after_sync();
       if (ok) {
-        float yr[16], yi[16];
-        tc::tmem_ld16(tl + 16 * part, yr);
-        tc::tmem_ld16(tl + 64 + 16 * part, yi);
+        float2 w = tw0;
+        // eight k1 at a time: half the accumulator registers live at once
 #pragma unroll
         for (int g = 0; g < 2; g++) {
+          float yr[8], yi[8];
+          tc::tmem_ld8x2(tl + 16 * part + 8 * g, yr, tl + 64 + 16 * part + 8 * g, yi);
           float zr[8], zi[8];
 #pragma unroll
           for (int b = 0; b < 8; b++) {
-            const float2 w = tw[8 * g + b];
-            const float xr = yr[8 * g + b], xi = yi[8 * g + b];
+            const float xr = yr[b], xi = yi[b];
             zr[b] = xr * w.x - xi * w.y;
             zi[b] = xr * w.y + xi * w.x;
+            w = make_float2(w.x * tws.x - w.y * tws.y, w.x * tws.y + w.y * tws.x);
           }
           *reinterpret_cast<uint4 *>(sAZ + z_off + g * 128) =
               make_uint4(h2_bits(zr[0], zr[1]), h2_bits(zr[2], zr[3]), h2_bits(zr[4], zr[5]), h2_bits(zr[6], zr[7]));

@@ -113,6 +113,24 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// 8 consecutive fp32 columns at each of two TMEM addresses of this thread's
+// lane, one wait for both (warp-collective)
+__device__ __forceinline__ void tmem_ld8x2(uint32_t ta, float *va, uint32_t tb, float *vb) {
+  uint32_t a[8], b[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7])
+               : "r"(ta));
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(b[0]), "=r"(b[1]), "=r"(b[2]), "=r"(b[3]), "=r"(b[4]), "=r"(b[5]), "=r"(b[6]), "=r"(b[7])
+               : "r"(tb));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    va[i] = __uint_as_float(a[i]);
+    vb[i] = __uint_as_float(b[i]);
+  }
+}
+
 // Shared-memory matrix descriptor, no swizzle ("interleave") canonical
 // layouts built from 8x16-byte core matrices:
 //   K-major : core matrix = 8 rows x 8 K-elements; lbo = byte step between
