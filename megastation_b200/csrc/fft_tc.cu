@@ -428,18 +428,23 @@ __global__ void __launch_bounds__(kFtThreads, 1)
         arrive(&st_ready);
         return;
       }
-      float vr[16], vi[16];
-      tc::tmem_ld16(tl + 128 + 16 * part, vr);
-      tc::tmem_ld16(tl + 192 + 16 * part, vi);
       if (pairs) {
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          const uint32_t own = bf2_bits(vr[j] * inv, vi[j] * inv);
-          const uint32_t other = __shfl_xor_sync(0xffffffffu, own, 1);
-          const uint32_t s0 = (s_base + 64 * j) & (kFtN - 2);
-          *reinterpret_cast<uint32_t *>(stg_mine + 2 * s0) = __byte_perm(own, other, perm);
+        for (int jb = 0; jb < 16; jb += 8) {
+          float vr[8], vi[8];
+          tc::tmem_ld8x2(tl + 128 + 16 * part + jb, vr, tl + 192 + 16 * part + jb, vi);
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const uint32_t own = bf2_bits(vr[j] * inv, vi[j] * inv);
+            const uint32_t other = __shfl_xor_sync(0xffffffffu, own, 1);
+            const uint32_t s0 = (s_base + 64 * (jb + j)) & (kFtN - 2);
+            *reinterpret_cast<uint32_t *>(stg_mine + 2 * s0) = __byte_perm(own, other, perm);
+          }
         }
       } else {
+        float vr[16], vi[16];
+        tc::tmem_ld16(tl + 128 + 16 * part, vr);
+        tc::tmem_ld16(tl + 192 + 16 * part, vi);
 #pragma unroll
         for (int j = 0; j < 16; j++) {
           const uint32_t sc = (s_base + 64 * j) & (kFtN - 1);
