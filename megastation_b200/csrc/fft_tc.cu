@@ -183,9 +183,12 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 
 // Bounded wait that also gives up as soon as another thread has failed.
 __device__ __forceinline__ bool ft_wait(uint64_t *bar, uint32_t parity, volatile int *fail) {
-  if (tc::mbar_try_wait(bar, parity)) return true;
+  // a 20 us suspend hint: waiting warps poll less and leave issue slots to
+  // the others (an A/B on one B200: 45.4 -> 44.5 us for the slot launch;
+  // within the spread between boxes)
+  if (tc::mbar_try_wait_hint(bar, parity, 20000u)) return true;
   const uint64_t t0 = tc::globaltimer();
-  while (!tc::mbar_try_wait(bar, parity)) {
+  while (!tc::mbar_try_wait_hint(bar, parity, 20000u)) {
     if (*fail || tc::globaltimer() - t0 > 1000000000ull) {
       *fail = 1;
       return false;

@@ -44,6 +44,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
+// try_wait that may suspend the thread until the phase completes or
+// hint_ns have passed, whichever comes first (fewer polling instructions
+// for warps that wait long)
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t *bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Waits for completion of the phase with the given parity; gives up after
 // limit_ns of wall time and returns false (the caller records an error).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
