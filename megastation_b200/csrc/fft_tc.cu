@@ -378,7 +378,15 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     // the twiddle phase (15 FP32 complex products: about 2e-6 relative, far
     // below the FP16 rounding of the result); holding all 16 twiddles for the
     // whole kernel cost 32 registers and made the threads spill
-    const float2 tw0 = __ldg(p.tw + ((e_n2 * 16 * part) & (kFtN - 1)));
+    float2 tw0 = __ldg(p.tw + ((e_n2 * 16 * part) & (kFtN - 1)));
+    if constexpr (kFixedScale<DT>) {
+      // integer samples: the FFT of q * 2^-8 (int16) or of q (int8) is the
+      // FFT of the normalised samples q / 2^15 or q / 2^7 times 2^7; the
+      // exact 1/128 rides in the twiddles (GEMM 2 is linear), so the
+      // epilogues need no multiply
+      tw0.x *= 1.0f / 128.0f;
+      tw0.y *= 1.0f / 128.0f;
+    }
     const float2 tws = __ldg(p.tw + e_n2);
     const uint32_t z_off = mnmaj_off(64 * e_r + 16 * part, e_n2);
     // GEMM-2 epilogue: TMEM lane (r, k1), k2 in [16 part, 16 part + 16); bin
@@ -396,9 +404,9 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     __shared__ float s_inv[2][2];  // [unit parity][row] inverse row scales
 
     auto store_unit = [&](uint32_t i) {
-      // integer samples: the FFT of q * 2^-8 (int16) or of q (int8) is the
-      // FFT of the normalised samples q / 2^15 or q / 2^7 times 2^7
-      const float inv = kFixedScale<DT> ? 1.0f / 128.0f : s_inv[i & 1][s_r];
+      // row scale to undo (integer samples: none, the 1/128 is already in
+      // the twiddles)
+      const float inv = kFixedScale<DT> ? 1.0f : s_inv[i & 1][s_r];
       const uint32_t row = 2 * unit_of(i) + s_r;  // the same for the whole warp
       if (row < p.pilot_rows) {
         // LS estimate conj(X) p of subcarrier sc for user u0 + sc % sg into
@@ -486,15 +494,24 @@ __global__ void __launch_bounds__(kFtThreads, 1)
                 hr = __halves2half2(__short2half_rn((short)(a & 0xFFFFu)), __short2half_rn((short)(b & 0xFFFFu)));
                 hi = __halves2half2(__short2half_rn((short)(a >> 16)), __short2half_rn((short)(b >> 16)));
               } else {
+                // int8 (re, im, re, im) bytes: with the sign bits flipped a
+                // byte is x + 128, and the FP16 bit pattern 0x64XX is
+                // 1024 + XX exactly, so one byte permute per half2 and one
+                // subtraction of 1152 give x (exact)
                 const uint4 w = raw[c2][0];
-                const uint32_t v = t == 0 ? w.x : t == 1 ? w.y : t == 2 ? w.z : w.w;  // samples 2t, 2t+1
-                hr = __halves2half2(__short2half_rn((short)(int8_t)(v & 0xFFu)),
-                                    __short2half_rn((short)(int8_t)((v >> 16) & 0xFFu)));
-                hi = __halves2half2(__short2half_rn((short)(int8_t)((v >> 8) & 0xFFu)),
-                                    __short2half_rn((short)(int8_t)(v >> 24)));
+                const uint32_t v = (t == 0 ? w.x : t == 1 ? w.y : t == 2 ? w.z : w.w) ^ 0x80808080u;
+                const uint32_t rb = __byte_perm(v, 0x64646464u, 0x4240u);  // bytes 0, 2 (re)
+                const uint32_t ib = __byte_perm(v, 0x64646464u, 0x4341u);  // bytes 1, 3 (im)
+                const __half2 bias = __float2half2_rn(1152.0f);
+                memcpy(&hr, &rb, 4);
+                memcpy(&hi, &ib, 4);
+                hr = __hsub2(hr, bias);
+                hi = __hsub2(hi, bias);
               }
-              hr = __hmul2(hr, sc2);
-              hi = __hmul2(hi, sc2);
+              if constexpr (DT == MB_IQ_I16) {
+                hr = __hmul2(hr, sc2);
+                hi = __hmul2(hi, sc2);
+              }
               memcpy(&rw[t], &hr, 4);
               memcpy(&iw[t], &hi, 4);
             }
