@@ -98,10 +98,12 @@ __global__ void __launch_bounds__(kEqThreads, 1)
       tc::mbar_arrive_expect_tx(&full_bar[s], y_bytes + a_tile);
       tc::bulk_g2s(sa, a_g + (uint64_t)kt * a_tile, a_tile, &full_bar[s]);
       const uint32_t kk0 = kt * kKT, plane = kk0 / q.Mp, b0 = kk0 % q.Mp;
-      for (uint32_t j = 0; j < ncols / 8; j++) {
-        const uint32_t col0 = j * 8, l = col0 / p.sg, sl = col0 % p.sg;
+      // boxes of 16 (swizzled, 2 KB) or 8 (1 KB) columns by the 64 k rows
+      const uint32_t bw = q.y16 ? 16 : 8;
+      for (uint32_t j = 0; j < ncols / bw; j++) {
+        const uint32_t col0 = j * bw, l = col0 / p.sg, sl = col0 % p.sg;
         const int32_t row = (int32_t)(((l_off + l) * 2 + plane) * p.M + b0);
-        tc::tma_load_2d(sy + j * 1024, &ymap, (int32_t)(s_base + sl), row, &full_bar[s]);
+        tc::tma_load_2d(sy + j * bw * 128, &ymap, (int32_t)(s_base + sl), row, &full_bar[s]);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -119,9 +121,12 @@ __global__ void __launch_bounds__(kEqThreads, 1)
       const uint32_t y0 = tc::smem_u32(eq_smem + s * stage_bytes), a0 = y0 + y_tile;
 #pragma unroll
       for (int ks = 0; ks < kKT / 16; ks++) {
-        // Y: MN-major, 8-antenna K groups 128 B apart, 8-subcarrier MN
-        // chunks 1024 B apart (one tensor box each)
-        const uint64_t yd = tc::smem_desc(y0 + ks * 256, 128, 1024);
+        // Y: MN-major.  8-column boxes: 8-antenna K groups 128 B apart,
+        // 8-subcarrier MN chunks 1024 B apart (one box each); 16-column
+        // swizzled boxes: 32-byte atoms of 16 columns 2048 B apart (one box
+        // each), 8-antenna K groups 256 B apart
+        const uint64_t yd = q.y16 ? tc::smem_desc_mn_sw32(y0 + ks * 512, 2048, 256)
+                                  : tc::smem_desc(y0 + ks * 256, 128, 1024);
         // image: K-major, K core matrices 128 B apart, 8-row groups 1024 B apart
         const uint64_t ad = tc::smem_desc(a0 + ks * 256, 128, 1024);
         tc::mma_f16(tmem, yd, ad, idesc, (kt | ks) != 0);
@@ -364,10 +369,14 @@ mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, ui
   MB_CUDA_TRY(cudaGetDevice(&dev));
   mb_status cs = equalize_tc_configure(s.MM, p.Qm, dev);
   if (cs != MB_OK) return cs;
-  // tensor map over y_lp rows [nb * 2 * M][S_pad], box 8 subcarriers x 64
-  // antennas (one 1 KB group of MN-major core matrices)
+  // tensor map over y_lp rows [nb * 2 * M][S_pad], box 16 subcarriers x 64
+  // antennas with the 32-byte swizzle (one 2 KB MN-major SW32 atom column:
+  // whole 32-byte sectors per antenna row) when groups are whole boxes, else
+  // 8 subcarriers x 64 antennas (one 1 KB group of MN-major core matrices)
+  q.y16 = p.sg % 16 == 0 ? 1 : 0;
   CUtensorMap ymap;
-  mb_status tr = make_tmap_2d_bf16(&ymap, y_lp, S_pad, (uint64_t)nb * 2 * p.M, S_pad, 8, kKT);
+  mb_status tr = make_tmap_2d_bf16(&ymap, y_lp, S_pad, (uint64_t)nb * 2 * p.M, S_pad, q.y16 ? 16 : 8, kKT,
+                                   q.y16 != 0);
   if (tr != MB_OK) return tr;
   const dim3 grid(G, ny);
   (s.MM == 64 ? eq_tc_kernel_of<64>(p.Qm) : eq_tc_kernel_of<128>(p.Qm))<<<grid, kEqThreads, smem, st>>>(q, ymap);

@@ -12,6 +12,7 @@ struct EqTcParams {
   const __nv_bfloat16 *y_lp;  // [nb][re|im][M][S_pad]
   uint32_t S_pad, Mp, nkt, N, l0, tmem_cols;
   uint32_t spc, nb;           // symbols per CTA, symbols in the launch
+  uint32_t y16;               // 1: 16-subcarrier y boxes, 32-byte swizzle (sg % 16 == 0)
   int *err;
 };
 

@@ -116,7 +116,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 mb_status make_tmap_2d_bf16(CUtensorMap *map, const void *base, uint64_t width, uint64_t rows,
-                            uint64_t pitch_elems, uint32_t box_x, uint32_t box_y) {
+                            uint64_t pitch_elems, uint32_t box_x, uint32_t box_y, bool sw32) {
   static EncodeTiledFn fn = nullptr;
   static std::mutex mu;
   {
@@ -130,12 +130,14 @@ mb_status make_tmap_2d_bf16(CUtensorMap *map, const void *base, uint64_t width, 
     }
   }
   if ((pitch_elems * 2) % 16 || (reinterpret_cast<uintptr_t>(base) % 16)) return MB_BAD_ARG;
+  if (sw32 && box_x * 2 != 32) return MB_BAD_ARG;
   cuuint64_t dims[2] = {width, rows};
   cuuint64_t strides[1] = {pitch_elems * 2};
   cuuint32_t box[2] = {box_x, box_y};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
-                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  sw32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? MB_OK : MB_BAD_ARG;
 }

@@ -164,6 +164,15 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
   return d;
 }
 
+// Shared-memory matrix descriptor of an MN-major operand in the 32-byte
+// swizzle canonical layout: atoms of 16 MN elements (32 bytes) by 8 K rows
+// (256 bytes, as a 32-byte-swizzled TMA box row group stores them: the two
+// 16-byte halves of rows 4-7 swapped); lbo = byte step between atoms along
+// MN, sbo = byte step between 8-row K groups; start 256-byte aligned.
+__device__ __forceinline__ uint64_t smem_desc_mn_sw32(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return smem_desc(saddr, lbo, sbo) | ((uint64_t)6 << 61);  // layout type 6: 32-byte swizzle
+}
+
 // Instruction descriptor, kind::f16: FP32 accumulate, BF16 A and B.
 __host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N, bool a_mn_major,
                                                   bool b_mn_major) {
@@ -227,9 +236,11 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
 }  // namespace tc
 
 // Host: a 2-D BF16 tensor map over rows of `pitch_elems` elements (row pitch
-// a multiple of 16 bytes), box = box_x elements by box_y rows, no swizzle.
+// a multiple of 16 bytes), box = box_x elements by box_y rows; no swizzle,
+// or with sw32 (box_x = 16) the 32-byte swizzle: box row y's two 16-byte
+// halves swap places when y % 8 >= 4 (boxes 256-byte aligned).
 mb_status make_tmap_2d_bf16(CUtensorMap *map, const void *base, uint64_t width, uint64_t rows,
-                            uint64_t pitch_elems, uint32_t box_x, uint32_t box_y);
+                            uint64_t pitch_elems, uint32_t box_x, uint32_t box_y, bool sw32 = false);
 // Host: a 2-D byte tensor map, 128-byte boxes of box_y rows, 128-byte
 // swizzle in shared memory.
 mb_status make_tmap_2d_u8_sw128(CUtensorMap *map, const void *base, uint64_t width, uint64_t rows,
