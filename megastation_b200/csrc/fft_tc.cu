@@ -205,12 +205,19 @@ __global__ void __launch_bounds__(kFtThreads, 1)
   // need them); the staging rows follow
   uint8_t *sF = ft_smem, *sAZ = ft_smem + kMat, *sRing = ft_smem + 2 * kMat;
   uint8_t *sStg = sRing + 2 * kStage;
+  // GEMM operand buffers: integer samples fill at most half of a ring slot,
+  // so a second buffer (unit i uses buffer i & 1) sits behind ring slot 0's
+  // samples and the conversion of unit i + 1 need not wait for GEMM 2 of
+  // unit i to read the first; other sample types keep the one buffer.
+  // d2_full[u & 1] completes when GEMM 2 of unit u has finished.
+  constexpr bool kAZ2 = Fmt<DT>::kUnitBytes + kMat <= kStage;
+  uint8_t *const sAZ1 = kAZ2 ? sRing + Fmt<DT>::kUnitBytes : sAZ;
   // Each barrier completes once per unit.  a_ready comes as a pair per ring
   // slot, waited with parity (i >> 1) & 1: the copy warp may trail the
   // compute warps by two units (while it drains a bulk store), and a plain
   // parity wait would then alias a later phase.  full is per slot anyway;
   // every other barrier's waiters are at most one phase behind.
-  __shared__ uint64_t bar_mats, full[2], a_ready[2], z_ready, st_ready, d1_full, d2_full, st_done;
+  __shared__ uint64_t bar_mats, full[2], a_ready[2], z_ready, st_ready, d1_full, d2_full[2], st_done;
   __shared__ uint32_t tmem_slot;
   __shared__ __align__(16) uint32_t s_rmax[16];
   __shared__ volatile int s_fail;
@@ -232,7 +239,8 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     tc::mbar_init(&z_ready, kFtCompute / 32);
     tc::mbar_init(&st_ready, kFtCompute / 32);
     tc::mbar_init(&d1_full, 1);
-    tc::mbar_init(&d2_full, 1);
+    tc::mbar_init(&d2_full[0], 1);
+    tc::mbar_init(&d2_full[1], 1);
     tc::mbar_init(&st_done, 1);
     s_fail = 0;
     tc::fence_mbar_init();
@@ -255,37 +263,40 @@ __global__ void __launch_bounds__(kFtThreads, 1)
   if (warp == kFtCompute / 32) {
     // ================================================== GEMM warp
     if (lane == 0) {
-      const uint32_t fa = tc::smem_u32(sF), az = tc::smem_u32(sAZ);
+      const uint32_t fa = tc::smem_u32(sF);
       const uint32_t idesc = tc::idesc_f16(128, 128, true, false);  // A MN-major, B K-major
-      // both GEMMs read the operand buffer (MN-major) and F (K-major)
-      uint64_t da[8], db[8];
+      // both GEMMs read the unit's operand buffer (MN-major) and F (K-major);
+      // k step ks of the operand is 4096 bytes on, i.e. 256 in the
+      // descriptor's address field (no carry: addresses stay below 256 KB)
+      const uint64_t da_0 = tc::smem_desc(tc::smem_u32(sAZ), 2048, 128);
+      const uint64_t da_1 = tc::smem_desc(tc::smem_u32(sAZ1), 2048, 128);
+      uint64_t db[8];
 #pragma unroll
-      for (int ks = 0; ks < 8; ks++) {
-        da[ks] = tc::smem_desc(az + ks * 4096, 2048, 128);
-        db[ks] = tc::smem_desc(fa + ks * 256, 128, 2048);
-      }
+      for (int ks = 0; ks < 8; ks++) db[ks] = tc::smem_desc(fa + ks * 256, 128, 2048);
       uint32_t n_d1 = 0, n_d2 = 0;
       bool ok = ft_wait(&bar_mats, 0, &s_fail);
       for (uint32_t i = 0; i < n_units && ok; i++) {
         // GEMM 1: D1 (128 (r, n2) x 128 (p', k1)) = A (samples) x F
         if (!ft_wait(&a_ready[i & 1], (i >> 1) & 1, &s_fail)) break;
         tc::fence_after_sync();
+        const uint64_t da = (i & 1) ? da_1 : da_0;
 #pragma unroll
-        for (int ks = 0; ks < 8; ks++) tc::mma_f16(tmem, da[ks], db[ks], idesc, ks > 0);
+        for (int ks = 0; ks < 8; ks++) tc::mma_f16(tmem, da + (uint64_t)(ks * 256), db[ks], idesc, ks > 0);
         tc::mma_commit(&d1_full);
         n_d1++;
         // GEMM 2: D2 (128 (r, k1) x 128 (p', k2)) = Z x F
         if (!ft_wait(&z_ready, i & 1, &s_fail)) break;
         tc::fence_after_sync();
 #pragma unroll
-        for (int ks = 0; ks < 8; ks++) tc::mma_f16(tmem + 128, da[ks], db[ks], idesc, ks > 0);
-        tc::mma_commit(&d2_full);
+        for (int ks = 0; ks < 8; ks++) tc::mma_f16(tmem + 128, da + (uint64_t)(ks * 256), db[ks], idesc, ks > 0);
+        tc::mma_commit(&d2_full[i & 1]);
         n_d2++;
       }
       if (s_fail) {
         // a wait ran out: let the issued GEMMs drain (bounded)
         if (n_d1) tc::mbar_wait(&d1_full, (n_d1 - 1) & 1, 100000000ull);
-        if (n_d2) tc::mbar_wait(&d2_full, (n_d2 - 1) & 1, 100000000ull);
+        for (uint32_t u = n_d2 >= 2 ? n_d2 - 2 : 0; u < n_d2; u++)
+          tc::mbar_wait(&d2_full[u & 1], (u >> 1) & 1, 100000000ull);
       }
     }
   } else if (warp == kFtCompute / 32 + 1) {
@@ -350,6 +361,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       if (ok) ok = ft_wait(bar, parity, &s_fail);
       ok = __all_sync(0xffffffffu, ok);
     };
+    auto wait_d2 = [&](uint32_t u) { wait_ok(&d2_full[u & 1], (u >> 1) & 1); };
     auto arrive = [&](uint64_t *bar) {
       tc::fence_proxy_async_smem();
       tc::fence_before_sync();
@@ -548,20 +560,24 @@ __global__ void __launch_bounds__(kFtThreads, 1)
           }
         }
       }
-      // the operand buffer holds Z of the previous unit until GEMM 2 has read it
-      if (i > 0) wait_ok(&d2_full, (i - 1) & 1);
+      // the operand buffer holds Z of its previous unit (i - 2 with two
+      // buffers, i - 1 with one) until that unit's GEMM 2 has read it
+      uint8_t *az = (i & 1) ? sAZ1 : sAZ;
+      if (kAZ2 ? i > 1 : i > 0) wait_d2(kAZ2 ? i - 2 : i - 1);
       tc::fence_after_sync();
       if (ok) {
 #pragma unroll
         for (int c2 = 0; c2 < 2; c2++) {
-          *reinterpret_cast<uint4 *>(sAZ + a_off[c2]) = re[c2];
-          *reinterpret_cast<uint4 *>(sAZ + a_off[c2] + 16384) = im[c2];
+          *reinterpret_cast<uint4 *>(az + a_off[c2]) = re[c2];
+          *reinterpret_cast<uint4 *>(az + a_off[c2] + 16384) = im[c2];
         }
       }
       arrive(&a_ready[i & 1]);
       // (b) GEMM-2 epilogue of the previous unit into the staging rows,
       // once the bulk copies of the unit before it have read them
       if (i > 0) {
+        wait_d2(i - 1);  // D2 of unit i - 1 (already waited with one buffer)
+        tc::fence_after_sync();
         if (i > 1) wait_ok(&st_done, (i - 2) & 1);
         if (ok) store_unit(i - 1);
         else arrive(&st_ready);
@@ -584,9 +600,9 @@ __global__ void __launch_bounds__(kFtThreads, 1)
             zi[b] = xr * w.y + xi * w.x;
             w = make_float2(w.x * tws.x - w.y * tws.y, w.x * tws.y + w.y * tws.x);
           }
-          *reinterpret_cast<uint4 *>(sAZ + z_off + g * 128) =
+          *reinterpret_cast<uint4 *>(az + z_off + g * 128) =
               make_uint4(h2_bits(zr[0], zr[1]), h2_bits(zr[2], zr[3]), h2_bits(zr[4], zr[5]), h2_bits(zr[6], zr[7]));
-          *reinterpret_cast<uint4 *>(sAZ + z_off + g * 128 + 16384) =
+          *reinterpret_cast<uint4 *>(az + z_off + g * 128 + 16384) =
               make_uint4(h2_bits(zi[0], zi[1]), h2_bits(zi[2], zi[3]), h2_bits(zi[4], zi[5]), h2_bits(zi[6], zi[7]));
         }
       }
@@ -594,7 +610,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
     }
     // the last unit's inverse scales were written after the last barrier
     if constexpr (!kFixedScale<DT>) compute_sync();
-    wait_ok(&d2_full, (n_units - 1) & 1);
+    wait_d2(n_units - 1);
     tc::fence_after_sync();
     if (n_units > 1) wait_ok(&st_done, (n_units - 2) & 1);
     if (ok) store_unit(n_units - 1);
