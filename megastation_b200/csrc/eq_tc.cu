@@ -203,7 +203,6 @@ __global__ void __launch_bounds__(kEqThreads, 1)
     if (tid == 0 && q.err) atomicOr(q.err, tc::kErrTimeout);
   } else {
     tc::fence_after_sync();
-    const __half zero = __float2half_rn(0.f);
     // chunk loop not unrolled: the chunk's bytes are always in sqw[0], the
     // array rotating by one chunk per pass
 #pragma unroll 1
@@ -218,24 +217,22 @@ __global__ void __launch_bounds__(kEqThreads, 1)
       for (int j = 0; j < 8; j++) {
         if (ch * 8 + j >= p.K) break;
         const float2 x = make_float2(v[2 * j], v[2 * j + 1]);
-        __half lv[8];
-        demod(QM, x, lv);
+        __half2 lv[QM / 2];  // (Re, Im) pairs, bit-identical to demod()
+        demod2<QM>(x, lv);
         if (llr_on) {
           if (pair) {
 #pragma unroll
-            for (int qb = 0; qb < QM; qb += 2)
-              reinterpret_cast<__half2 *>(lpu)[qb / 2] = __halves2half2(lv[qb], lv[qb + 1]);
+            for (int h = 0; h < QM / 2; h++) reinterpret_cast<__half2 *>(lpu)[h] = lv[h];
           } else {
 #pragma unroll
-            for (int qb = 0; qb < QM; qb++)
-              if (base + qb < p.row_len32) lpu[qb] = lv[qb];
+            for (int h = 0; h < QM / 2; h++) {
+              if (base + 2 * h < p.row_len32) lpu[2 * h] = __low2half(lv[h]);
+              if (base + 2 * h + 1 < p.row_len32) lpu[2 * h + 1] = __high2half(lv[h]);
+            }
           }
         }
         if (hpu) {
-          uint32_t hb = 0;
-#pragma unroll
-          for (int qb = 0; qb < QM; qb++) hb = (hb << 1) | (__hlt(lv[qb], zero) ? 1u : 0u);
-          hb &= nvm;
+          const uint32_t hb = hard2<QM>(lv) & nvm;
           uint32_t win = 0;
 #pragma unroll
           for (uint32_t k = 0; k < NSUB; k++)

@@ -57,6 +57,38 @@ def test_equalize_tc_vs_oracle(mb, K, M, S, sg, n_sym, Qm):
         assert (bits_g[sure] == bits_r[sure]).all()
 
 
+@pytest.mark.parametrize("Qm", [2, 4, 6, 8])
+def test_equalize_tc_demap_bit_exact(mb, Qm):
+    # The tensor-core equalizer's LLRs are the reference's FP16 demapper
+    # (the oracle's restatement, pinned bit-exact by the golden vectors)
+    # applied to its own equalized symbols x, bit for bit; its hard bits are
+    # those LLRs' signs (l < 0) descrambled by the LFSR sequence.
+    K, M, S, sg, n_sym = 16, 64, 256, 16, 2
+    rng = np.random.default_rng(900 + Qm)
+    G = S // sg
+    W = ((rng.standard_normal((G, M, K)) + 1j * rng.standard_normal((G, M, K))) / np.sqrt(2 * M)).astype(np.complex64)
+    y = ((rng.standard_normal((n_sym, M, S)) + 1j * rng.standard_normal((n_sym, M, S))) / np.sqrt(2)).astype(np.complex64)
+    cb = (S * Qm * 9) // 10 // Qm * Qm
+    zeros, stride = 2 * Qm + 2, cb + 2 * Qm + 6
+    n_valid = min(S * Qm, cb)
+    llr_d = torch.zeros(n_sym, K, stride, dtype=torch.float16, device="cuda")
+    hard_d = torch.zeros(n_sym, K, (n_valid + 7) // 8, dtype=torch.uint8, device="cuda")
+    x_d = torch.zeros(n_sym, K, S, dtype=torch.complex64, device="cuda")
+    mb.Equalize.equalize_tc(dev(W), dev(y), llr_d, sg, Qm, cb, zeros, 1, hard=hard_d, scrambler=mb.Scrambler(),
+                            x=x_d)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    llr_g, hard_g, x_g = llr_d.cpu().numpy(), hard_d.cpu().numpy(), x_d.cpu().numpy()
+    seq = orc.scrambler_seq127()
+    ns = n_valid // Qm  # whole subcarriers inside the code block
+    for l in range(n_sym):
+        ref = orc.demod(Qm, x_g[l, :, :ns]).reshape(K, ns * Qm)
+        got = llr_g[l][:, zeros:zeros + ns * Qm]
+        assert (got.view(np.uint16) == ref.view(np.uint16)).all()
+        bits = (ref < 0).astype(np.uint8) ^ seq[np.arange(ns * Qm) % seq.size][None, :]
+        assert (np.unpackbits(hard_g[l], axis=1)[:, :ns * Qm] == bits).all()
+
+
 @pytest.mark.parametrize("M,K,G", [(256, 32, 7), (64, 16, 5), (128, 64, 3), (200, 24, 4), (8, 4, 2),
                                    (256, 64, 2), (384, 64, 3)])
 def test_zf_mixed_vs_oracle(mb, M, K, G):
