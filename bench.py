@@ -4,8 +4,9 @@
 Workload (one "step" = one uplink slot of one cell): 256 antennas x 32 users,
 4096-point FFT with 3276 data subcarriers, 14 OFDM symbols (2 comb-pilot
 symbols + 12 data symbols), 64-QAM at 25 dB SNR over an 8-tap exponential
-power-delay-profile channel with antenna correlation 0.5; complex float32
-time-domain samples in.  Per slot: pilot FFT + LS estimate, per-group ZF
+power-delay-profile channel with antenna correlation 0.5; int8 time-domain
+IQ samples in by default (the reference's production sample type; --iq picks
+int16, complex float32 or FP16).  Per slot: pilot FFT + LS estimate, per-group ZF
 (Gram, inverse, detector), uplink FFT, equalize + FP16 LLR demod + descrambled
 hard bits.  Inputs are seeded synthetic slots (megastation_b200.datagen).
 
@@ -26,7 +27,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=12, snr_db=25.0, channel="tdl",
-                n_taps=8, tap_decay=2.0, rho=0.5, iq_dtype="int16", seed=2024)
+                n_taps=8, tap_decay=2.0, rho=0.5, iq_dtype="int8", seed=2024)
 # bytes per IQ sample of each input format
 IQ_BYTES = {"c64": 8, "int16": 4, "int8": 2, "f16": 4}
 METRIC = "slots/s"
@@ -270,8 +271,9 @@ def run_reference(args, rank, world):
     """The reference arm.  The reference implements this path only as CUDA
     operators (cuFFT, cuBLAS/cuSOLVER, its SIMT equalizer); where they were
     built from the reference tree (oracle/_ref, kind "reference") they run on
-    this GPU in process.cc's order on the same slot shapes with int16
-    samples (the reference FFT takes integer IQ only).  Otherwise the FP32
+    this GPU in process.cc's order on the same slot shapes and integer
+    samples as --iq (int8 by default; int16 stands in for the float formats,
+    since the reference FFT takes integer IQ only).  Otherwise the FP32
     host C++/OpenMP restatement (kind "port") runs on all host cores.  Rank 0
     only."""
     from megastation_b200 import datagen
