@@ -282,8 +282,8 @@ def run_reference(args, rank, world):
     cfg = datagen.CellConfig(**{**WORKLOAD, "iq_dtype": args.iq})
     from oracle import ref_ops
     cb, zeros, stride = cfg.ldpc()
-    if ref_ops.available():
-        import torch
+    import torch
+    if ref_ops.available() and torch.cuda.is_available():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         # the reference FFT takes integer samples only (fft_op.cu:194-200)
         iq_ref = args.iq if args.iq in ("int8", "int16") else "int16"
