@@ -218,8 +218,8 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
-// 2-D tiled tensor copy global -> shared (box from the tensor map), no
-// multicast; x must be a multiple of 16 bytes / element size
+// 2-D tiled tensor copy global -> shared (box from the tensor map) into
+// this CTA's own shared memory; x must be a multiple of 16 bytes / element size
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int32_t x, int32_t y,
                                             uint64_t *bar) {
   asm volatile(
