@@ -73,9 +73,19 @@ const char *mb_version(void);
 mb_status mb_tables_init(int device);
 
 /* Device error word of the current device: bits set by kernels whose
- * bounded waits gave up (1 = mbarrier wait timeout).  Synchronises the
- * device, copies the word to *out and clears it when clear != 0. */
+ * bounded waits gave up (1 = mbarrier wait timeout), OR-ed with the word of
+ * mb_equalize_tc_noalloc's kernels.  Synchronises the device, copies the
+ * word to *out and clears both when clear != 0. */
 mb_status mb_device_error(int *out, int clear);
+
+/* Self-test of the bounded device wait (no reference counterpart): one
+ * warp waits on a shared-memory mbarrier through the wait the tensor-core
+ * kernels use, giving up after limit_ns (1 .. 1e9) nanoseconds.  With
+ * arm = 0 nothing arrives, the wait runs out and mb_device_error then
+ * reports the timeout bit (1); with arm != 0 the barrier completes and no
+ * bit is set.  Shows, without faulting or hanging the GPU, that an expired
+ * wait ends the kernel with an error the host can read. */
+mb_status mb_selftest_wait(uint64_t limit_ns, int arm, void *stream);
 
 /* Host-side pilot sequence p/|p|^2 of length S (fft/fft_op.cu:176-192 over
  * utils.h:54-95).  out: S host complex values. */
@@ -257,7 +267,12 @@ mb_status mb_equalize_tc(const mb_c32 *W, const mb_c32 *y, uint32_t K,
  * previous call's contents: calls that can overlap on the GPU (different
  * streams, other host threads) race and must be serialised by the caller.
  * Nothing in the scratch needs to start at zero: every byte a call reads was
- * written earlier in the same call. */
+ * written earlier in the same call.  A bounded device wait that gives up
+ * sets bit 1 of an error word that is also fixed in the library (the
+ * library's own word is allocated on first use); mb_device_error reports
+ * and clears it together with that word.  The device addresses looked up
+ * at the first call belong to the device's context: after cudaDeviceReset
+ * this entry point must not be called again in the process. */
 mb_status mb_equalize_tc_noalloc(const mb_c32 *W, const mb_c32 *y, uint32_t K,
                                  uint32_t M, uint32_t S, uint32_t sg,
                                  uint32_t n_sym, uint32_t Qm, uint64_t cb_size,

@@ -113,6 +113,7 @@ def _load():
         "mb_equalize_tc_noalloc": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U64, U64, U64, U32,
                                         VP, VP, VP, VP, VP]),
         "mb_device_error": (ST, [ctypes.POINTER(ctypes.c_int), I32]),
+        "mb_selftest_wait": (ST, [U64, I32, VP]),
         "mb_precode": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U32, VP, VP]),
         "mb_modulate": (ST, [VP, VP, U64, U64, U64, U32, U32, VP, VP]),
         "mb_scramble": (ST, [VP, VP, U64, U64, VP]),

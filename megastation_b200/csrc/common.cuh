@@ -63,6 +63,9 @@ struct DeviceTables {
   uint32_t *lfsr127_bits;  // 127 bits packed LSB-first in 4 words
   int *err;                // device error word (mb_tc error bits)
 };
-const DeviceTables *device_tables();  // for the current device; nullptr on error
+// for the current device, built once per device under a lock (the QAM maps
+// of the modulator are uploaded then too); nullptr on error
+const DeviceTables *device_tables();
+mb_status upload_mod_tables();  // modscr.cu: QAM maps to the current device
 
 }  // namespace mb

@@ -33,6 +33,9 @@ mb_status w_image(const float2 *W, void *img, uint32_t G, uint32_t M, uint32_t K
 // (symbol, subcarrier) columns
 mb_status equalize_tc(const EqParams &p, const void *a_img, const void *y_lp, uint32_t S_pad,
                       uint32_t l0, uint32_t nb, int *err, cudaStream_t st, uint32_t max_cols = 0);
+// error word of mb_equalize_tc_noalloc's kernels on the current device
+// (0 when it has not run there), cleared when clear is set
+mb_status noalloc_error_word(int *bits, bool clear);
 // y [nb][M][S] c32 -> y_lp [nb][re|im][M][S_pad] BF16
 mb_status y_to_lp(const float2 *y, void *y_lp, uint32_t nb, uint32_t M, uint32_t S,
                   uint32_t S_pad, cudaStream_t st);

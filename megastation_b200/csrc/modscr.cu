@@ -1,6 +1,5 @@
 // modscr.cu -- QAM modulation with DM-RS insertion and byte scrambling.
 #include <algorithm>
-#include <atomic>
 #include <math.h>
 
 #include "common.cuh"
@@ -44,13 +43,12 @@ static void host_mod_table(int Qm, float2 *t) {
   }
 }
 
-static mb_status upload_mod_tables() {
-  static float2 h[4][256];
-  static bool built = false;
-  if (!built) {
-    for (int q = 0; q < 4; q++) host_mod_table(2 * (q + 1), h[q]);
-    built = true;
-  }
+// Uploads the QAM maps to the current device.  Called once per device by
+// device_tables() under its lock, so concurrent first calls of mb_modulate
+// cannot race on the upload.
+mb_status upload_mod_tables() {
+  float2 h[4][256];
+  for (int q = 0; q < 4; q++) host_mod_table(2 * (q + 1), h[q]);
   MB_CUDA_TRY(cudaMemcpyToSymbol(c_mod_table, h, sizeof(h)));
   return MB_OK;
 }
@@ -112,18 +110,7 @@ extern "C" mb_status mb_modulate(const uint8_t *in, mb_c32 *out,
   if (pilot_spacing && !pilot_table) return MB_BAD_ARG;
   if (num_ues > 65535) return MB_BAD_SHAPE;
   if (num_carriers == 0 || num_ues == 0) return MB_OK;
-  {
-    // per-device one-time table upload
-    static std::atomic<uint64_t> done{0};
-    int dev = 0;
-    MB_CUDA_TRY(cudaGetDevice(&dev));
-    uint64_t bit = 1ull << (dev & 63);
-    if (!(done.load() & bit)) {
-      mb_status s = upload_mod_tables();
-      if (s != MB_OK) return s;
-      done.fetch_or(bit);
-    }
-  }
+  if (!device_tables()) return MB_CUDA_ERROR;  // the QAM maps are uploaded with the tables
   dim3 grid((unsigned)((num_carriers + 255) / 256), (unsigned)num_ues);
   modulate_kernel<<<grid, 256, 0, as_stream(stream)>>>(
       in, reinterpret_cast<float2 *>(out), in_bytes, num_carriers, num_ues, Qm,

@@ -21,16 +21,43 @@ namespace {
 // the library holds these bytes until the process exits.
 constexpr uint64_t kNoAllocScratchBytes = 32ull << 20;
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+// The error word of this entry point's kernels (bit 1: a bounded mbarrier
+// wait gave up), kept beside the scratch because the library's own error
+// word is allocated on first use.  mb_device_error reports and clears it
+// together with that word.
+static __device__ int g_noalloc_err;
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// with that device current.  In host code the array's name is only a handle
-// for the runtime, not a device address.
+// Device addresses of g_noalloc_scratch and g_noalloc_err per device, looked
+// up once per device with that device current.  In host code the arrays'
+// names are only handles for the runtime, not device addresses.  The cached
+// addresses belong to the device's current context: after cudaDeviceReset
+// they are stale, and this entry point must not be called again in that
+// process (as with every other per-device table of the library).
 std::mutex g_noalloc_mu;
 void *g_noalloc_addr[64];
+int *g_noalloc_err_addr[64];
 
 }  // namespace
 
 using namespace mb;
+
+// Reads (and optionally clears) this entry point's error word on the current
+// device; 0 when the entry point has not run there.
+mb_status mb::noalloc_error_word(int *bits, bool clear) {
+  *bits = 0;
+  int dev = 0;
+  MB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return MB_OK;
+  int *addr = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    addr = g_noalloc_err_addr[dev];
+  }
+  if (!addr) return MB_OK;
+  MB_CUDA_TRY(cudaMemcpy(bits, addr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (clear) MB_CUDA_TRY(cudaMemset(addr, 0, sizeof(int)));
+  return MB_OK;
+}
 
 extern "C" mb_status mb_equalize_tc_noalloc(const mb_c32 *W, const mb_c32 *y, uint32_t K,
                                             uint32_t M, uint32_t S, uint32_t sg,
@@ -59,18 +86,22 @@ extern "C" mb_status mb_equalize_tc_noalloc(const mb_c32 *W, const mb_c32 *y, ui
   MB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return MB_UNSUPPORTED;
   uint8_t *base = nullptr;
+  int *err = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_addr[dev]) {
-      void *addr = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+      void *addr = nullptr, *eaddr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+      if (e == cudaSuccess) e = cudaGetSymbolAddress(&eaddr, g_noalloc_err);
       if (e != cudaSuccess) {
         (void)cudaGetLastError();
         return record_error(e);
       }
+      g_noalloc_err_addr[dev] = reinterpret_cast<int *>(eaddr);
       g_noalloc_addr[dev] = addr;
     }
     base = reinterpret_cast<uint8_t *>(g_noalloc_addr[dev]);
+    err = g_noalloc_err_addr[dev];
   }
   uint8_t *img = base;
   uint8_t *ylp = base + img_bytes;
@@ -88,7 +119,7 @@ extern "C" mb_status mb_equalize_tc_noalloc(const mb_c32 *W, const mb_c32 *y, ui
     for (uint32_t j = 0; j < nc;) {
       uint32_t nb = std::min(nb_max, nc - j);
       while (nb > 1 && !equalize_tc_supported(K, sg, nb)) nb--;
-      s = equalize_tc(p, img, ylp + (uint64_t)j * sym_bytes, S_pad, c0 + j, nb, nullptr, st);
+      s = equalize_tc(p, img, ylp + (uint64_t)j * sym_bytes, S_pad, c0 + j, nb, err, st);
       if (s != MB_OK) return s;
       j += nb;
     }

@@ -8,6 +8,7 @@
 
 #include "common.cuh"
 #include "tc.cuh"
+#include "eq_tc.cuh"
 
 namespace mb {
 
@@ -62,7 +63,7 @@ static mb_status build_tables(DeviceTables &t) {
   MB_CUDA_TRY(cudaMalloc(&t.lfsr127_bits, sizeof(words)));
   MB_CUDA_TRY(cudaMemcpy(t.lfsr127_bits, words, sizeof(words),
                          cudaMemcpyHostToDevice));
-  return MB_OK;
+  return upload_mod_tables();
 }
 
 const DeviceTables *device_tables() {
@@ -171,9 +172,37 @@ mb_status make_tmap_2d_u8_sw128(CUtensorMap *map, const void *base, uint64_t wid
   return r == CUDA_SUCCESS ? MB_OK : MB_BAD_ARG;
 }
 
+// One warp waits on a shared-memory mbarrier of arrival count 1 through the
+// same bounded wait as the tensor-core kernels.  With arm = 0 nothing ever
+// arrives, so the wait runs out after limit_ns and the timeout bit lands in
+// the device error word; with arm != 0 thread 0 arrives first and the wait
+// completes at once.  Nothing else is in flight in the CTA, so giving up is
+// a plain return.
+__global__ void wait_selftest_kernel(uint64_t limit_ns, int arm, int *err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&bar, 1);
+    tc::fence_mbar_init();
+  }
+  __syncwarp();
+  if (arm && threadIdx.x == 0) tc::mbar_arrive(&bar);
+  __syncwarp();
+  const bool ok = tc::mbar_wait(&bar, 0, limit_ns);
+  if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) atomicOr(err, tc::kErrTimeout);
+}
+
 }  // namespace mb
 
 using namespace mb;
+
+extern "C" mb_status mb_selftest_wait(uint64_t limit_ns, int arm, void *stream) {
+  if (limit_ns == 0 || limit_ns > 1000000000ull) return MB_BAD_ARG;
+  const DeviceTables *t = device_tables();
+  if (!t) return MB_CUDA_ERROR;
+  wait_selftest_kernel<<<1, 32, 0, as_stream(stream)>>>(limit_ns, arm, t->err);
+  MB_LAUNCH_CHECK();
+  return MB_OK;
+}
 
 extern "C" const char *mb_status_str(mb_status s) {
   switch (s) {
@@ -208,6 +237,10 @@ extern "C" mb_status mb_device_error(int *out, int clear) {
   MB_CUDA_TRY(cudaDeviceSynchronize());
   MB_CUDA_TRY(cudaMemcpy(out, t->err, sizeof(int), cudaMemcpyDeviceToHost));
   if (clear) MB_CUDA_TRY(cudaMemset(t->err, 0, sizeof(int)));
+  int na = 0;  // the fixed-scratch equalizer keeps its own word
+  const mb_status s = noalloc_error_word(&na, clear != 0);
+  if (s != MB_OK) return s;
+  *out |= na;
   return MB_OK;
 }
 

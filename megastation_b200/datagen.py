@@ -26,7 +26,9 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import ops
+# The generator is plain numpy and imports nothing else from this package, so
+# that a process which must not load the library (a timing run of the
+# reference's own operators) can still build the same seeded slots.
 
 
 @dataclass
@@ -71,8 +73,59 @@ class CellConfig:
     def ldpc(self):
         """(cb_size, zeros, cb_stride): encoded bits, punctured bits and the
         tight row stride of the LLR layout for one code block per symbol."""
-        e, p, _ = ops.ldpc_sizes(self.S, self.Qm, self.code_rate)
+        e, p, _ = ldpc_sizes(self.S, self.Qm, self.code_rate)
         return e, p, e + p
+
+
+# TS 38.212 Table 5.3.2-1 lifting sizes, ascending
+_LIFTING = sorted([2, 4, 8, 16, 32, 64, 128, 256, 3, 6, 12, 24, 48, 96, 192, 384, 5, 10, 20, 40, 80, 160,
+                   320, 7, 14, 28, 56, 112, 224, 9, 18, 36, 72, 144, 288, 11, 22, 44, 88, 176, 352, 13, 26,
+                   52, 104, 208, 15, 30, 60, 120, 240])
+
+
+def ldpc_sizes(S, Qm, code_rate=1.0 / 3.0, base_graph=1, pilot_spacing=0, downlink=False):
+    """(encoded, punctured, decoded) bits of one code block, the sizing of
+    config/config.cc:84-135: the largest lifting size Zc with kb*Zc not above
+    the symbol's uncoded bits (kb = 22 for BG1, 10 for BG2), round(kb/rate)
+    - (kb-2) parity rows, the first 2*Zc systematic bits punctured.  Host
+    arithmetic, the same as the library's mb_ldpc_sizes."""
+    kb = 22 if base_graph == 1 else 10
+    data = S - S // pilot_spacing if (downlink and pilot_spacing) else S
+    uncoded = int(float(data * Qm) * code_rate)
+    z = _LIFTING[-1]
+    for a, b in zip(_LIFTING[:-1], _LIFTING[1:]):
+        if kb * a <= uncoded < kb * b:
+            z = a
+            break
+    rows = int(np.floor(kb / code_rate + 0.5)) - (kb - 2)
+    return (kb - 2 + rows) * z, 2 * z, kb * z
+
+
+def _zc_length(S):
+    """utils.h:56-62: the largest prime <= S from the table ending at 2039,
+    2039 itself when S is larger or nothing matches."""
+    n = 2039
+    sieve = np.ones(n + 1, bool)
+    sieve[:2] = False
+    for d in range(2, int(n ** 0.5) + 1):
+        if sieve[d]:
+            sieve[d * d::d] = False
+    primes = np.nonzero(sieve[:min(S, n) + 1])[0]
+    return 2039 if (len(primes) == 0 or S >= 2039) else int(primes[-1])
+
+
+def pilot_values(S):
+    """The transmitted comb pilot of subcarrier i, p[i] = zc(i mod L) e^{j pi i / 4}
+    (fft/fft_op.cu:176-192 over utils.h:54-95; the receiver's table is
+    p / |p|^2): Zadoff-Chu of length L, the largest prime <= S, root
+    round(2L/31), phases rounded to float as the reference forms them."""
+    L = _zc_length(S)
+    root = np.floor(L * 2.0 / 31.0 + 0.5)
+    i = np.arange(S, dtype=np.int64)
+    m = (i % L).astype(np.float64)
+    th = (-np.pi * root * m * (m + 1) / L).astype(np.float32).astype(np.float64)
+    a = (np.float32(np.pi / 4) * i.astype(np.float32)).astype(np.float64)
+    return np.exp(1j * (th + a)).astype(np.complex64)
 
 
 def mod_table(Qm):
@@ -202,8 +255,7 @@ def make_slot(cfg):
     rng = np.random.default_rng(np.random.Philox(cfg.seed))
     M, K, S, sg, Qm, U, P = cfg.M, cfg.K, cfg.S, cfg.sg, cfg.Qm, cfg.U, cfg.P
     H = _channel(cfg, rng)
-    ps = ops.pilot_sign(S).numpy()
-    pilot_raw = (ps / (np.abs(ps) ** 2)).astype(np.complex64)  # p = ps / |ps|^2
+    pilot_raw = pilot_values(S)
     nbits = S * Qm
     bits = rng.integers(0, 2, (U, K, nbits), dtype=np.uint8)
     seq = scrambling_bits(cfg, nbits)

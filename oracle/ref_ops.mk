@@ -2,7 +2,9 @@
 # the reference tree, in place, with the C shim ref_shim.cu, into
 # _ref/libref_ops.so.  Test infrastructure only; nothing is copied from the
 # reference tree.  Usage: make -f ref_ops.mk REF=<reference tree>
-REF ?= /root/reference
+ifeq ($(REF),)
+$(error REF=<MegaStation tree> is required)
+endif
 OPS := $(REF)/src/operators
 NVCC ?= nvcc
 SITE := $(shell python -c "import site; print(site.getsitepackages()[0])" 2>/dev/null)

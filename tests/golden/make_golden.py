@@ -7,7 +7,8 @@ mounted.  The files are the reference's own fixtures, byte for byte:
   test/beamform/{csi_in,csi_out,precoder}.data   (test/beamform/test_beamform.cc:19-95)
   test/sgemv/{csi,bsVec,equalize,prec,ueVec,precoded}.data (test/sgemv/test_sgemv.cc:32-196)
 
-Usage: python tests/golden/make_golden.py [/path/to/MegaStation]
+Usage: python tests/golden/make_golden.py /path/to/MegaStation
+(or with the tree's location in the MEGASTATION_REF environment variable)
 """
 import os
 import shutil
@@ -32,4 +33,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MEGASTATION_REF")
+    if not root:
+        sys.exit("usage: make_golden.py <MegaStation tree> (or set MEGASTATION_REF)")
+    main(root)

@@ -69,3 +69,33 @@ def test_cells_autotune_keeps_results(cells_data):
     s.synchronize()
     for c in range(len(cfgs)):
         assert torch.equal(llr[c], ref[c][0]) and torch.equal(hard[c], ref[c][1]), c
+
+
+@pytest.mark.parametrize("n,seed,precision", [(32, 3, "mixed"), (6, 11, "fp32")],
+                         ids=["bench-32-cells-mixed", "6-cells-fp32"])
+def test_cells_vs_oracle(n, seed, precision):
+    """Every cell of a batched slot against the FP64 oracle run on that cell
+    alone (pilot FFT, ZF, FFT, equalize, descrambled hard bits); the 32-cell
+    set is the batched-cells workload of the bench (seed 3)."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import megastation_b200 as mb
+    from megastation_b200 import cells, datagen
+
+    from slot_oracle import check_uplink, oracle_uplink
+    cfgs = datagen.make_cells(n=n, seed=seed)
+    data = [datagen.make_slot(c) for c in cfgs]
+    iqs = [torch.from_numpy(d["iq"]).cuda() for d in data]
+    cs = cells.Cells(cfgs, precision=precision)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        cs(iqs, stream=s)
+        llr, hard = cs(iqs, stream=s)
+    s.synchronize()
+    assert mb.ops.device_error() == 0
+    for c, (cfg, d) in enumerate(zip(cfgs, data)):
+        # 0: solved, 2: solved on the FP64 fallback (cells with as many users
+        # as antennas have ill-conditioned groups); never 1 (not PD)
+        assert np.isin(cs.status[c].cpu().numpy(), (0, 2)).all(), c
+        _, ref = oracle_uplink(cfg, d)
+        check_uplink(cfg, ref, llr[c].cpu().numpy(), hard[c].cpu().numpy(), precision, f"cell {c}")

@@ -69,3 +69,26 @@ def test_pipe_wait_bounds_and_timer(mb):
     assert 0.0 < ms < 10000.0
     with pytest.raises(ValueError):
         pipe.submit(iq[:1].contiguous(), l, h)  # wrong size
+
+
+def test_pipe_vs_oracle(mb):
+    """Slots through the host-buffer pipeline against the FP64 oracle (not
+    only against the direct slot): the bench's 256x32 int8 shape, three
+    distinct slots in flight through a depth-2 ring."""
+    from megastation_b200 import datagen, slot
+
+    from slot_oracle import check_uplink, oracle_uplink
+    base = dict(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=12, snr_db=25.0, channel="tdl", rho=0.5,
+                n_taps=8, tap_decay=2.0, iq_dtype="int8")
+    cfgs = [datagen.CellConfig(**{**base, "seed": 40 + r}) for r in range(3)]
+    data = [datagen.make_slot(c) for c in cfgs]
+    pipe = slot.SlotPipeline(cfgs[0], precision="mixed", sym_batch=12, depth=2)
+    iqs = [torch.from_numpy(d["iq"]).pin_memory() for d in data]
+    outs = [pipe.host_outputs() for _ in data]
+    tickets = [pipe.submit(iq, l, h) for iq, (l, h) in zip(iqs, outs)]
+    for t in tickets:
+        assert pipe.wait(t, timeout_ms=60000)
+    assert mb.ops.device_error() == 0
+    for (l, h), cfg, d in zip(outs, cfgs, data):
+        _, ref = oracle_uplink(cfg, d)
+        check_uplink(cfg, ref, l.numpy(), h.numpy(), "mixed", f"seed {cfg.seed}")
