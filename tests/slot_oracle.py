@@ -36,10 +36,21 @@ def oracle_uplink(cfg, d):
 TOL = {"fp32": dict(sure=0.5, abs=0.25, rel=5e-3), "mixed": dict(sure=4.0, abs=1.0, rel=0.02)}
 
 
+def tolerance(cfg, precision):
+    """TOL of the path, widened for the mixed path on cells with fewer than
+    four antennas per user: the BF16 rounding of W and y in x = W y is
+    amplified by the cancellation in that sum, which grows with the
+    channel's condition (M / K = 1 or 2 in the batched-cells workload)."""
+    t = dict(TOL[precision])
+    if precision == "mixed" and cfg.M < 4 * cfg.K:
+        t.update(sure=10.0, rel=0.06)
+    return t
+
+
 def check_uplink(cfg, ref, llr, hard, precision, what=""):
     """llr [U][K][stride] (float16 numpy), hard [U][K][hrow] against the
     oracle's per-symbol outputs `ref`."""
-    t = TOL[precision]
+    t = tolerance(cfg, precision)
     cb, zeros, _ = cfg.ldpc()
     n_valid = min(cb, cfg.S * cfg.Qm)
     for l in range(cfg.U):
