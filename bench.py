@@ -9,6 +9,10 @@ IQ samples in by default (the reference's production sample type; --iq picks
 int16, complex float32 or FP16).  Per slot: pilot FFT + LS estimate, per-group ZF
 (Gram, inverse, detector), uplink FFT, equalize + FP16 LLR demod + descrambled
 hard bits.  Inputs are seeded synthetic slots (megastation_b200.datagen).
+The mixed ZF starts its two Newton-Schulz steps from the learned polynomial
+initial iterate (its network trained in the run by the library's kernels;
+--init exact for the Gauss-Jordan inverse), so the headline is the mixed +
+learned path of the metric, with the plain FP32 path timed beside it.
 
 Lines printed (rank 0): one JSON object.  Multi-GPU (torchrun): replicas, one
 independent slot stream per GPU (the path has no exchange step).
@@ -54,6 +58,12 @@ def parse():
     ap.add_argument("--no-evm", action="store_true")
     ap.add_argument("--ns-iters", type=int, default=2, help="Newton-Schulz steps of the mixed ZF (config 2 names 2)")
     ap.add_argument("--sym-batch", type=int, default=12)
+    ap.add_argument("--init", default="learned", choices=["learned", "exact"],
+                    help="initial iterate of the mixed ZF's Newton-Schulz steps: the learned polynomial "
+                         "(network trained in the run by the library's kernels) or the exact inverse")
+    ap.add_argument("--init-realisations", type=int, default=2440,
+                    help="channel realisations per training shape (x 205 groups x 2 shapes)")
+    ap.add_argument("--init-steps", type=int, default=3000, help="Adam steps of the initial-iterate network")
     ap.add_argument("--iq", default="int8", choices=["int8", "int16", "c64", "f16"],
                     help="sample format of the cell256x32 workload: int8 is the reference's production "
                          "QuanT (utils/types.h:26), int16 the other integer format its FFT takes")
@@ -398,11 +408,44 @@ def repeat_windows(step, stream, args, ms_first, dist, world):
             "us_per_slot_median": float(1e3 * np.median(w_ms.numpy()) / args.steps)}
 
 
-def time_slots(slot_mod, cfg, precision, sym_batch, iq_dev, llr, hard, stream, steps, warmup, dist):
+def train_zf_init(args):
+    """The learned initial iterate's network (6 -> 64 -> 64 -> 4), trained on
+    the GPU by the library's own forward, backward and Adam kernels on the
+    quadratic residual targets of every group of seeded channel
+    realisations of 256 x 32 and 128 x 16 cells (8-tap channel, correlation
+    0.3-0.7, SNR 18-30 dB); returns the network and a training record with
+    its held-out residual against the fixed Neumann polynomial."""
+    import torch
+    from megastation_b200 import learned
+    t0 = time.perf_counter()
+    data = learned.zf_init_training_set([(256, 32), (128, 16)], n_real=args.init_realisations, seed=1)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    net = learned.make_zf_init_net(width=64, seed=3)
+    t0 = time.perf_counter()
+    hist = learned.train(net, data, steps=args.init_steps, batch=4096, lr=2e-3, seed=5, log_every=1000)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    held = learned.zf_init_training_set([(256, 32)], n_real=20, seed=77, rho=(0.5, 0.5), tap_decay=(2.0, 2.0),
+                                        snr_db=(25.0, 25.0))
+    r_l, r_n = learned.poly_residual(net, held)
+    info = {"network": "6 -> 64 -> 64 -> 4, ReLU, BF16 weights, FP32 accumulation",
+            "samples": int(data[0].shape[0]), "realisations": 2 * args.init_realisations,
+            "steps": args.init_steps, "batch": 4096, "data_s": t_data, "train_s": t_train,
+            "loss_history": hist,
+            "heldout_residual": {"learned": r_l, "neumann": r_n,
+                                 "note": "mean ||I - Gn p(Gn)||_F^2 / K on 4100 groups of the bench channel"}}
+    del data
+    return net, info
+
+
+def time_slots(slot_mod, cfg, precision, sym_batch, iq_dev, llr, hard, stream, steps, warmup, dist, net=None):
     """K graph-replayed slots on device-resident inputs; returns ms."""
     import torch
     R = len(iq_dev)
     run = slot_mod.UplinkSlot(cfg, precision=precision, sym_batch=sym_batch, use_graph=True)
+    if net is not None:
+        run.set_zf_init(net)
     with torch.cuda.stream(stream):
         for k in range(max(warmup, 2 * R)):
             run(iq_dev[k % R], llr[k % 2], hard[k % 2], stream=stream)
@@ -418,7 +461,7 @@ def time_slots(slot_mod, cfg, precision, sym_batch, iq_dev, llr, hard, stream, s
     return e0.elapsed_time(e1)
 
 
-def time_in_flight(slot_mod, cfg, args, iq_dev, stride, hrow, dist, D=2):
+def time_in_flight(slot_mod, cfg, args, iq_dev, stride, hrow, dist, D=2, net=None):
     """The same slots with D of them in flight: D slot runners, each a
     captured graph on its own stream, taking every D-th slot; reported beside
     the headline (one slot at a time), not instead of it."""
@@ -427,6 +470,9 @@ def time_in_flight(slot_mod, cfg, args, iq_dev, stride, hrow, dist, D=2):
     streams = [torch.cuda.Stream() for _ in range(D)]
     runs = [slot_mod.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=True,
                                 ns_iters=args.ns_iters) for _ in range(D)]
+    if net is not None:
+        for r in runs:
+            r.set_zf_init(net)
     llr = [torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda") for _ in range(2 * D)]
     hard = [torch.zeros(cfg.U, cfg.K, hrow, dtype=torch.uint8, device="cuda") for _ in range(2 * D)]
 
@@ -456,7 +502,7 @@ def time_in_flight(slot_mod, cfg, args, iq_dev, stride, hrow, dist, D=2):
             "unit": UNIT, "us_per_slot": 1e3 * ms / args.steps}
 
 
-def evm_report(cfg, d, sym_batch, ns_iters=2):
+def evm_report(cfg, d, sym_batch, ns_iters=2, net=None):
     """EVM (dB) of the equalized symbols against the transmitted ones for the
     plain FP32 path, the mixed path and an FP64-ZF variant, on one slot.  The
     mixed row follows the mixed slot's arithmetic: the mixed-precision pilot
@@ -466,11 +512,14 @@ def evm_report(cfg, d, sym_batch, ns_iters=2):
     iq = torch.from_numpy(d["iq"]).cuda()
     cb, zeros, stride = cfg.ldpc()
     out = {}
-    for name, prec in (("fp64_zf", 2), ("plain_fp32", 0), ("mixed", 1)):
+    rows = [("fp64_zf", 2, None), ("plain_fp32", 0, None), ("mixed", 1, net)]
+    if net is not None:
+        rows.append(("mixed_exact_init", 1, None))
+    for name, prec, nt in rows:
         csi = torch.zeros(cfg.G, cfg.M, cfg.K, dtype=torch.complex64, device="cuda")
         pf = mb.PilotFFT(cfg.start, cfg.N, cfg.S, cfg.M, cfg.K, cfg.sg)
         (pf.mixed if prec == 1 else pf)(iq[:cfg.P], csi)
-        mb.Beamform(cfg.M, cfg.K, cfg.G, precision=prec, ns_iters=ns_iters).beamform_uplink(
+        mb.Beamform(cfg.M, cfg.K, cfg.G, precision=prec, ns_iters=ns_iters, init_net=nt).beamform_uplink(
             csi, S=cfg.S, sc_group=cfg.sg)
         uf = mb.UplinkFFT(cfg.start, cfg.N, cfg.S, cfg.M)
         if prec == 1:
@@ -494,7 +543,7 @@ def evm_report(cfg, d, sym_batch, ns_iters=2):
     return out
 
 
-def hard_bits_report(cfg, d, sym_batch, ns_iters=2, tol=4.0):
+def hard_bits_report(cfg, d, sym_batch, ns_iters=2, tol=4.0, net=None):
     """The mixed slot's descrambled hard bits against the plain FP32 slot's
     on the same samples (both through the slot runner the bench times): the
     number of bits that differ where the plain path's |LLR| > tol, the total
@@ -508,6 +557,8 @@ def hard_bits_report(cfg, d, sym_batch, ns_iters=2, tol=4.0):
     out = {}
     for name in ("fp32", "mixed"):
         run = slot.UplinkSlot(cfg, precision=name, sym_batch=sym_batch, ns_iters=ns_iters)
+        if name == "mixed" and net is not None:
+            run.set_zf_init(net)
         llr, hard = run(iq)
         torch.cuda.synchronize()
         bits = np.unpackbits(hard.cpu().numpy(), axis=-1)[..., :n_valid]
@@ -536,6 +587,8 @@ def workload_config(cfg, args, R=None):
             "M": cfg.M, "K": cfg.K, "N": cfg.N, "S": cfg.S, "sg": cfg.sg, "Qm": cfg.Qm, "P": cfg.P,
             "U": cfg.U, "iq_dtype": cfg.iq_dtype, "precision": args.precision, "sym_batch": args.sym_batch,
             "ns_iters": args.ns_iters,
+            "zf_init": ("learned polynomial (network trained in the run), exact inverse as fallback"
+                        if args.precision == "mixed" and args.init == "learned" else "exact inverse"),
             "l2": f"inputs {cfg.symbols * cfg.M * cfg.N * IQ_BYTES[cfg.iq_dtype] / 1e6:.1f} MB per slot, {R} "
                   "slots rotated (larger than the 126 MB L2)",
             "seed": cfg.seed}
@@ -852,8 +905,13 @@ def main():
     iq_host = torch.from_numpy(d["iq"]).pin_memory()
     iq_dev = [iq_host.cuda() for _ in range(R)]
     stream = torch.cuda.Stream()
+    net, init_info = None, None
+    if args.precision == "mixed" and args.init == "learned":
+        net, init_info = train_zf_init(args)
     run = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=True,
                           ns_iters=args.ns_iters)
+    if net is not None:
+        run.set_zf_init(net)
     llr = [torch.zeros(cfg.U, cfg.K, stride, dtype=torch.float16, device="cuda") for _ in range(2)]
     hard = [torch.zeros(cfg.U, cfg.K, hrow, dtype=torch.uint8, device="cuda") for _ in range(2)]
 
@@ -892,6 +950,16 @@ def main():
     # cover all of them
     repeat = repeat_windows(step, stream, args, ms, dist, world)
     clk = clocks.stop()
+    # groups the last timed slot solved from the learned iterate (status 3)
+    st_last = run.status.cpu().numpy()
+    if init_info is not None:
+        init_info["groups_from_learned_iterate"] = f"{int((st_last == 3).sum())} of {st_last.size}"
+    exact = None
+    if net is not None:
+        ems_x = max_over_ranks(time_slots(slot, cfg, "mixed", args.sym_batch, iq_dev, llr, hard, stream,
+                                          args.steps, args.warmup, dist), dist)
+        exact = {"value": job_value(world, args.steps, ems_x), "unit": UNIT, "us_per_slot": 1e3 * ems_x / args.steps,
+                 "note": "the same mixed slot with the exact (Gauss-Jordan) initial iterate"}
     plain = None
     if args.precision == "mixed" and not args.no_plain:
         pms = time_slots(slot, cfg, "fp32", args.sym_batch, iq_dev, llr, hard, stream, args.steps,
@@ -900,15 +968,17 @@ def main():
         pv = job_value(world, args.steps, pms)
         plain = {"value": pv, "unit": UNIT, "us_per_slot": 1e3 * pms / args.steps,
                  "speedup_mixed_over_plain": value / pv}
-    evm = None if args.no_evm or rank != 0 else evm_report(cfg, d, args.sym_batch, args.ns_iters)
-    hb = None if args.no_evm or rank != 0 else hard_bits_report(cfg, d, args.sym_batch, args.ns_iters)
-    inflight = None if args.no_inflight else time_in_flight(slot, cfg, args, iq_dev, stride, hrow, dist)
+    evm = None if args.no_evm or rank != 0 else evm_report(cfg, d, args.sym_batch, args.ns_iters, net=net)
+    hb = None if args.no_evm or rank != 0 else hard_bits_report(cfg, d, args.sym_batch, args.ns_iters, net=net)
+    inflight = None if args.no_inflight else time_in_flight(slot, cfg, args, iq_dev, stride, hrow, dist, net=net)
     launches_per_slot = slot_launches(cfg, args.sym_batch, args.precision == "mixed")
 
     # ---- roofline pass: the same slots with every kernel alone on the slot
     # stream (timing mode serialises the side-stream FFT) and CUDA events at
     # the stage boundaries
     run_t = slot.UplinkSlot(cfg, precision=args.precision, sym_batch=args.sym_batch, use_graph=False)
+    if net is not None:
+        run_t.set_zf_init(net)
     with torch.cuda.stream(stream):
         for k in range(3):
             run_t(iq_dev[k % R], llr[0], hard[0], stream=stream)
@@ -930,6 +1000,8 @@ def main():
     if not args.no_e2e:
         pipe = slot.SlotPipeline(cfg, precision=args.precision, sym_batch=args.sym_batch, depth=2,
                                  ns_iters=args.ns_iters)
+        if net is not None:
+            pipe.set_zf_init(net)
         outs = [pipe.host_outputs() for _ in range(2)]
         for k in range(4):
             t = pipe.submit(iq_host, *outs[k % 2])
@@ -962,7 +1034,8 @@ def main():
             "data": "synthetic (seeded generator, megastation_b200.datagen)",
             "config": workload_config(cfg, args), "clocks": clk, "e2e": e2e,
             "gpu_launches": launches_per_slot * args.steps, "roofline": roof, "cpu_baseline": cpu,
-            "plain_fp32": plain, "evm_db": evm, "hard_bits_vs_plain": hb, "repeat": repeat,
+            "plain_fp32": plain, "mixed_exact_init": exact, "zf_init": init_info, "evm_db": evm,
+            "hard_bits_vs_plain": hb, "repeat": repeat,
             "in_flight": inflight,
             "parallelism": f"replicas x{world}"}
     print(json.dumps(line), flush=True)

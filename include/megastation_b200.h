@@ -60,6 +60,8 @@ typedef struct {
   float re, im;
 } mb_c32;
 
+typedef struct mb_mlp mb_mlp; /* the learned initialiser's network (below) */
+
 const char *mb_status_str(mb_status s);
 /* Version string of this library build. */
 const char *mb_version(void);
@@ -160,6 +162,16 @@ mb_status mb_fft_pilot_mixed(mb_fft *fft, const void *iq, int iq_dtype,
 mb_status mb_ifft_downlink(mb_fft *fft, const mb_c32 *in, uint32_t n_sym,
                            void *out, int out_dtype, void *stream);
 
+/* Mixed-precision inverse FFT (no reference counterpart; the transform and
+ * quantiser of mb_ifft_downlink): in [n_sym][M][N] pairs of in_dtype
+ * (MB_IQ_C32 or MB_IQ_F16), out [n_sym][M][N] pairs of out_dtype.  For
+ * N = 4096, 16-byte aligned buffers and int16, int8 or FP16 outputs the
+ * butterflies run on the tensor cores (FP16 operands scaled per row by a
+ * power of two, FP32 accumulation); otherwise mb_ifft_downlink (c32 input
+ * only: MB_UNSUPPORTED for FP16 input then). */
+mb_status mb_ifft_downlink_mixed(mb_fft *fft, const void *in, int in_dtype, uint32_t n_sym, void *out,
+                                 int out_dtype, void *stream);
+
 /* ------------------------------------------------------- zero forcing --- */
 /* Replaces Beamform (beamform/beamform.h:27-84). */
 typedef enum {
@@ -177,7 +189,10 @@ typedef struct {
   uint32_t precision;     /* mb_zf_precision */
   uint32_t ns_iters;      /* Newton-Schulz refinements (MIXED), e.g. 2 */
   float cond_threshold;   /* FP64 fallback above this estimate, e.g. 1e4 */
-  uint32_t reserved;
+  uint32_t init;          /* MIXED initial iterate: 0 = exact inverse (FP32
+                             Gauss-Jordan); 1 = learned polynomial
+                             (mb_zf_set_init_net), exact inverse where the
+                             learned iterate is not accepted */
 } mb_zf_opts;
 
 typedef struct mb_zf mb_zf;
@@ -197,6 +212,29 @@ mb_status mb_zf_uplink(mb_zf *zf, mb_c32 *csi, uint32_t groups, uint32_t S,
                        uint32_t sc_group, const mb_zf_opts *opts,
                        int32_t *group_status, float *group_cond,
                        void *stream);
+
+/* Learned initial iterate of the mixed ZF (no reference counterpart): the
+ * network net (an mb_mlp with 6 inputs, width <= 256 and 4 outputs; not
+ * owned, read at every launch, so later training takes effect) maps six
+ * scale-free spectral features of a group's Gram G to the coefficients a of
+ * X0 = (a0 I + a1 Gn + a2 Gn^2 + a3 Gn^3) / tau, Gn = G / tau,
+ * tau = tr(G) / K; the features, with t_k = tr(Gn^k) / K: t2 - 1,
+ * t3 - 3 t2 + 2, t4 - 4 t3 + 6 t2 - 3, min and max of diag(Gn) minus 1,
+ * K / M.  ns_iters Newton-Schulz steps follow (at most two more while
+ * 0.04 < ||I - G X||_F < 0.3); a group whose last residual before the final
+ * step exceeds 0.04 is solved by the exact inverse instead.  Used when
+ * mb_zf_opts.init = 1; group_status then reports 3 for groups solved from
+ * the learned iterate.  net NULL clears it. */
+mb_status mb_zf_set_init_net(mb_zf *zf, const mb_mlp *net);
+
+/* Training data of that network (no reference counterpart): for each group
+ * g of csi [G][M][K] (K <= 64), in FP64, features [G][6] as above and the
+ * quadratic form of the normalised squared residual,
+ * ||I - Gn p_a(Gn)||_F^2 / K = a^T A a - 2 b^T a + 1 with A [G][4][4],
+ * A_ij = t_(i+j+2), and b [G][4], b_i = t_(i+1) (device FP32 outputs; the
+ * mb_mlp_loss_grad loss with c = 1). */
+mb_status mb_zf_init_targets(const mb_c32 *csi, uint32_t groups, uint32_t M, uint32_t K,
+                             float *features, float *A, float *b, void *stream);
 
 /* Beamform::beamform_downlink (beamform.cu:154-168, beam_utils.cuh:40-80):
  * P[g][u][b] = W[g][b][u] / max_{b,u} |W[g][b][u]|. */
@@ -291,6 +329,19 @@ mb_status mb_precode(const mb_c32 *P, const mb_c32 *s, uint32_t M,
                      uint32_t start, uint32_t n_sym, mb_c32 *out,
                      void *stream);
 
+/* Mixed-precision precode on the tensor cores (no reference counterpart;
+ * the contract of mb_precode): z [n_sym][M][N] FP16 (re, im) pairs at the
+ * data bins (s + start + N/2) mod N; the guard bins are left as they are
+ * (zero them once).  BF16 operands, FP32 accumulation (tcgen05.mma): a CTA
+ * per subcarrier group, 128 antennas and up to 128 (symbol, subcarrier)
+ * columns.  The caller provides a device scratch buffer of
+ * mb_precode_tc_scratch bytes for the BF16 precoder images (built from P
+ * in the call).  Requires K <= 64. */
+mb_status mb_precode_tc_scratch(uint32_t M, uint32_t K, uint32_t S, uint32_t sg, uint64_t *img_bytes);
+mb_status mb_precode_tc(const mb_c32 *P, const mb_c32 *s, uint32_t M, uint32_t K, uint32_t S,
+                        uint32_t sg, uint32_t N, uint32_t start, uint32_t n_sym, void *z,
+                        void *scratch_img, void *stream);
+
 /* -------------------------------------------------- modulate / scramble -- */
 /* Modulation::modulate (modulation/modulation.cu:115-128,
  * modulation_kernel.cuh:37-68): bits of user u (in_bytes per user, LSB
@@ -368,6 +419,9 @@ mb_status mb_pipe_io_bytes(const mb_pipe *pipe, uint64_t *iq_bytes,
 mb_status mb_pipe_submit(mb_pipe *pipe, const void *iq_host, uint16_t *llr_host,
                          uint8_t *hard_host, uint64_t *ticket);
 mb_status mb_pipe_wait(mb_pipe *pipe, uint64_t ticket, uint32_t timeout_ms);
+/* The pipeline's slots take the mixed ZF's learned initial iterate
+ * (mb_slot_set_zf_init); waits for the slots in flight first. */
+mb_status mb_pipe_set_zf_init(mb_pipe *pipe, const mb_mlp *net);
 /* Device timer: after mb_pipe_timer_start, the next submitted slot records
  * a start event before its sample copy and every slot after it an end
  * event after its result copies; mb_pipe_timer_ms waits for the last end
@@ -385,6 +439,11 @@ mb_status mb_pipe_timer_ms(mb_pipe *pipe, double *ms);
  * [7] recorded calls; then clears the record. */
 mb_status mb_slot_timing(mb_slot *slot, uint32_t max_calls);
 mb_status mb_slot_stage_ms(mb_slot *slot, double *out8);
+
+/* The mixed-precision slot's ZF from the learned initial iterate of
+ * mb_zf_set_init_net (net an mb_mlp of that shape, not owned; NULL: the
+ * exact inverse).  Captured slot graphs are dropped and captured again. */
+mb_status mb_slot_set_zf_init(mb_slot *slot, const mb_mlp *net);
 
 /* Device views of the slot's internal buffers (for inspection and tests):
  * CSI/W [G][M][K], precoder [G][K][M].  In the mixed-precision path without
@@ -432,7 +491,6 @@ mb_status mb_cells_set_tuning(mb_cells *cells, const uint32_t *sym_batch,
  * averaged over the batch.  Parameters are flat FP32: W1 [n_in][width], b1,
  * W2 [width][width], b2, W3 [width][n_out], b3.  All x / y / A / b / c /
  * loss pointers are device memory; params and grads copies are host. */
-typedef struct mb_mlp mb_mlp;
 mb_status mb_mlp_create(uint32_t n_in, uint32_t width, uint32_t n_out, uint32_t max_batch,
                         uint64_t seed, mb_mlp **out);
 mb_status mb_mlp_destroy(mb_mlp *mlp);

@@ -53,7 +53,7 @@ class MbFftDesc(ctypes.Structure):
 
 class MbZfOpts(ctypes.Structure):
     _fields_ = [("precision", U32), ("ns_iters", U32), ("cond_threshold", ctypes.c_float),
-                ("reserved", U32)]
+                ("init", U32)]
 
 
 class MbCellDesc(ctypes.Structure):
@@ -90,6 +90,7 @@ def _load():
         "mb_pipe_io_bytes": (ST, [VP, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64)]),
         "mb_pipe_submit": (ST, [VP, VP, VP, VP, ctypes.POINTER(U64)]),
         "mb_pipe_wait": (ST, [VP, U64, U32]),
+        "mb_pipe_set_zf_init": (ST, [VP, VP]),
         "mb_pipe_timer_start": (ST, [VP]),
         "mb_pipe_timer_ms": (ST, [VP, ctypes.POINTER(ctypes.c_double)]),
         "mb_fft_create": (ST, [ctypes.POINTER(MbFftDesc), ctypes.POINTER(VP)]),
@@ -103,6 +104,9 @@ def _load():
         "mb_zf_destroy": (ST, [VP]),
         "mb_zf_uplink": (ST, [VP, VP, U32, U32, U32, ctypes.POINTER(MbZfOpts), VP, VP, VP]),
         "mb_zf_precoder": (ST, [VP, VP, U32, U32, U32, VP]),
+        "mb_zf_set_init_net": (ST, [VP, VP]),
+        "mb_zf_init_targets": (ST, [VP, U32, U32, U32, VP, VP, VP, VP]),
+        "mb_slot_set_zf_init": (ST, [VP, VP]),
         "mb_scrambler_create": (ST, [I32, U32, U32, U64, ctypes.POINTER(VP)]),
         "mb_scrambler_destroy": (ST, [VP]),
         "mb_equalize": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U64, U64, U64, U32,
@@ -115,6 +119,9 @@ def _load():
         "mb_device_error": (ST, [ctypes.POINTER(ctypes.c_int), I32]),
         "mb_selftest_wait": (ST, [U64, I32, VP]),
         "mb_precode": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U32, VP, VP]),
+        "mb_precode_tc_scratch": (ST, [U32, U32, U32, U32, ctypes.POINTER(U64)]),
+        "mb_precode_tc": (ST, [VP, VP, U32, U32, U32, U32, U32, U32, U32, VP, VP, VP]),
+        "mb_ifft_downlink_mixed": (ST, [VP, VP, I32, U32, VP, I32, VP]),
         "mb_modulate": (ST, [VP, VP, U64, U64, U64, U32, U32, VP, VP]),
         "mb_scramble": (ST, [VP, VP, U64, U64, VP]),
         "mb_slot_create": (ST, [ctypes.POINTER(MbCellDesc), ctypes.POINTER(VP)]),

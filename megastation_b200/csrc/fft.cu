@@ -592,6 +592,29 @@ mb_status mb::fft_pilot_fill(mb_fft *f, const void *iq, int iq_dtype, uint32_t n
   return launch_fft<kPilot>(f->logn, p, st);
 }
 
+bool mb::fft_ifft_tc_ok(mb_fft *f, const void *in, int in_dtype, const void *out, int out_dtype) {
+  return f && fft_tc_inverse_supported(f->tc, in, in_dtype, out, out_dtype);
+}
+
+mb_status mb::fft_tc_inverse_slot(mb_fft *f, const void *in, uint32_t n_sym, void *out, int out_dtype,
+                                  cudaStream_t st) {
+  if (!fft_ifft_tc_ok(f, in, MB_IQ_F16, out, out_dtype)) return MB_BAD_ARG;
+  const DeviceTables *tab = device_tables();
+  return fft_tc_inverse(f->tc, in, MB_IQ_F16, n_sym * f->d.bs_num, out, out_dtype, tab ? tab->err : nullptr, st);
+}
+
+extern "C" mb_status mb_ifft_downlink_mixed(mb_fft *f, const void *in, int in_dtype, uint32_t n_sym, void *out,
+                                            int out_dtype, void *stream) {
+  if (!f || !in || !out || !dtype_ok(in_dtype) || !dtype_ok(out_dtype)) return MB_BAD_ARG;
+  if (fft_tc_inverse_supported(f->tc, in, in_dtype, out, out_dtype)) {
+    const DeviceTables *tab = device_tables();
+    return fft_tc_inverse(f->tc, in, in_dtype, n_sym * f->d.bs_num, out, out_dtype, tab ? tab->err : nullptr,
+                          as_stream(stream));
+  }
+  if (in_dtype != MB_IQ_C32) return MB_UNSUPPORTED;
+  return mb_ifft_downlink(f, reinterpret_cast<const mb_c32 *>(in), n_sym, out, out_dtype, stream);
+}
+
 extern "C" mb_status mb_ifft_downlink(mb_fft *f, const mb_c32 *in,
                                       uint32_t n_sym, void *out, int out_dtype,
                                       void *stream) {

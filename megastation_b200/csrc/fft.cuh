@@ -45,4 +45,17 @@ mb_status fft_tc_slot(const FftTcPlan *plan, const void *iq, int iq_dtype, uint3
                       uint32_t S, uint32_t K, uint32_t sg, uint32_t tail_rem, const float2 *pilot, float2 *csi,
                       void *y_lp, uint32_t S_pad, int *err, cudaStream_t st);
 
+// inverse FFT on the tensor cores (N = 4096): rows of N spectrum samples
+// (c32 or FP16 pairs) -> int16 / int8 quantised or FP16 time samples as
+// mb_ifft_downlink (FP16 operands, FP32 accumulation)
+bool fft_tc_inverse_supported(const FftTcPlan *plan, const void *in, int in_dtype, const void *out, int out_dtype);
+mb_status fft_tc_inverse(const FftTcPlan *plan, const void *in, int in_dtype, uint32_t rows, void *out,
+                         int out_dtype, int *err, cudaStream_t st);
+// the same through an FFT handle: true when the handle's tensor-core plan
+// takes these buffers
+bool fft_ifft_tc_ok(mb_fft *f, const void *in, int in_dtype, const void *out, int out_dtype);
+// n_sym symbols of FP16 spectra [n_sym][M][N] through the handle's
+// tensor-core inverse FFT (fft_ifft_tc_ok must hold)
+mb_status fft_tc_inverse_slot(mb_fft *f, const void *in, uint32_t n_sym, void *out, int out_dtype, cudaStream_t st);
+
 }  // namespace mb

@@ -89,6 +89,16 @@ struct FtParams {
   uint32_t units;       // ceil(rows / 2)
   uint32_t upc;         // units per CTA
   int *err;
+  // inverse mode (DownlinkIFFT): every row is one [N] spectrum in bin
+  // order; the unnormalised inverse FFT is conj(FFT(conj(z))), so the
+  // conversion negates the imaginary parts, the GEMMs and twiddles are the
+  // forward ones, and the store negates them back, scales by out_scale / N
+  // and writes all N samples interleaved (int16 / int8 quantised as
+  // ifft_callback.cuh:37-52, or FP16)
+  uint32_t inverse;
+  int out_dtype;
+  float out_scale;      // (max + 1) / N for integer outputs, 1 / N for FP16
+  void *tout;           // [rows][N] pairs of out_dtype
 };
 
 template <int DT>
@@ -320,6 +330,18 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       // S rounded up to 8 go out by bulk copy (within the row pitch)
       auto issue_stores = [&](uint32_t i) {
         const uint32_t u = unit_of(i);
+        if (p.inverse) {
+          // each staged row holds the N output samples in time order
+          const uint32_t ob = p.out_dtype == MB_IQ_I8 ? 2 : 4;
+          for (uint32_t r = 0; r < 2; r++) {
+            const uint32_t row = 2 * u + r;
+            if (row >= p.rows) break;
+            bulk_s2g(reinterpret_cast<uint8_t *>(p.tout) + (uint64_t)row * kFtN * ob, sStg + 2 * r * kStgPitch,
+                     kFtN * ob);
+          }
+          bulk_commit();
+          return;
+        }
         for (uint32_t r = 0; r < 2; r++) {
           const uint32_t row = 2 * u + r;
           if (row >= p.rows) break;
@@ -420,6 +442,38 @@ __global__ void __launch_bounds__(kFtThreads, 1)
       // the twiddles)
       const float inv = kFixedScale<DT> ? 1.0f : s_inv[i & 1][s_r];
       const uint32_t row = 2 * unit_of(i) + s_r;  // the same for the whole warp
+      if (!kFixedScale<DT> && p.inverse) {
+        // time sample n = k1 + 64 k2 of row s_r: conj of the forward bin,
+        // times the row's inverse scale and out_scale; consecutive lanes
+        // write consecutive samples
+        uint8_t *srow = sStg + 2 * s_r * kStgPitch;
+        const float f = inv * p.out_scale;
+        const bool i16 = p.out_dtype == MB_IQ_I16, i8 = p.out_dtype == MB_IQ_I8;
+        const float qmax = i16 ? 32767.f : 127.f, qmin = i16 ? -32768.f : -128.f;
+#pragma unroll
+        for (int jb = 0; jb < 16; jb += 8) {
+          float vr[8], vi[8];
+          tc::tmem_ld8x2(tl + 128 + 16 * part + jb, vr, tl + 192 + 16 * part + jb, vi);
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const uint32_t n = s_k1 + 64 * (16 * part + jb + j);
+            const float re = vr[j] * f, im = -vi[j] * f;
+            if (i16 || i8) {
+              int qr = __float2int_rn(re), qi = __float2int_rn(im);
+              if (re > qmax) qr = (int)qmax; else if (re < qmin) qr = (int)qmin;
+              if (im > qmax) qi = (int)qmax; else if (im < qmin) qi = (int)qmin;
+              if (i16)
+                *reinterpret_cast<short2 *>(srow + 4 * n) = make_short2((short)qr, (short)qi);
+              else
+                *reinterpret_cast<char2 *>(srow + 2 * n) = make_char2((char)qr, (char)qi);
+            } else {
+              *reinterpret_cast<__half2 *>(srow + 4 * n) = __floats2half2_rn(re, im);
+            }
+          }
+        }
+        arrive(&st_ready);
+        return;
+      }
       if (row < p.pilot_rows) {
         // LS estimate conj(X) p of subcarrier sc for user u0 + sc % sg into
         // csi[sc / sg][b][u] (fft_callback.cuh:76-108); a user with no pilot
@@ -548,6 +602,7 @@ __global__ void __launch_bounds__(kFtThreads, 1)
           float scale, inv;
           row_scale(rmax, scale, inv);
           if ((tid & 255) == 0) s_inv[i & 1][rh] = inv;
+          const float iscale = p.inverse ? -scale : scale;  // conj(z) for the inverse
 #pragma unroll
           for (int c2 = 0; c2 < 2; c2++) {
             float2 v[8];
@@ -555,8 +610,8 @@ __global__ void __launch_bounds__(kFtThreads, 1)
             for (int j = 0; j < 8; j++) v[j] = chunk_sample<DT>(raw[c2], j);
             re[c2] = make_uint4(h2_bits(v[0].x * scale, v[1].x * scale), h2_bits(v[2].x * scale, v[3].x * scale),
                                 h2_bits(v[4].x * scale, v[5].x * scale), h2_bits(v[6].x * scale, v[7].x * scale));
-            im[c2] = make_uint4(h2_bits(v[0].y * scale, v[1].y * scale), h2_bits(v[2].y * scale, v[3].y * scale),
-                                h2_bits(v[4].y * scale, v[5].y * scale), h2_bits(v[6].y * scale, v[7].y * scale));
+            im[c2] = make_uint4(h2_bits(v[0].y * iscale, v[1].y * iscale), h2_bits(v[2].y * iscale, v[3].y * iscale),
+                                h2_bits(v[4].y * iscale, v[5].y * iscale), h2_bits(v[6].y * iscale, v[7].y * iscale));
           }
         }
       }
@@ -738,6 +793,28 @@ mb_status fft_tc_uplink_lp(const FftTcPlan *pl, const void *iq, int iq_dtype, ui
   p.err = err;
   p.pilot_rows = 0;
   return fft_tc_launch(pl, iq, iq_dtype, p, st, upc);
+}
+
+bool fft_tc_inverse_supported(const FftTcPlan *pl, const void *in, int in_dtype, const void *out, int out_dtype) {
+  return pl && (in_dtype == MB_IQ_C32 || in_dtype == MB_IQ_F16) &&
+         (out_dtype == MB_IQ_I16 || out_dtype == MB_IQ_I8 || out_dtype == MB_IQ_F16) &&
+         (reinterpret_cast<uintptr_t>(in) & 15) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+}
+
+mb_status fft_tc_inverse(const FftTcPlan *pl, const void *in, int in_dtype, uint32_t rows, void *out, int out_dtype,
+                         int *err, cudaStream_t st) {
+  if (!fft_tc_inverse_supported(pl, in, in_dtype, out, out_dtype)) return MB_BAD_ARG;
+  if (rows == 0) return MB_OK;
+  FtParams p{};
+  p.rows = rows;
+  p.pilot_rows = 0;
+  p.M = 1;
+  p.inverse = 1;
+  p.out_dtype = out_dtype;
+  p.out_scale = out_dtype == MB_IQ_I16 ? 32768.f / kFtN : out_dtype == MB_IQ_I8 ? 128.f / kFtN : 1.f / kFtN;
+  p.tout = out;
+  p.err = err;
+  return fft_tc_launch(pl, in, in_dtype, p, st, 0);
 }
 
 bool fft_tc_pilot_supported(const FftTcPlan *pl, const void *iq) {

@@ -552,3 +552,23 @@ extern "C" mb_status mb_mlp_adam_step(mb_mlp *n, float lr, void *stream) {
   MB_CUDA_TRY(mlp_refresh_bf16(n, st));
   return MB_OK;
 }
+
+#include "zf.cuh"
+
+// The mixed ZF reads the network of its learned initial iterate from the
+// handle's own device buffers (the BF16 copies are refreshed by every
+// parameter update), so a captured slot replays with the current weights.
+mb_status mb::mlp_zf_init_view(const mb_mlp *n, ZfNetView *v) {
+  if (!n || !v) return MB_BAD_ARG;
+  if (n->n_in != kZfInitFeatures || n->n_out != kZfInitCoeffs || n->width == 0 ||
+      n->width > kZfInitMaxWidth)
+    return MB_BAD_SHAPE;
+  v->w1 = n->wb + n->off[0];
+  v->w2 = n->wb + n->off[2];
+  v->w3 = n->wb + n->off[4];
+  v->b1 = n->p + n->off[1];
+  v->b2 = n->p + n->off[3];
+  v->b3 = n->p + n->off[5];
+  v->width = n->width;
+  return MB_OK;
+}

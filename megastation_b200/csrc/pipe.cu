@@ -161,6 +161,13 @@ extern "C" mb_status mb_pipe_wait(mb_pipe *p, uint64_t ticket, uint32_t timeout_
   }
 }
 
+extern "C" mb_status mb_pipe_set_zf_init(mb_pipe *p, const mb_mlp *net) {
+  if (!p || !p->slot) return MB_BAD_ARG;
+  // no slot of the pipeline may be in flight while the choice changes
+  if (p->comp) MB_CUDA_TRY(cudaStreamSynchronize(p->comp));
+  return mb_slot_set_zf_init(p->slot, net);
+}
+
 extern "C" mb_status mb_pipe_io_bytes(const mb_pipe *p, uint64_t *iq, uint64_t *llr, uint64_t *hard) {
   if (!p || !iq || !llr || !hard) return MB_BAD_ARG;
   *iq = p->iq_bytes;

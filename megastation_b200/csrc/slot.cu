@@ -17,6 +17,7 @@
 #include "eq_tc.cuh"
 #include "fft.cuh"
 #include "zf.cuh"
+#include "precode_tc.cuh"
 
 using namespace mb;
 
@@ -36,6 +37,12 @@ struct mb_slot {
   uint32_t sb_cap;    // uplink symbols the y / y_lp buffers hold (>= sym_batch)
   uint32_t eq_cols;   // tensor-core equalizer columns per CTA (0: 128)
   float2 *precoded;   // [D][M][N]
+  const mb_mlp *zf_net;  // learned initial iterate of the mixed ZF (not owned), or null
+  // mixed-precision downlink on the tensor cores (N = 4096): the BF16
+  // precoder images (built with the precoder in the uplink's ZF stage) and
+  // the FP16 precoded spectra [D][M][N], whose guard bins stay zero
+  void *pc_img;
+  void *z16;
   cudaStream_t side;
   cudaStream_t crit;  // pilot FFT -> ZF: the critical path, at the highest stream priority
   cudaEvent_t ev_fork, ev_join, ev_crit;
@@ -124,6 +131,8 @@ extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   cudaFree(s->y_lp);
   cudaFree(s->img_w);
   cudaFree(s->precoded);
+  cudaFree(s->pc_img);
+  cudaFree(s->z16);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->crit) cudaStreamDestroy(s->crit);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
@@ -168,6 +177,15 @@ static mb_status slot_create(const mb_cell_desc *cell, bool sb_cap_all, mb_slot 
   alloc((void **)&s->precoder, sizeof(float2) * gmk);
   if (c.D) alloc((void **)&s->wmax, sizeof(float) * s->G);
   alloc((void **)&s->precoded, sizeof(float2) * (size_t)c.D * c.M * c.N);
+  if (c.D && c.zf_precision == MB_ZF_MIXED && c.N == 4096 && precode_tc_supported(c.K, c.sg) &&
+      (c.out_dtype == MB_IQ_I16 || c.out_dtype == MB_IQ_I8 || c.out_dtype == MB_IQ_F16)) {
+    alloc(&s->pc_img, (size_t)s->G * precode_tc_shape(c.M, c.K).img_group_bytes);
+    alloc(&s->z16, sizeof(__half2) * (size_t)c.D * c.M * c.N);
+    if (s->z16) {
+      const cudaError_t e = cudaMemset(s->z16, 0, sizeof(__half2) * (size_t)c.D * c.M * c.N);
+      if (e != cudaSuccess) st = record_error(e);
+    }
+  }
   const bool mixed = c.zf_precision == MB_ZF_MIXED;
   if (mixed && st == MB_OK && !equalize_tc_supported(c.K, c.sg, s->c.sym_batch))
     st = MB_UNSUPPORTED;
@@ -290,11 +308,18 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   MARK(mk->pilot);
   float2 *prec = c.D ? s->precoder : nullptr;
   if (mixed) {
-    mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, 0};
+    mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, s->zf_net ? 1u : 0u};
+    ZfNetView v{};
+    if (s->zf_net) {
+      r = mlp_zf_init_view(s->zf_net, &v);
+      if (r != MB_OK) return r;
+    }
     // W in FP32 only feeds the downlink precoder; the equalizer reads the image
     r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr,
-                     s->wmax);
+                     s->wmax, &v);
     if (r == MB_OK && prec) r = precoder_scale(s->csi, prec, s->wmax, c.M, c.K, s->G, cs);
+    // the tensor-core downlink's BF16 precoder images, from the same precoder
+    if (r == MB_OK && prec && s->pc_img) r = precoder_image(prec, s->pc_img, s->G, c.M, c.K, cs);
   } else {
     r = zf_chol(s->csi, prec, s->G, c.M, c.K, c.zf_precision == MB_ZF_FP64, status, nullptr, cs);
   }
@@ -399,6 +424,16 @@ extern "C" mb_status mb_slot_downlink(mb_slot *s, const mb_c32 *symbols,
   const mb_cell_desc &c = s->c;
   if (!c.D) return MB_BAD_SHAPE;
   cudaStream_t st = as_stream(stream);
+  if (s->pc_img && fft_ifft_tc_ok(s->fft, s->z16, MB_IQ_F16, out, c.out_dtype)) {
+    // mixed precision: precode on the tensor cores into FP16 spectra, then
+    // the tensor-core inverse FFT with the output quantiser
+    const DeviceTables *tab = device_tables();
+    if (!tab) return MB_CUDA_ERROR;
+    mb_status r = precode_tc(s->pc_img, reinterpret_cast<const float2 *>(symbols), s->z16, c.M, c.K, c.S, c.sg,
+                             c.N, (c.N - c.S) / 2, c.D, tab->err, st);
+    if (r != MB_OK) return r;
+    return fft_tc_inverse_slot(s->fft, s->z16, c.D, out, c.out_dtype, st);
+  }
   mb_status r = mb_precode(reinterpret_cast<const mb_c32 *>(s->precoder), symbols,
                            c.M, c.K, c.S, c.sg, c.N, (c.N - c.S) / 2, c.D,
                            reinterpret_cast<mb_c32 *>(s->precoded), st);
@@ -448,6 +483,22 @@ extern "C" mb_status mb_slot_buffers(mb_slot *s, mb_c32 **csi, mb_c32 **precoder
   if (!s) return MB_BAD_ARG;
   if (csi) *csi = reinterpret_cast<mb_c32 *>(s->csi);
   if (precoder) *precoder = reinterpret_cast<mb_c32 *>(s->precoder);
+  return MB_OK;
+}
+
+extern "C" mb_status mb_slot_set_zf_init(mb_slot *s, const mb_mlp *net) {
+  if (!s) return MB_BAD_ARG;
+  if (net && s->c.zf_precision != MB_ZF_MIXED) return MB_UNSUPPORTED;
+  if (net) {
+    ZfNetView v;
+    const mb_status r = mlp_zf_init_view(net, &v);
+    if (r != MB_OK) return r;
+  }
+  if (net == s->zf_net) return MB_OK;
+  // captured slots hold the previous choice in their kernel parameters
+  for (auto &e : s->graphs) cudaGraphExecDestroy(e.exec);
+  s->graphs.clear();
+  s->zf_net = net;
   return MB_OK;
 }
 

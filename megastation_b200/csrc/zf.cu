@@ -337,7 +337,8 @@ using namespace mb;
 
 struct mb_zf {
   uint32_t M, K, max_groups;
-  void *img_w;  // mixed-precision detector images, sized for max_groups
+  void *img_w;        // mixed-precision detector images, sized for max_groups
+  const mb_mlp *net;  // network of the learned initial iterate (not owned), or null
 };
 
 extern "C" mb_status mb_zf_create(uint32_t num_bs, uint32_t num_ue,
@@ -347,7 +348,7 @@ extern "C" mb_status mb_zf_create(uint32_t num_bs, uint32_t num_ue,
   if (num_bs == 0 || num_ue == 0 || num_ue > num_bs || num_ue > 64)
     return MB_BAD_SHAPE;
   if (!device_tables()) return MB_CUDA_ERROR;
-  mb_zf *z = new mb_zf{num_bs, num_ue, max_groups, nullptr};
+  mb_zf *z = new mb_zf{num_bs, num_ue, max_groups, nullptr, nullptr};
   const uint64_t bytes = zf_mixed_scratch_bytes(max_groups, num_bs, num_ue);
   cudaError_t e = cudaSuccess;
   if (bytes) e = cudaMalloc(&z->img_w, bytes);
@@ -385,10 +386,28 @@ extern "C" mb_status mb_zf_uplink(mb_zf *z, mb_c32 *csi, uint32_t groups,
       return zf_chol(c, nullptr, groups, z->M, z->K, false, status, cond, st);
     case MB_ZF_FP64:
       return zf_chol(c, nullptr, groups, z->M, z->K, true, status, cond, st);
-    case MB_ZF_MIXED:
-      return zf_mixed_run(c, z->img_w, groups, z->M, z->K, opts, status, cond, st);
+    case MB_ZF_MIXED: {
+      ZfNetView v{};
+      if (opts && opts->init == 1) {
+        if (!z->net) return MB_BAD_ARG;
+        const mb_status r = mlp_zf_init_view(z->net, &v);
+        if (r != MB_OK) return r;
+      }
+      return zf_mixed_run(c, z->img_w, groups, z->M, z->K, opts, status, cond, st, true, nullptr, &v);
+    }
   }
   return MB_BAD_ARG;
+}
+
+extern "C" mb_status mb_zf_set_init_net(mb_zf *z, const mb_mlp *net) {
+  if (!z) return MB_BAD_ARG;
+  if (net) {
+    ZfNetView v;
+    const mb_status r = mlp_zf_init_view(net, &v);
+    if (r != MB_OK) return r;
+  }
+  z->net = net;
+  return MB_OK;
 }
 
 extern "C" mb_status mb_zf_precoder(const mb_c32 *W, mb_c32 *P, uint32_t M,

@@ -1,5 +1,7 @@
 // zf.cuh -- internal launchers of the zero-forcing kernels.
 #pragma once
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace mb {
@@ -16,9 +18,24 @@ mb_status zf_chol(float2 *csi, float2 *precoder, uint32_t groups, uint32_t M,
 // W in place (FP32) and its per-group max |W| in wmax (if not null);
 // without write_w csi is left as scratch
 uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K);
+
+// Device view of the network of the learned polynomial initial iterate
+// (an mb_mlp with kZfInitFeatures inputs and kZfInitCoeffs outputs): BF16
+// weights W1 [n_in][width], W2 [width][width], W3 [width][n_out] and FP32
+// biases, all device memory owned by the mb_mlp.
+constexpr uint32_t kZfInitFeatures = 6, kZfInitCoeffs = 4, kZfInitMaxWidth = 256;
+struct ZfNetView {
+  const __nv_bfloat16 *w1, *w2, *w3;
+  const float *b1, *b2, *b3;
+  uint32_t width;
+};
+// fills v from an mb_mlp of the right shape (MB_BAD_SHAPE otherwise)
+mb_status mlp_zf_init_view(const mb_mlp *n, ZfNetView *v);
+
+// net (nullable) is used when opts->init == 1
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
                        const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
-                       bool write_w = true, float *wmax = nullptr);
+                       bool write_w = true, float *wmax = nullptr, const ZfNetView *net = nullptr);
 // precoder P[g][u][b] = W[g][b][u] / wmax[g] from a precomputed per-group max
 mb_status precoder_scale(const float2 *W, float2 *P, const float *wmax, uint32_t M, uint32_t K,
                          uint32_t groups, cudaStream_t st);

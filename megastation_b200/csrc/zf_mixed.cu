@@ -36,9 +36,12 @@ namespace mb {
 
 namespace {
 constexpr int kKT = 64;        // reduction elements per k tile
+constexpr float kPolyAccept = 0.04f;  // ||I - G X||_F before the last step of an accepted learned iterate
 constexpr int kThreads = 256;  // 8 warps; warps w and w+4 share TMEM lane quadrant w
 
 struct ZfmParams {
+  ZfNetView net;      // network of the learned initial iterate (used when learned)
+  uint32_t learned;   // 1: initial iterate from the learned polynomial, exact inverse as fallback
   float2 *csi;        // [G][M][K]: in CSI, out W (FP32)
   uint8_t *img_w;     // [G] detector images for the equalizer (BF16)
   int32_t *status;
@@ -236,6 +239,169 @@ __device__ __forceinline__ void cmatmul_any(const float2 *A, uint32_t lda, const
       cmatmul<4, HERM>(A, lda, B, ldb, K, out);
   }
 }
+
+// Block sums of three values and the block min / max of two; every thread
+// gets the results.  sred holds 5 x 8 floats.
+__device__ __forceinline__ void block_reduce5(float &a, float &b, float &c, float &mn, float &mx,
+                                              float *sred) {
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if (lane == 0) {
+    sred[warp] = a;
+    sred[8 + warp] = b;
+    sred[16 + warp] = c;
+    sred[24 + warp] = mn;
+    sred[32 + warp] = mx;
+  }
+  __syncthreads();
+  a = b = c = 0.f;
+  mn = INFINITY;
+  mx = -INFINITY;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; w++) {
+    a += sred[w];
+    b += sred[8 + w];
+    c += sred[16 + w];
+    mn = fminf(mn, sred[24 + w]);
+    mx = fmaxf(mx, sred[32 + w]);
+  }
+  __syncthreads();
+}
+
+// Learned polynomial initial iterate (no reference counterpart).  With
+// tau = tr(G) / K and Gn = G / tau, the initial iterate is
+// X0 = (a0 I + a1 Gn + a2 Gn^2 + a3 Gn^3) / tau, whose coefficients a come
+// from the network evaluated on six scale-free features of the group:
+// with t_k = tr(Gn^k) / K (t_1 = 1), the central moments of Gn's
+// eigenvalues t2 - 1, t3 - 3 t2 + 2 and t4 - 4 t3 + 6 t2 - 3 (Gn^2 is
+// needed for the iterate anyway, so t3 = <Gn, Gn^2> / K and t4 =
+// ||Gn^2||^2 / K cost no product of their own), the smallest and largest
+// diagonal entry of Gn minus 1, and K / M.  ns_iters Newton-Schulz steps
+// X <- X (2I - G X) follow, and at most two more while the residual is
+// below 0.3 but above the acceptance bound; X stays a polynomial in G, so
+// both products are Hermitian and only their upper blocks are computed.
+// The Frobenius norm of E = I - G X comes with every step's first product;
+// the iterate is accepted when the last one is at most kPolyAccept = 0.04
+// (the returned X then has ||I - G X||_F <= 1.6e-3, below the BF16 rounding
+// of the detector image), otherwise the caller falls back to the exact
+// inverse.  The network: BF16 weights, FP32 activations and accumulation,
+// ReLU hidden layers (the arithmetic of mb_mlp_forward).  Result in Xs.
+template <int MM>
+__device__ bool poly_init(const float2 *Gs, uint32_t ld, float2 *Xs, float2 *P2, float2 *P3, float2 *Ts,
+                          float2 *Xn, uint32_t K, uint32_t M, const ZfNetView &net, uint32_t ns_iters,
+                          float *sred, float *act, float *coef) {
+  const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
+  // tau and the diagonal's range
+  float d = 0.f, z1 = 0.f, z2 = 0.f, dmin = INFINITY, dmax = -INFINITY;
+  for (uint32_t i = tid; i < K; i += kThreads) {
+    const float g = Gs[i * ld + i].x;
+    d += g;
+    dmin = fminf(dmin, g);
+    dmax = fmaxf(dmax, g);
+  }
+  block_reduce5(d, z1, z2, dmin, dmax, sred);
+  const float tau = d / (float)K;
+  if (!(tau > 0.f) || !(dmin > 0.f)) return false;  // uniform
+  const float it = 1.f / tau, it2 = it * it;
+  // Gn^2 (Hermitian)
+  cmatmul_any<MM, true>(Gs, ld, Gs, ld, K,
+                        [&](uint32_t i, uint32_t j, float2 s) { P2[i * K + j] = make_float2(s.x * it2, s.y * it2); });
+  __syncthreads();
+  // t2, t3, t4
+  float a2 = 0.f, a3 = 0.f, a4 = 0.f, n0 = INFINITY, n1 = -INFINITY;
+  for (uint32_t e = tid; e < K * K; e += kThreads) {
+    const float2 g = Gs[(e / K) * ld + e % K], p = P2[e];
+    const float gx = g.x * it, gy = g.y * it;
+    a2 += gx * gx + gy * gy;
+    a3 += gx * p.x + gy * p.y;
+    a4 += p.x * p.x + p.y * p.y;
+  }
+  block_reduce5(a2, a3, a4, n0, n1, sred);
+  const float t2 = a2 / (float)K, t3 = a3 / (float)K, t4 = a4 / (float)K;
+  // the network: layer 1 (6 -> width), layer 2 (width -> width), layer 3
+  // (width -> 4), hidden activations in act[0..width) and act[256..)
+  if (tid == 0) {
+    coef[0] = t2 - 1.f;
+    coef[1] = t3 - 3.f * t2 + 2.f;
+    coef[2] = t4 - 4.f * t3 + 6.f * t2 - 3.f;
+    coef[3] = dmin * it - 1.f;
+    coef[4] = dmax * it - 1.f;
+    coef[5] = (float)K / (float)M;
+  }
+  __syncthreads();
+  const uint32_t W = net.width;
+  if ((uint32_t)tid < W) {
+    float h = net.b1[tid];
+#pragma unroll
+    for (uint32_t k = 0; k < kZfInitFeatures; k++) h = fmaf(coef[k], __bfloat162float(net.w1[k * W + tid]), h);
+    act[tid] = fmaxf(h, 0.f);
+  }
+  __syncthreads();
+  if ((uint32_t)tid < W) {
+    float h = net.b2[tid];
+    for (uint32_t k = 0; k < W; k++) h = fmaf(act[k], __bfloat162float(net.w2[k * W + tid]), h);
+    act[kZfInitMaxWidth + tid] = fmaxf(h, 0.f);
+  }
+  __syncthreads();
+  if (warp < (int)kZfInitCoeffs) {
+    float y = 0.f;
+    for (uint32_t k = lane; k < W; k += 32)
+      y = fmaf(act[kZfInitMaxWidth + k], __bfloat162float(net.w3[k * kZfInitCoeffs + warp]), y);
+    for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+    if (lane == 0) coef[8 + warp] = y + net.b3[warp];
+  }
+  __syncthreads();
+  const float c0 = coef[8], c1 = coef[9], c2 = coef[10], c3 = coef[11];
+  // Gn^3 = Gn Gn^2 (Hermitian)
+  cmatmul_any<MM, true>(Gs, ld, P2, K, K,
+                        [&](uint32_t i, uint32_t j, float2 s) { P3[i * K + j] = make_float2(s.x * it, s.y * it); });
+  __syncthreads();
+  for (uint32_t e = tid; e < K * K; e += kThreads) {
+    const uint32_t i = e / K, j = e % K;
+    const float2 g = Gs[i * ld + j], p2 = P2[e], p3 = P3[e];
+    const float re = (i == j ? c0 : 0.f) + c1 * g.x * it + c2 * p2.x + c3 * p3.x;
+    const float im = c1 * g.y * it + c2 * p2.y + c3 * p3.y;
+    Xs[i * ld + j] = make_float2(re * it, im * it);
+  }
+  __syncthreads();
+  float2 *xc = Xs, *xn = Xn;
+  uint32_t ldc = ld, ldn = K;
+  float e_last = INFINITY;
+  // ns_iters steps, then up to two more only to rescue a near miss
+  // (0.04 < ||E|| < 0.3); a start further off goes to the exact inverse
+  for (uint32_t s = 0; s < ns_iters + 2; s++) {
+    if (s >= ns_iters && (e_last <= kPolyAccept || e_last >= 0.3f)) break;  // uniform
+    float en = 0.f;
+    cmatmul_any<MM, true>(Gs, ld, xc, ldc, K, [&](uint32_t i, uint32_t j, float2 v) {
+      const float ex = (i == j ? 1.f : 0.f) - v.x, ey = -v.y;  // E = I - G X; T = I + E
+      en += ex * ex + ey * ey;
+      Ts[i * K + j] = make_float2((i == j ? 1.f : 0.f) + ex, ey);
+    });
+    float u0 = 0.f, u1 = 0.f, m0 = INFINITY, m1 = -INFINITY;
+    block_reduce5(en, u0, u1, m0, m1, sred);  // also orders the Ts writes before their reads
+    e_last = sqrtf(en);
+    if (!(e_last < 1.f)) return false;  // uniform: the iteration would not converge
+    cmatmul_any<MM, true>(xc, ldc, Ts, K, K, [&](uint32_t i, uint32_t j, float2 v) { xn[i * ldn + j] = v; });
+    __syncthreads();
+    float2 *t = xc;
+    xc = xn;
+    xn = t;
+    const uint32_t l = ldc;
+    ldc = ldn;
+    ldn = l;
+  }
+  if (xc != Xs) {
+    for (uint32_t e = tid; e < K * K; e += kThreads) Xs[(e / K) * ld + e % K] = xc[e];
+    __syncthreads();
+  }
+  return e_last <= kPolyAccept;
+}
 }  // namespace
 
 template <int MM>
@@ -247,6 +413,8 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   __shared__ int flag, fail, piv_bad;
   __shared__ float red[kThreads], red2[kThreads];
   __shared__ float2 prow[MM];  // Gauss-Jordan pivot rows, two buffers of KP <= MM / 2
+  __shared__ float zi_red[40], zi_coef[16];     // learned initial iterate: reductions, features, coefficients
+  __shared__ float zi_act[2 * kZfInitMaxWidth];  // and the network's hidden activations
 
   constexpr uint32_t tile_bytes = MM * kKT * 2;
   constexpr uint32_t TC = 256;             // TMEM columns: the Gram (MM) or TCH W tiles
@@ -266,6 +434,9 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   // iterate in the R(X) image; both are free between the Gram and W = X C
   float2 *Ts = reinterpret_cast<float2 *>(lo_t[0]);
   float2 *Xn = reinterpret_cast<float2 *>(ximg);
+  // powers Gn^2, Gn^3 of the learned initial iterate (behind Xs; allotted
+  // only when the kernel runs learned)
+  float2 *P2 = Xs + K * ld, *P3 = P2 + K * K;
 
   float2 *cg = q.csi + (uint64_t)g * M * K;
   uint8_t *imgw = q.img_w + (uint64_t)g * q.nkt * tile_bytes;
@@ -371,6 +542,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   // ----------------------------------------- Gram out, inverse, refinement
   float cond_est = INFINITY;
   int st = 0;
+  bool used_learned = false;  // the learned initial iterate was accepted
   float wmx = 0.f;  // this thread's max |W| over the values it stored
   if (!fail) {
     // R(G) = A + P A P^T (plane 1 of R(C) is P times plane 0): rows 2u and
@@ -394,12 +566,16 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
     }
     tc::fence_before_sync();
     __syncthreads();
-    bool pd;
-    if (MM == 64)
-      pd = K <= 16 ? gj_inverse<16>(Gs, Xs, K, ld, prow, &piv_bad)
-                   : gj_inverse<32>(Gs, Xs, K, ld, prow, &piv_bad);
-    else
-      pd = gj_inverse<64>(Gs, Xs, K, ld, prow, &piv_bad);
+    bool pd = false;
+    if (q.learned)
+      used_learned = poly_init<MM>(Gs, ld, Xs, P2, P3, Ts, Xn, K, M, q.net, q.ns_iters, zi_red, zi_act, zi_coef);
+    if (!used_learned) {
+      if (MM == 64)
+        pd = K <= 16 ? gj_inverse<16>(Gs, Xs, K, ld, prow, &piv_bad)
+                     : gj_inverse<32>(Gs, Xs, K, ld, prow, &piv_bad);
+      else
+        pd = gj_inverse<64>(Gs, Xs, K, ld, prow, &piv_bad);
+    }
     if (pd) {
       // Newton-Schulz: T = 2I - G X; X <- X T, ping-ponging Xs and Xn
       float2 *xc = Xs, *xn = Xn;
@@ -424,6 +600,8 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
         for (uint32_t e = tid; e < K * K; e += kThreads) Xs[(e / K) * ld + e % K] = xc[e];
         __syncthreads();
       }
+    }
+    if (pd || used_learned) {
       // 1-norm condition estimate ||G||_1 ||X||_1 (both Hermitian): thread
       // t sums column j0 + t % 32 over rows t / 32, t / 32 + 8, ...; warp 0
       // adds the eight partial sums and takes the maximum over columns
@@ -643,7 +821,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
     if (tid == 0) q.wmax[g] = fail ? 0.f : red[0];
   }
   if (tid == 0) {
-    if (q.status) q.status[g] = fail ? 1 : st;
+    if (q.status) q.status[g] = fail ? 1 : (st == 0 && used_learned ? 3 : st);
     if (q.cond) q.cond[g] = cond_est;
     if (fail && q.err) atomicOr(q.err, tc::kErrTimeout);
   }
@@ -652,9 +830,10 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   if (warp == 0) tc::tmem_dealloc(tmem, TC);
 }
 
-static size_t zfm_smem(uint32_t K, uint32_t MM, uint32_t hi_slots) {
+static size_t zfm_smem(uint32_t K, uint32_t MM, uint32_t hi_slots, bool learned) {
   const size_t tile = (size_t)MM * kKT * 2;
-  return (hi_slots + 2) * tile + (size_t)MM * MM * 2 + 2 * (size_t)K * (K + 1) * sizeof(float2);
+  return (hi_slots + 2) * tile + (size_t)MM * MM * 2 + 2 * (size_t)K * (K + 1) * sizeof(float2) +
+         (learned ? 2 * (size_t)K * K * sizeof(float2) : 0);
 }
 
 uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K) {
@@ -664,12 +843,17 @@ uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K) {
 
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
                        const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
-                       bool write_w, float *wmax) {
+                       bool write_w, float *wmax, const ZfNetView *net) {
   if (K == 0 || K > 64) return MB_UNSUPPORTED;
+  const bool learned = opts && opts->init == 1;
+  if (opts && opts->init > 1) return MB_BAD_ARG;
+  if (learned && (!net || !net->w1 || net->width == 0 || net->width > kZfInitMaxWidth)) return MB_BAD_ARG;
   const TcShape s = tc_shape(M, K);
   const DeviceTables *tab = device_tables();
   if (!tab) return MB_CUDA_ERROR;
   ZfmParams q;
+  q.net = learned ? *net : ZfNetView{};
+  q.learned = learned ? 1 : 0;
   q.csi = csi;
   q.img_w = reinterpret_cast<uint8_t *>(img_w);
   q.status = status;
@@ -706,9 +890,9 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
   }
   const size_t avail = (size_t)maxs - (size_t)static_smem[which].load();
   // keep every hi tile in shared memory when it fits, else stream two
-  q.resident = zfm_smem(K, s.MM, q.nh) <= avail ? 1 : 0;
+  q.resident = zfm_smem(K, s.MM, q.nh, learned) <= avail ? 1 : 0;
   q.write_w = write_w ? 1 : 0;
-  const size_t smem = zfm_smem(K, s.MM, q.resident ? q.nh : 2);
+  const size_t smem = zfm_smem(K, s.MM, q.resident ? q.nh : 2, learned);
   if (smem > avail) return MB_UNSUPPORTED;
   if (groups == 0) return MB_OK;
   if (s.MM == 64)

@@ -228,3 +228,105 @@ def blend_loss(mlp, data, batch=8192):
 def make_mlp(sg=16, width=256, seed=0, max_batch=8192):
     """An untrained network whose output is the coarse blend (0, 1, 0, 0)."""
     return MLP(num_features(sg), width, N_BLEND, max_batch=max_batch, seed=seed, out_bias=[0, 1, 0, 0])
+
+
+# ---------------------------------------------------------------------------
+# Learned initial iterate of the group ZF (mixed precision, any cell shape):
+# a network maps six spectral features of a group's Gram to the coefficients
+# of a cubic polynomial X0 = p(Gn) / tau, the Newton-Schulz start that
+# replaces the exact inverse (mb_zf_set_init_net, mb_slot_set_zf_init).
+
+ZF_INIT_FEATURES, ZF_INIT_COEFFS = 6, 4
+# (I - (I - Gn))^-1 to third order: the untrained network's output, and the
+# fixed (not learned) polynomial the learned one is compared with
+NEUMANN3 = (4.0, -6.0, 4.0, -1.0)
+
+
+def make_zf_init_net(width=64, seed=0, max_batch=8192):
+    """An untrained initial-iterate network (6 -> width -> width -> 4, ReLU,
+    BF16 weights) whose output is the third-order Neumann polynomial."""
+    return MLP(ZF_INIT_FEATURES, width, ZF_INIT_COEFFS, max_batch=max_batch, seed=seed, out_bias=NEUMANN3)
+
+
+def group_csi(M, K, n, seed, G=205, sg=16, N=4096, S=3276, n_taps=8, rho=(0.3, 0.7), tap_decay=(1.0, 3.0),
+              snr_db=(18.0, 30.0), batch=32, device="cuda"):
+    """n comb-pilot CSI realisations [n][G][M][K] (complex64, device) of the
+    'tdl' channel of datagen: n_taps taps at 0..n_taps-1 samples with PDP
+    e^{-l / decay}, exponential receive correlation rho, CN(0, 1) per tap
+    and link; user u's estimate conj(H) sits at its pilot subcarrier
+    g sg + u mod sg, plus CN(0, 10^(-snr/10)) estimation noise.  rho, decay
+    and SNR are drawn uniformly per realisation from the given ranges.
+    Synthetic training data, generated with torch in batches."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    rng = np.random.default_rng(seed)
+    start = (N - S) // 2
+    s_pil = np.minimum(np.arange(G)[:, None] * sg + (np.arange(K)[None, :] % sg), S - 1)  # [G][K]
+    bins = (s_pil + start + N // 2) % N
+    f = torch.from_numpy((((bins + N // 2) % N) - N // 2).astype(np.float64)).to(device)
+    tau = torch.arange(n_taps, dtype=torch.float64, device=device)
+    ph = torch.exp(-2j * math.pi * f[..., None] * tau / N)  # [G][K][L]
+    idx = np.arange(M)
+    out = torch.empty(n, G, M, K, dtype=torch.complex64, device=device)
+    for i0 in range(0, n, batch):
+        B = min(batch, n - i0)
+        rh = rng.uniform(*rho, B)
+        dec = rng.uniform(*tap_decay, B)
+        snr = rng.uniform(*snr_db, B)
+        Rh = np.stack([np.linalg.cholesky(r ** np.abs(idx[:, None] - idx[None, :]) + 1e-12 * np.eye(M)) for r in rh])
+        pdp = np.exp(-np.arange(n_taps)[None, :] / dec[:, None])
+        pdp /= pdp.sum(1, keepdims=True)
+        w = torch.complex(torch.randn(B, n_taps, M, K, generator=g, device=device, dtype=torch.float64),
+                          torch.randn(B, n_taps, M, K, generator=g, device=device, dtype=torch.float64)) / math.sqrt(2)
+        w = torch.einsum("nab,nlbk->nlak", torch.from_numpy(Rh).to(device).to(w.dtype), w)
+        w = w * torch.from_numpy(np.sqrt(pdp)).to(device)[:, :, None, None]
+        H = torch.einsum("gkl,nlbk->ngbk", ph, w)  # [B][G][M][K]
+        nz = torch.complex(torch.randn(B, G, M, K, generator=g, device=device, dtype=torch.float64),
+                           torch.randn(B, G, M, K, generator=g, device=device, dtype=torch.float64))
+        sd = torch.from_numpy(np.sqrt(10.0 ** (-snr / 10.0) / 2)).to(device)[:, None, None, None]
+        out[i0:i0 + B] = (torch.conj(H) + nz * sd).to(torch.complex64)
+    return out
+
+
+def zf_init_targets(csi, stream=None):
+    """(features [G][6], A [G][4][4], b [G][4]) of every group of csi
+    [G][M][K] (mb_zf_init_targets, FP64 on the GPU)."""
+    G, M, K = csi.shape
+    F = torch.empty(G, ZF_INIT_FEATURES, dtype=torch.float32, device=csi.device)
+    A = torch.empty(G, ZF_INIT_COEFFS, ZF_INIT_COEFFS, dtype=torch.float32, device=csi.device)
+    b = torch.empty(G, ZF_INIT_COEFFS, dtype=torch.float32, device=csi.device)
+    check(LIB.mb_zf_init_targets(_dev(csi, "csi", torch.complex64), G, M, K, _dev(F, "features"), _dev(A, "A"),
+                                 _dev(b, "b"), _stream(stream)), "mb_zf_init_targets")
+    return F, A, b
+
+
+def zf_init_training_set(shapes, n_real, seed, **channel):
+    """Features, A, b and c = 1 of every group of n_real realisations per
+    (M, K) shape in `shapes` (group_csi's channel model)."""
+    Xs, As, bs = [], [], []
+    for k, (M, K) in enumerate(shapes):
+        done = 0
+        while done < n_real:
+            n = min(64, n_real - done)
+            csi = group_csi(M, K, n, seed + 7919 * k + done, **channel)
+            F, A, b = zf_init_targets(csi.view(-1, M, K))  # every group of every realisation
+            Xs.append(F)
+            As.append(A)
+            bs.append(b)
+            done += n
+    X, A, b = torch.cat(Xs), torch.cat(As), torch.cat(bs)
+    return X, A, b, torch.ones(X.shape[0], dtype=torch.float32, device=X.device)
+
+
+def poly_residual(net, data, batch=8192):
+    """Mean ||I - Gn p(Gn)||_F^2 / K over `data` for the network's
+    coefficients and for the fixed Neumann polynomial."""
+    X, A, b, c = data
+    tot_l, tot_n, n = 0.0, 0.0, X.shape[0]
+    a_n = torch.tensor(NEUMANN3, dtype=torch.float64, device=X.device)
+    for i in range(0, n, batch):
+        y = net.forward(X[i:i + batch].contiguous()).double()
+        Ai, bi = A[i:i + batch].double(), b[i:i + batch].double()
+        tot_l += float((torch.einsum("bi,bij,bj->b", y, Ai, y) - 2 * (bi * y).sum(1) + 1).sum())
+        tot_n += float((torch.einsum("i,bij,j->b", a_n, Ai, a_n) - 2 * (bi * a_n).sum(1) + 1).sum())
+    return tot_l / n, tot_n / n

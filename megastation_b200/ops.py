@@ -138,17 +138,44 @@ class DownlinkIFFT(_FFTBase):
         check(LIB.mb_ifft_downlink(self._h, _dev(inp, "in"), n_sym, _dev(out, "out"), code,
                                    _stream(stream)), "DownlinkIFFT")
 
+    def mixed(self, inp, out, stream=None):
+        """Mixed-precision inverse FFT (mb_ifft_downlink_mixed): inp
+        [..., M, N] complex64 or [..., M, N, 2] float16 spectra; at N = 4096
+        with int16 / int8 / float16 outputs on the tensor cores."""
+        ptr, in_code, n_sym = _iq(inp, "in", self.bs_num, self.ofdm_ca)
+        if in_code not in (_lib.MB_IQ_C32, _lib.MB_IQ_F16):
+            raise ValueError("in must be complex64 or float16 pairs")
+        if out.dtype not in _IQ_CODE:
+            raise ValueError(f"unsupported output dtype {out.dtype}")
+        code = _IQ_CODE[out.dtype]
+        per = 1 if code == _lib.MB_IQ_C32 else 2
+        if out.numel() != n_sym * self.bs_num * self.ofdm_ca * per:
+            raise ValueError("out size mismatch")
+        check(LIB.mb_ifft_downlink_mixed(self._h, ptr, in_code, n_sym, _dev(out, "out"), code, _stream(stream)),
+              "DownlinkIFFT.mixed")
+
 
 class Beamform:
     """beamform/beamform.h:27-84: zero-forcing detector and precoder."""
 
     def __init__(self, num_bs, num_ue, batch_count, precision=_lib.MB_ZF_FP32, ns_iters=2,
-                 cond_threshold=1e4):
+                 cond_threshold=1e4, init_net=None):
         h = ctypes.c_void_p()
         check(LIB.mb_zf_create(num_bs, num_ue, batch_count, ctypes.byref(h)), "Beamform")
         self._h = h
         self.num_bs, self.num_ue, self.batch_count = num_bs, num_ue, batch_count
         self.opts = _lib.MbZfOpts(precision, ns_iters, cond_threshold, 0)
+        self._net = None
+        if init_net is not None:
+            self.set_init_net(init_net)
+
+    def set_init_net(self, net):
+        """The mixed ZF starts Newton-Schulz from the learned polynomial
+        iterate of `net` (a learned.MLP with 6 inputs and 4 outputs); None
+        returns to the exact inverse."""
+        check(LIB.mb_zf_set_init_net(self._h, net._h if net is not None else None), "Beamform.set_init_net")
+        self._net = net  # the library does not own it: keep it alive
+        self.opts.init = 1 if net is not None else 0
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -291,6 +318,29 @@ class Precode:
         check(LIB.mb_precode(_dev(precoded, "precoded"), _dev(ueVec, "ueVec"), M, K, S, precode_skip,
                              N, bs_start, n_sym, _dev(bsVec, "bsVec"), _stream(stream)),
               "Precode.precode")
+
+
+    @staticmethod
+    def precode_tc(precoded, ueVec, z, precode_skip, bs_start, scratch=None, stream=None):
+        """Mixed-precision precode on the tensor cores (mb_precode_tc):
+        z [n_sym, M, N, 2] float16 gets the data bins; the other bins are
+        left as they are.  scratch: a uint8 CUDA tensor of at least
+        mb_precode_tc_scratch bytes (allocated here when None)."""
+        K, M = precoded.shape[-2], precoded.shape[-1]
+        S = ueVec.shape[-1]
+        n_sym = ueVec.numel() // (K * S)
+        if z.dtype != torch.float16 or z.shape[-1] != 2 or z.shape[-3] != M or z.numel() % (n_sym * M * 2):
+            raise ValueError("z must be [n_sym, M, N, 2] float16")
+        N = z.shape[-2]
+        nb = _lib.U64()
+        check(LIB.mb_precode_tc_scratch(M, K, S, precode_skip, ctypes.byref(nb)), "mb_precode_tc_scratch")
+        if scratch is None:
+            scratch = torch.empty(nb.value, dtype=torch.uint8, device=z.device)
+        if scratch.numel() < nb.value:
+            raise ValueError(f"scratch needs {nb.value} bytes")
+        check(LIB.mb_precode_tc(_dev(precoded, "precoded", torch.complex64), _dev(ueVec, "ueVec", torch.complex64),
+                                M, K, S, precode_skip, N, bs_start, n_sym, _dev(z, "z"), _dev(scratch, "scratch"),
+                                _stream(stream)), "Precode.precode_tc")
 
 
 class Modulation:

@@ -55,6 +55,13 @@ class UplinkSlot:
               "mb_slot_downlink")
         return out
 
+    def set_zf_init(self, net):
+        """Mixed ZF from the learned polynomial initial iterate of `net` (a
+        learned.MLP with 6 inputs and 4 outputs); None: the exact inverse.
+        Status 3 then marks groups solved from the learned iterate."""
+        check(LIB.mb_slot_set_zf_init(self._h, net._h if net is not None else None), "mb_slot_set_zf_init")
+        self._zf_net = net  # not owned by the library: keep it alive
+
     def timing(self, max_calls):
         """Record per-stage CUDA events for the next max_calls slots."""
         check(LIB.mb_slot_timing(self._h, max_calls), "mb_slot_timing")
@@ -143,6 +150,12 @@ class SlotPipeline:
             return False
         check(r, "mb_pipe_wait")
         return True
+
+    def set_zf_init(self, net):
+        """The pipeline's slots take the learned initial iterate of `net`
+        (UplinkSlot.set_zf_init); None: the exact inverse."""
+        check(LIB.mb_pipe_set_zf_init(self._h, net._h if net is not None else None), "mb_pipe_set_zf_init")
+        self._zf_net = net
 
     def timer_start(self):
         """Device timer from the next submitted slot's sample copy on."""

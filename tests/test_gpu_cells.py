@@ -98,4 +98,5 @@ def test_cells_vs_oracle(n, seed, precision):
         # as antennas have ill-conditioned groups); never 1 (not PD)
         assert np.isin(cs.status[c].cpu().numpy(), (0, 2)).all(), c
         _, ref = oracle_uplink(cfg, d)
-        check_uplink(cfg, ref, llr[c].cpu().numpy(), hard[c].cpu().numpy(), precision, f"cell {c}")
+        check_uplink(cfg, ref, llr[c].cpu().numpy(), hard[c].cpu().numpy(), precision, f"cell {c}",
+                     sent=d["bits"])

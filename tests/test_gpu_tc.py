@@ -275,7 +275,7 @@ def test_mixed_hard_bits_match_plain_path(mb, iq_dtype):
     iq = torch.from_numpy(d["iq"]).cuda()
     res = {}
     for prec in ("fp32", "mixed"):
-        run = slot.UplinkSlot(cfg, precision=prec, sym_batch=12, use_graph=True)
+        run = slot.UplinkSlot(cfg, precision=prec, sym_batch=12)
         llr, hard = run(iq)
         torch.cuda.synchronize()
         res[prec] = (llr.cpu().numpy().astype(np.float32)[..., zeros:zeros + n_valid],
