@@ -56,7 +56,8 @@ def test_ifft_tc_vs_oracle(mb, in_dtype, out_dtype):
     start = (N - S) // 2
     bins = (np.arange(S) + start + N // 2) % N
     x = np.zeros((D, M, N), np.complex64)
-    amp = {"int16": 0.05, "int8": 0.05, "f16": 1.0}[out_dtype]
+    # spectra sized so that the time samples span many LSBs of the format
+    amp = {"int16": 0.05, "int8": 2.0, "f16": 1.0}[out_dtype]
     x[..., bins] = (amp * (rng.standard_normal((D, M, S)) + 1j * rng.standard_normal((D, M, S)))).astype(np.complex64)
     if in_dtype == "f16":
         xin = torch.from_numpy(np.stack([x.real, x.imag], -1).astype(np.float16)).cuda()
