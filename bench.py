@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--rotate", type=int, default=4, help="distinct input slots cycled (L2 flush)")
     ap.add_argument("--windows", type=int, default=10,
                     help="minimum number of repeated K-slot windows timed after the headline window")
+    ap.add_argument("--min-slots", type=int, default=1000,
+                    help="full256x64: consecutive slots timed for the latency percentiles (at least --steps)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -623,7 +625,7 @@ def run_full(args):
     stream = torch.cuda.Stream()
     # the workload's latency percentiles are over at least 1000 consecutive
     # slots (the distinct seeded inputs rotated)
-    n = max(args.steps, 1000)
+    n = max(args.steps, args.min_slots)
 
     def step(k):
         run(iqs[k % R], llr[k % 2], hard[k % 2], stream=stream)
