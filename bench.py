@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-inflight", action="store_true", help="skip timing two slots in flight")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the short runs of the full-slot (256x64) and 32-cell workloads in the default line")
     return ap.parse_args()
 
 
@@ -597,7 +599,7 @@ def workload_config(cfg, args, R=None):
             "seed": cfg.seed}
 
 
-def run_full(args):
+def measure_full(args, n_min=None):
     """Uplink + downlink slots of a 256-antenna, 64-user cell (N = 4096,
     S = 3276, P = 4 pilot, U = 5 uplink, D = 5 downlink symbols, 256-QAM at
     30 dB, correlated 8-tap channel): uplink FP16 LLRs and descrambled hard
@@ -625,7 +627,7 @@ def run_full(args):
     stream = torch.cuda.Stream()
     # the workload's latency percentiles are over at least 1000 consecutive
     # slots (the distinct seeded inputs rotated)
-    n = max(args.steps, args.min_slots)
+    n = max(args.steps, args.min_slots if n_min is None else n_min)
 
     def step(k):
         run(iqs[k % R], llr[k % 2], hard[k % 2], stream=stream)
@@ -685,7 +687,12 @@ def run_full(args):
                          if args.precision == "mixed" else "FP32 precode and FP32 Stockham inverse FFT"),
             "note": "ZF from the exact initial iterate: the learned polynomial's network is trained for "
                     "K/M = 1/8 cells, and at K/M = 1/4 most groups would fall back to the exact inverse"}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_full(args):
+    """Prints measure_full's line (config 5 as a workload of its own)."""
+    print(json.dumps(measure_full(args)), flush=True)
 
 
 def run_learned(args):
@@ -815,7 +822,7 @@ def run_learned(args):
     print(json.dumps(line), flush=True)
 
 
-def run_cells(args):
+def measure_cells(args, steps=None, reps=10):
     """The batched uneven-cells workload: 32 seeded cells (antennas, users,
     subcarriers, QAM drawn per cell), one CUDA graph launch per slot, tile
     choices from the autotuner; value = batched slots (all 32 cells) per
@@ -826,11 +833,12 @@ def run_cells(args):
     cfgs = datagen.make_cells(n=32, seed=3)
     data = [datagen.make_slot(c) for c in cfgs]
     R = 2
+    steps = args.steps if steps is None else steps
     iqs = [[torch.from_numpy(d["iq"]).cuda() for d in data] for _ in range(R)]
     stream = torch.cuda.Stream()
     cs = cells.Cells(cfgs, precision=args.precision)
     with torch.cuda.stream(stream):
-        choice, tuned_us = cs.autotune(iqs[0], reps=10, stream=stream)
+        choice, tuned_us = cs.autotune(iqs[0], reps=reps, stream=stream)
         for k in range(max(args.warmup, 2 * R)):
             cs(iqs[k % R], stream=stream)
     stream.synchronize()
@@ -840,7 +848,7 @@ def run_cells(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    for k in range(args.steps):
+    for k in range(steps):
         cs(iqs[k % R], stream=stream)
     e1.record(stream)
     e1.synchronize()
@@ -855,27 +863,32 @@ def run_cells(args):
     stream.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
-    for k in range(args.steps):
+    for k in range(steps):
         for c, r in enumerate(runs):
             r(iqs[k % R][c], stream=stream)
     f1.record(stream)
     f1.synchronize()
     ms_seq = f0.elapsed_time(f1)
     launches = sum(slot_launches(c, max(c.U, 1), args.precision == "mixed") for c in cfgs)
-    line = {"metric": "batched slots/s (32 uneven cells)", "value": args.steps / (ms / 1e3),
-            "unit": "slots/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": "batched slots/s (32 uneven cells)", "value": steps / (ms / 1e3),
+            "unit": "slots/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": MIXED_DTYPE if args.precision == "mixed" else "f32",
             "data": "synthetic (seeded, megastation_b200.datagen.make_cells)",
             "config": {"workload": "32 uneven cells: M in {32,64,128}, K in {4,8,16,32}, S in {600,1200,3276} "
                                    "with N in {1024,2048,4096}, QAM {4,16,64}, i.i.d. Rayleigh, 15-25 dB, seed 3",
                        "cells": [[c.M, c.K, c.N, c.S, c.Qm] for c in cfgs],
                        "l2": f"{sum(d['iq'].nbytes for d in data) / 1e6:.0f} MB of samples per slot, {R} slots rotated"},
-            "clocks": clk, "gpu_launches": launches * args.steps, "graph_launches_per_slot": 1,
+            "clocks": clk, "gpu_launches": launches * steps, "graph_launches_per_slot": 1,
             "autotune": {"us_per_slot_tuned": tuned_us, "choices": choice},
-            "one_handle_per_cell": {"value": args.steps / (ms_seq / 1e3), "unit": "slots/s",
+            "one_handle_per_cell": {"value": steps / (ms_seq / 1e3), "unit": "slots/s",
                                     "note": "32 graph launches per slot on one stream"}}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_cells(args):
+    """Prints measure_cells's line (config 3 as a workload of its own)."""
+    print(json.dumps(measure_cells(args)), flush=True)
 
 
 def main():
@@ -1030,6 +1043,21 @@ def main():
                "pipeline": "mb_pipe (depth 2): H2D of slot k+1 and D2H of slot k-1 overlap slot k"}
         del pipe
 
+    # short runs of the other measured workloads, so that their numbers come
+    # with every default run: the full uplink + downlink slot (256 x 64,
+    # 200 consecutive slots, latency percentiles) and the 32 uneven cells
+    # (autotuned, 50 batched slots); their own --workload lines go further
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        f = measure_full(args, n_min=200)
+        c = measure_cells(args, steps=50, reps=5)
+        configs = {
+            "full256x64": {**{k: f[k] for k in ("metric", "value", "unit", "ms_per_step", "latency_us",
+                                                   "uplink_evm_db", "downlink", "gpu_launches")},
+                           "workload": f["config"]["workload"], "slots": f["steps"]},
+            "cells32": {**{k: c[k] for k in ("metric", "value", "unit", "ms_per_step", "autotune",
+                                                "one_handle_per_cell", "gpu_launches")},
+                        "workload": c["config"]["workload"], "steps": c["steps"]}}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(cfg, d, args.cpu_seconds)
@@ -1047,7 +1075,7 @@ def main():
             "config": workload_config(cfg, args), "clocks": clk, "e2e": e2e,
             "gpu_launches": launches_per_slot * args.steps, "roofline": roof, "cpu_baseline": cpu,
             "plain_fp32": plain, "mixed_exact_init": exact, "zf_init": init_info, "evm_db": evm,
-            "hard_bits_vs_plain": hb, "repeat": repeat,
+            "hard_bits_vs_plain": hb, "repeat": repeat, "other_workloads": configs,
             "in_flight": inflight,
             "parallelism": f"replicas x{world}"}
     print(json.dumps(line), flush=True)

@@ -68,18 +68,33 @@ __global__ void __launch_bounds__(kPcThreads, 1) precode_tc_kernel(const PcParam
     for (uint32_t kt = 0; kt < q.nkt; kt++) tc::bulk_g2s(sB + kt * kBTile, src + (uint64_t)kt * kBTile, kBTile, &img_bar);
   }
   if (warp == 0) tc::tmem_alloc(&tmem_slot, 256);
-  // A: thread -> (column c, user pair); s_u of column (l, sl) in BF16, Re in
-  // plane 0 and Im in plane 1; columns beyond ncols are zero
+  // A: work item -> (column cc, 8 users u0..u0+7): eight loads of s_u at the
+  // column's (symbol, subcarrier) (consecutive threads: consecutive columns,
+  // so consecutive subcarriers), then one 16-byte store of the BF16 real
+  // parts (plane 0) and one of the imaginary parts (plane 1); columns beyond
+  // ncols and users beyond K are zero
   const uint32_t s0 = g * q.sg;
-  for (uint32_t e = tid; e < kCols * q.Kp; e += kPcThreads) {
-    const uint32_t u = e / kCols, cc = e % kCols;  // consecutive threads: consecutive columns
-    float2 v = make_float2(0.f, 0.f);
-    if (cc < ncols && u < q.K) {
-      const uint32_t l = cc / q.sg, s = s0 + cc % q.sg;
-      if (s < q.S) v = __ldg(q.sym + ((uint64_t)(l_off + l) * q.K + u) * q.S + s);
+  {
+    const uint32_t cc = tid % kCols;
+    const uint32_t l = cc / q.sg, s = s0 + cc % q.sg;
+    const bool col_ok = cc < ncols && s < q.S;
+    const float2 *src = q.sym + (uint64_t)(l_off + l) * q.K * q.S + s;
+    for (uint32_t u0 = (tid / kCols) * 8; u0 < q.Kp; u0 += (kPcThreads / kCols) * 8) {
+      float2 v[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        v[j] = col_ok && u0 + j < q.K ? __ldg(src + (uint64_t)(u0 + j) * q.S) : make_float2(0.f, 0.f);
+      uint32_t re[4], im[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const __nv_bfloat162 a = __floats2bfloat162_rn(v[2 * j].x, v[2 * j + 1].x);
+        const __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * j].y, v[2 * j + 1].y);
+        re[j] = *reinterpret_cast<const uint32_t *>(&a);
+        im[j] = *reinterpret_cast<const uint32_t *>(&b);
+      }
+      *reinterpret_cast<uint4 *>(sA + kmaj(cc, u0, kATile)) = make_uint4(re[0], re[1], re[2], re[3]);
+      *reinterpret_cast<uint4 *>(sA + kmaj(cc, q.Kp + u0, kATile)) = make_uint4(im[0], im[1], im[2], im[3]);
     }
-    *reinterpret_cast<__nv_bfloat16 *>(sA + kmaj(cc, u, kATile)) = __float2bfloat16_rn(v.x);
-    *reinterpret_cast<__nv_bfloat16 *>(sA + kmaj(cc, q.Kp + u, kATile)) = __float2bfloat16_rn(v.y);
   }
   tc::fence_proxy_async_smem();
   tc::fence_before_sync();
@@ -140,26 +155,41 @@ __global__ void __launch_bounds__(kPcThreads, 1) precode_tc_kernel(const PcParam
   if (warp == 0) tc::tmem_dealloc(tmem, 256);
 }
 
-// P [G][K][M] (the scaled precoder) -> the per-(group, half) B tiles
+// P [G][K][M] (the scaled precoder) -> the per-(group, half) B tiles.  A
+// work item is one antenna b and 8 users u0..u0+7: eight loads of P[u][b]
+// (consecutive threads: consecutive antennas, coalesced), then the four
+// 16-byte chunks of rows 2b (Re z) and 2b+1 (Im z) in planes 0 and 1.
 __global__ void precoder_image_kernel(const float2 *P, __nv_bfloat16 *img, uint32_t M, uint32_t K,
                                       uint32_t Kp, uint32_t H, uint32_t nkt) {
   const uint32_t g = blockIdx.x, h = blockIdx.y;
-  const uint32_t per = nkt * (kBTile / 2);  // elements of one (group, half)
-  __nv_bfloat16 *out = img + ((uint64_t)g * H + h) * per;
+  uint8_t *out = reinterpret_cast<uint8_t *>(img) + ((uint64_t)g * H + h) * nkt * kBTile;
   const float2 *Pg = P + (uint64_t)g * K * M;
-  for (uint32_t e = threadIdx.x; e < per; e += blockDim.x) {
-    // e in memory order: k tile, row group, k chunk, row, element
-    const uint32_t el = e % 8, rr = (e / 8) % 8, kc = (e / 64) % 8, rg = (e / 512) % (2 * kAnt / 8),
-                   kt = e / (kBTile / 2);
-    const uint32_t n = rg * 8 + rr, kk = kt * kKT + kc * 8 + el;
-    const uint32_t b = h * kAnt + n / 2, ri = n & 1, pl = kk / Kp, u = kk % Kp;
-    float v = 0.f;
-    if (b < M && u < K) {
-      const float2 p = Pg[(uint64_t)u * M + b];
-      // Re z = Re P Re s - Im P Im s; Im z = Im P Re s + Re P Im s
-      v = ri == 0 ? (pl == 0 ? p.x : -p.y) : (pl == 0 ? p.y : p.x);
+  const uint32_t items = kAnt * (Kp / 8);
+  for (uint32_t e = threadIdx.x; e < items; e += blockDim.x) {
+    const uint32_t bl = e % kAnt, u0 = (e / kAnt) * 8, b = h * kAnt + bl;
+    float2 p[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      p[j] = b < M && u0 + j < K ? __ldg(Pg + (uint64_t)(u0 + j) * M + b) : make_float2(0.f, 0.f);
+    // Re z = Re P Re s - Im P Im s; Im z = Im P Re s + Re P Im s
+    uint32_t w[4][4];  // [ri * 2 + plane][pair]
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const float2 a = p[2 * j], c = p[2 * j + 1];
+      const __nv_bfloat162 r0 = __floats2bfloat162_rn(a.x, c.x), r1 = __floats2bfloat162_rn(-a.y, -c.y);
+      const __nv_bfloat162 i0 = __floats2bfloat162_rn(a.y, c.y), i1 = __floats2bfloat162_rn(a.x, c.x);
+      w[0][j] = *reinterpret_cast<const uint32_t *>(&r0);
+      w[1][j] = *reinterpret_cast<const uint32_t *>(&r1);
+      w[2][j] = *reinterpret_cast<const uint32_t *>(&i0);
+      w[3][j] = *reinterpret_cast<const uint32_t *>(&i1);
     }
-    out[e] = __float2bfloat16_rn(v);
+#pragma unroll
+    for (int ri = 0; ri < 2; ri++)
+#pragma unroll
+      for (int pl = 0; pl < 2; pl++) {
+        const uint32_t *v = w[ri * 2 + pl];
+        *reinterpret_cast<uint4 *>(out + kmaj(2 * bl + ri, pl * Kp + u0, kBTile)) = make_uint4(v[0], v[1], v[2], v[3]);
+      }
   }
 }
 
