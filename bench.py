@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cell256x32",
-                    choices=["cell256x32", "cells32", "full256x64", "learned128x16"],
+                    choices=["cell256x32", "cells32", "full256x64", "learned128x16", "learned256x32"],
                     help="cells32: 32 seeded uneven cells in one graph launch per slot (autotuned); "
                          "full256x64: uplink + downlink slot, 256-QAM, latency percentiles; "
                          "learned128x16: per-subcarrier ZF with the learned initialiser")
@@ -695,29 +695,40 @@ def run_full(args):
     print(json.dumps(measure_full(args)), flush=True)
 
 
-def run_learned(args):
-    """Per-subcarrier ZF with the learned initialiser on a 128-antenna,
-    16-user cell (N = 2048, S = 1200, 16-QAM, 25 dB) over the delay-spread
-    TDL channel (8 taps, delay spread uniform in 50-300 ns): the MLP is
-    trained on the GPU (library kernels) on pilot CSI of seeded channel
-    realisations, about 1e6 subcarrier samples with exact FP64 inverse labels;
-    then EVM and uncoded BER of per-group ZF, exact per-subcarrier ZF, and the
-    learned and coarse iterates with 0-2 Newton-Schulz steps on slots of
-    50-300 ns, and slots/s of each detector path (graph-replayed slot:
-    pilot FFT, ZF, uplink FFT, equalize)."""
+def run_learned(args, shape="128x16"):
+    """Per-subcarrier ZF with the learned initialiser, on a 128-antenna,
+    16-user cell (N = 2048, S = 1200, 16-QAM, 25 dB; config 4) or, with
+    shape "256x32", on the headline cell (N = 4096, S = 3276, 64-QAM, 25 dB),
+    over the delay-spread TDL channel (8 taps, delay spread uniform in
+    50-300 ns): the MLP is trained on the GPU (library kernels) on pilot CSI
+    of seeded channel realisations, about 1e6 subcarrier samples with exact
+    FP64 inverse labels; then EVM and uncoded BER of per-group ZF, exact
+    per-subcarrier ZF, and the learned and coarse iterates with 0-2
+    Newton-Schulz steps on slots of 50-300 ns, and slots/s of each detector
+    path (graph-replayed FP32 slot: pilot FFT, ZF, uplink FFT, equalize)."""
     import torch
     import megastation_b200 as mb
     from megastation_b200 import datagen, learned
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    cfg = datagen.CellConfig(M=128, K=16, N=2048, S=1200, sg=16, Qm=4, U=13, snr_db=25.0, channel="tdl_ds",
-                             seed=4040)
+    if shape == "256x32":
+        cfg = datagen.CellConfig(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=12, snr_db=25.0, channel="tdl_ds",
+                                 seed=4041)
+        n_default, n_held = 305, 4  # x 3276 subcarriers ~ 1e6 samples
+    else:
+        cfg = datagen.CellConfig(M=128, K=16, N=2048, S=1200, sg=16, Qm=4, U=13, snr_db=25.0, channel="tdl_ds",
+                                 seed=4040)
+        n_default, n_held = 834, 16  # x 1200 subcarriers ~ 1e6 samples
     lz = learned.LearnedZF(cfg.M, cfg.K, cfg.S, cfg.sg)
     net = learned.make_mlp(cfg.sg, seed=1)
-    n_real = int(os.environ.get("MB_LEARNED_REALISATIONS", "834"))  # x 1200 subcarriers ~ 1e6 samples
+    n_real = int(os.environ.get("MB_LEARNED_REALISATIONS", str(n_default)))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    data = learned.training_set(lz, learned.pilot_csi(cfg, n_real, seed=7))
-    held = learned.training_set(lz, learned.pilot_csi(cfg, 16, seed=8))
+    parts = []
+    for i0 in range(0, n_real, 32):  # pilot CSI in chunks (256 x 32: 54 MB per realisation)
+        parts.append(learned.training_set(lz, learned.pilot_csi(cfg, min(32, n_real - i0), seed=7 + 1000 * i0)))
+    data = tuple(torch.cat([p[k] for p in parts]) for k in range(4))
+    del parts
+    held = learned.training_set(lz, learned.pilot_csi(cfg, n_held, seed=8))
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
     t0 = time.perf_counter()
@@ -804,12 +815,14 @@ def run_learned(args):
                        "us_per_slot": 1e3 * e0.elapsed_time(e1) / args.steps}
         del graphs
     mean = lambda n, k: float(np.mean([v[k] for v in quality[n].values()]))
+    wl = ("256x32, N=4096, S=3276, 64-QAM, 25 dB, 8-tap TDL, delay spread 50-300 ns" if shape == "256x32"
+          else "128x16, N=2048, S=1200, 16-QAM, 25 dB, 8-tap TDL, delay spread 50-300 ns")
     line = {"metric": "slots/s (per-subcarrier ZF, learned init + 1 Newton-Schulz step)",
             "value": speed["learned_ns1"]["slots_per_s"], "unit": "slots/s", "n_gpus": 1, "steps": args.steps,
             "warmup": 5, "ms_per_step": speed["learned_ns1"]["us_per_slot"] / 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 detector, bf16 MLP weights",
             "data": "synthetic (seeded, megastation_b200.datagen / learned.pilot_csi)",
-            "config": {"workload": "128x16, N=2048, S=1200, 16-QAM, 25 dB, 8-tap TDL, delay spread 50-300 ns",
+            "config": {"workload": wl,
                        "mlp": "22 -> 256 -> 256 -> 4, ReLU, BF16 weights, FP32 accumulate",
                        "training_realisations": n_real, "training_samples": int(data[0].shape[0]),
                        "steps": steps, "batch": 4096},
@@ -901,7 +914,8 @@ def main():
         return
     if args.workload != "cell256x32":
         if rank == 0:
-            {"cells32": run_cells, "full256x64": run_full, "learned128x16": run_learned}[args.workload](args)
+            {"cells32": run_cells, "full256x64": run_full, "learned128x16": run_learned,
+             "learned256x32": lambda a: run_learned(a, "256x32")}[args.workload](args)
         return
 
     import torch

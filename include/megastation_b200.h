@@ -503,7 +503,9 @@ mb_status mb_mlp_loss_grad(mb_mlp *mlp, const float *x, const float *A, const fl
                            const float *c, uint32_t batch, float *loss, void *stream);
 mb_status mb_mlp_adam_step(mb_mlp *mlp, float lr, void *stream);
 
-/* Per-subcarrier ZF from the comb-pilot CSI [G][M][K] (K <= 32, M K <= 3072):
+/* Per-subcarrier ZF from the comb-pilot CSI [G][M][K] (K <= 32; M K up to
+ * what one subcarrier's FP64 CSI needs in shared memory, M K <= 14336 on a
+ * B200, e.g. 256 x 32):
  * each user's pilots are interpolated linearly along frequency to a CSI
  * estimate c_s [M][K] per subcarrier, G_s is the reference's Gram C C^H of
  * it (C[u][b] = c_s[b][u]), the Grams at the group centres (subcarrier g sg + sg/2) are inverted

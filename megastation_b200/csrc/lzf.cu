@@ -28,6 +28,7 @@
 // alpha + 1 with A_jk = Re tr(Y_j^H Y_k) / ||X*||^2, b_j = Re tr(Y_j^H X*) /
 // ||X*||^2.
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "common.cuh"
@@ -524,10 +525,39 @@ static size_t detect_smem(const mb_lzf *z) {
                                                                      (size_t)z->M * z->K));
 }
 
+// The kernels that stage one subcarrier's M x K CSI in shared memory take
+// up to the device's opt-in limit (raised once per device): 256 x 32 needs
+// 64 KB (FP32 Gram), 88 KB (detector) and 128 KB (FP64 Gram of the targets).
+static mb_status lzf_configure(size_t *limit) {
+  static std::atomic<uint64_t> configured{0};
+  static std::atomic<int> lim[64] = {};
+  int dev = 0, maxs = 0;
+  MB_CUDA_TRY(cudaGetDevice(&dev));
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(configured.load() & bit)) {
+    MB_CUDA_TRY(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    int l = maxs;
+    const void *ks[3] = {(const void *)sub_gram_kernel, (const void *)sub_detect_kernel,
+                         (const void *)gram_kernel<double>};
+    for (const void *k : ks) {
+      cudaFuncAttributes fa;
+      MB_CUDA_TRY(cudaFuncGetAttributes(&fa, k));
+      MB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs - (int)fa.sharedSizeBytes));
+      l = std::min(l, maxs - (int)fa.sharedSizeBytes);
+    }
+    lim[dev & 63].store(l);
+    configured.fetch_or(bit);
+  }
+  *limit = (size_t)lim[dev & 63].load();
+  return MB_OK;
+}
+
 static mb_status lzf_shared_mem_ok(const mb_lzf *z) {
   // one subcarrier's M x K CSI is staged in shared memory (FP64 for targets)
-  return (size_t)z->M * z->K * sizeof(double2) <= 48 * 1024 && detect_smem(z) <= 48 * 1024 ? MB_OK
-                                                                                            : MB_UNSUPPORTED;
+  size_t limit = 0;
+  const mb_status r = lzf_configure(&limit);
+  if (r != MB_OK) return r;
+  return (size_t)z->M * z->K * sizeof(double2) <= limit && detect_smem(z) <= limit ? MB_OK : MB_UNSUPPORTED;
 }
 
 extern "C" mb_status mb_lzf_features(mb_lzf *z, const mb_c32 *csi, float *features, void *stream) {

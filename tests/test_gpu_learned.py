@@ -191,3 +191,19 @@ def test_learned_slot_evm(trained):
     # Newton-Schulz step brings either start to within a tenth of a dB
     assert e[("learned", 0)] < e[("coarse", 0)] - 0.5, e
     assert abs(e[("learned", 1)] - e[("coarse", 1)]) <= 0.1, e
+
+
+def test_lzf_exact_at_headline_shape(mb):
+    """The per-subcarrier path at 256 antennas x 32 users (its CSI staged in
+    shared memory beyond the default 48 KB): exact per-subcarrier ZF against
+    the ZF oracle on the interpolated CSI, for a sample of subcarriers."""
+    from megastation_b200 import datagen, learned
+    cfg = datagen.CellConfig(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=2, snr_db=25.0, channel="tdl_ds",
+                             delay_spread_ns=150.0, seed=21)
+    csi = learned.pilot_csi(cfg, 1, seed=22)[0]
+    lz = learned.LearnedZF(cfg.M, cfg.K, cfg.S, cfg.sg)
+    W = lz.run(csi, init=learned.EXACT, ns_iters=0).cpu().numpy()
+    c = om.interp_csi(csi.cpu().numpy(), cfg.S, cfg.sg)
+    pick = np.arange(0, cfg.S, 97)
+    Wr = orc.zf(c[pick].astype(np.complex64), S=len(pick), sg=1)
+    assert np.abs(W[pick] - Wr).max() <= 2e-3 * np.abs(Wr).max()
