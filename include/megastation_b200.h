@@ -479,6 +479,13 @@ mb_status mb_cells_autotune(mb_cells *cells, const void *const *iq, uint16_t *co
                             uint32_t *sym_batch_out, uint32_t *eq_cols_out,
                             double *us_per_slot);
 mb_status mb_cells_get_tuning(const mb_cells *cells, uint32_t *sym_batch, uint32_t *eq_cols);
+/* The third knob, per cell: the CTAs of each tensor-core FFT launch (cells
+ * with N = 4096 in mixed precision; 0 = one per SM, the default).  A CTA
+ * of that FFT holds a whole SM, so fewer CTAs (each taking more two-row
+ * units) leave SMs to the other cells' kernels; mb_cells_autotune tries
+ * 74, 37 and 18 per class after the other knobs. */
+mb_status mb_cells_get_fft_ctas(const mb_cells *cells, uint32_t *fft_ctas);
+mb_status mb_cells_set_fft_ctas(mb_cells *cells, const uint32_t *fft_ctas);
 mb_status mb_cells_set_tuning(mb_cells *cells, const uint32_t *sym_batch,
                               const uint32_t *eq_cols);
 

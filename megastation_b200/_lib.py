@@ -137,6 +137,8 @@ def _load():
         "mb_cells_autotune": (ST, [VP, VP, VP, VP, U32, VP, ctypes.POINTER(U32), ctypes.POINTER(U32),
                                    ctypes.POINTER(ctypes.c_double)]),
         "mb_cells_get_tuning": (ST, [VP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
+        "mb_cells_get_fft_ctas": (ST, [VP, ctypes.POINTER(U32)]),
+        "mb_cells_set_fft_ctas": (ST, [VP, ctypes.POINTER(U32)]),
         "mb_cells_set_tuning": (ST, [VP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
     }
     for name, (res, args) in sigs.items():

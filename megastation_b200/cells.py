@@ -55,23 +55,28 @@ class Cells:
         return llr, hard
 
     def autotune(self, iqs, reps=20, stream=None):
-        """Picks sym_batch and equalizer columns per CTA per cell class by
-        timing the batched slot; returns (per-cell choices, us per slot)."""
+        """Picks sym_batch, equalizer columns per CTA and the tensor-core
+        FFT's CTAs per launch per cell class by timing the batched slot;
+        returns (per-cell choices, us per slot)."""
         n = len(self.cfgs)
         sb, cols = (ctypes.c_uint32 * n)(), (ctypes.c_uint32 * n)()
         us = ctypes.c_double()
         check(LIB.mb_cells_autotune(self._h, _ptrs(iqs), _ptrs(self.llr), _ptrs(self.hard), reps,
                                     _stream(stream), sb, cols, ctypes.byref(us)), "mb_cells_autotune")
-        return [{"sym_batch": sb[i], "eq_cols": cols[i]} for i in range(n)], us.value
+        return self.tuning(), us.value
 
     def tuning(self):
         n = len(self.cfgs)
-        sb, cols = (ctypes.c_uint32 * n)(), (ctypes.c_uint32 * n)()
+        sb, cols, fc = (ctypes.c_uint32 * n)(), (ctypes.c_uint32 * n)(), (ctypes.c_uint32 * n)()
         check(LIB.mb_cells_get_tuning(self._h, sb, cols), "mb_cells_get_tuning")
-        return [{"sym_batch": sb[i], "eq_cols": cols[i]} for i in range(n)]
+        check(LIB.mb_cells_get_fft_ctas(self._h, fc), "mb_cells_get_fft_ctas")
+        return [{"sym_batch": sb[i], "eq_cols": cols[i], "fft_ctas": fc[i]} for i in range(n)]
 
     def set_tuning(self, choices):
         n = len(self.cfgs)
         sb = (ctypes.c_uint32 * n)(*[c["sym_batch"] for c in choices])
         cols = (ctypes.c_uint32 * n)(*[c["eq_cols"] for c in choices])
         check(LIB.mb_cells_set_tuning(self._h, sb, cols), "mb_cells_set_tuning")
+        if all("fft_ctas" in c for c in choices):
+            fc = (ctypes.c_uint32 * n)(*[c["fft_ctas"] for c in choices])
+            check(LIB.mb_cells_set_fft_ctas(self._h, fc), "mb_cells_set_fft_ctas")

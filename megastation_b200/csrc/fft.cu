@@ -499,12 +499,13 @@ extern "C" mb_status mb_fft_uplink_bf16(mb_fft *f, const void *iq, int iq_dtype,
 }
 
 mb_status mb::fft_uplink_lp(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,
-                            void *y_lp, uint32_t S_pad, cudaStream_t st) {
+                            void *y_lp, uint32_t S_pad, cudaStream_t st, uint32_t max_ctas) {
   if (!f || !iq || !y_lp || !dtype_ok(iq_dtype) || S_pad < f->d.ofdm_num) return MB_BAD_ARG;
   if (fft_tc_lp_supported(f->tc, iq, S_pad, y_lp)) {
     const DeviceTables *tab = device_tables();
-    return fft_tc_uplink_lp(f->tc, iq, iq_dtype, n_sym * f->d.bs_num, f->d.bs_num, f->d.ofdm_num, y_lp, S_pad,
-                            tab ? tab->err : nullptr, st);
+    const uint32_t rows = n_sym * f->d.bs_num;
+    return fft_tc_uplink_lp(f->tc, iq, iq_dtype, rows, f->d.bs_num, f->d.ofdm_num, y_lp, S_pad,
+                            tab ? tab->err : nullptr, st, fft_tc_upc(rows, max_ctas));
   }
   FftParams p{};
   p.in = iq;
@@ -545,12 +546,13 @@ bool mb::fft_slot_tc_ok(mb_fft *f, const void *iq, uint32_t S_pad, const void *y
 }
 
 mb_status mb::fft_slot_tc(mb_fft *f, const void *iq, int iq_dtype, uint32_t P, uint32_t U, mb_c32 *csi,
-                          void *y_lp, uint32_t S_pad, cudaStream_t st) {
+                          void *y_lp, uint32_t S_pad, cudaStream_t st, uint32_t max_ctas) {
   if (!fft_slot_tc_ok(f, iq, S_pad, y_lp) || !dtype_ok(iq_dtype) || !csi) return MB_BAD_ARG;
   const uint32_t S = f->d.ofdm_num, sg = f->d.sc_group, G = (S + sg - 1) / sg;
   const DeviceTables *tab = device_tables();
   return fft_tc_slot(f->tc, iq, iq_dtype, P, U, f->d.bs_num, S, f->d.ue_num, sg, G >= 2 ? S % sg : 0, f->pilot,
-                     reinterpret_cast<float2 *>(csi), y_lp, S_pad, tab ? tab->err : nullptr, st);
+                     reinterpret_cast<float2 *>(csi), y_lp, S_pad, tab ? tab->err : nullptr, st,
+                     fft_tc_upc((uint64_t)(P + U) * f->d.bs_num, max_ctas));
 }
 
 extern "C" mb_status mb_fft_pilot_mixed(mb_fft *f, const void *iq, int iq_dtype, uint32_t n_sym,

@@ -845,7 +845,7 @@ mb_status fft_tc_pilot(const FftTcPlan *pl, const void *iq, int iq_dtype, uint32
 
 mb_status fft_tc_slot(const FftTcPlan *pl, const void *iq, int iq_dtype, uint32_t P, uint32_t U, uint32_t M,
                       uint32_t S, uint32_t K, uint32_t sg, uint32_t tail_rem, const float2 *pilot, float2 *csi,
-                      void *y_lp, uint32_t S_pad, int *err, cudaStream_t st) {
+                      void *y_lp, uint32_t S_pad, int *err, cudaStream_t st, uint32_t upc) {
   if (!fft_tc_lp_supported(pl, iq, S_pad, y_lp) || S > kFtN || S > S_pad || sg == 0 || sg >= kFtN || !pilot ||
       !csi)
     return MB_BAD_ARG;
@@ -866,7 +866,7 @@ mb_status fft_tc_slot(const FftTcPlan *pl, const void *iq, int iq_dtype, uint32_
   p.G = (S + sg - 1) / sg;
   p.sg_magic = (uint32_t)((0x100000000ull + sg - 1) / sg);
   p.err = err;
-  return fft_tc_launch(pl, iq, iq_dtype, p, st, 0);
+  return fft_tc_launch(pl, iq, iq_dtype, p, st, upc);
 }
 
 }  // namespace mb

@@ -36,6 +36,7 @@ struct mb_slot {
   uint32_t S_pad;
   uint32_t sb_cap;    // uplink symbols the y / y_lp buffers hold (>= sym_batch)
   uint32_t eq_cols;   // tensor-core equalizer columns per CTA (0: 128)
+  uint32_t fft_ctas;  // CTAs of each tensor-core FFT launch (0: one per SM)
   float2 *precoded;   // [D][M][N]
   const mb_mlp *zf_net;  // learned initial iterate of the mixed ZF (not owned), or null
   // mixed-precision downlink on the tensor cores (N = 4096): the BF16
@@ -160,6 +161,7 @@ static mb_status slot_create(const mb_cell_desc *cell, bool sb_cap_all, mb_slot 
   s->c.sym_batch = std::min(s->c.sym_batch, std::max<uint32_t>(c.U, 1));
   s->sb_cap = sb_cap_all ? std::max<uint32_t>(c.U, 1) : s->c.sym_batch;
   s->eq_cols = 0;
+  s->fft_ctas = 0;
   s->G = (c.S + c.sg - 1) / c.sg;
   s->n_valid = std::min<uint64_t>((uint64_t)c.S * c.Qm, c.cb_size);
   s->hrow = (s->n_valid + 7) / 8;
@@ -257,7 +259,7 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   // planar BF16 rows for the tensor-core equalizer
   auto fft_batch = [&](uint32_t l0, uint32_t nb, cudaStream_t fs) {
     const void *src = iq_b + (size_t)(c.P + l0) * sym_bytes;
-    return mixed ? fft_uplink_lp(s->fft, src, c.iq_dtype, nb, s->y_lp, s->S_pad, fs)
+    return mixed ? fft_uplink_lp(s->fft, src, c.iq_dtype, nb, s->y_lp, s->S_pad, fs, s->fft_ctas)
                  : mb_fft_uplink(s->fft, src, c.iq_dtype, nb, reinterpret_cast<mb_c32 *>(s->y), fs);
   };
   // Mixed precision at N = 4096: the pilot symbols and the first uplink
@@ -292,7 +294,8 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   }
   if (combined) {
     MARK(mk->fft_b[0]);
-    r = fft_slot_tc(s->fft, iq, c.iq_dtype, c.P, nb0, reinterpret_cast<mb_c32 *>(s->csi), s->y_lp, s->S_pad, cs);
+    r = fft_slot_tc(s->fft, iq, c.iq_dtype, c.P, nb0, reinterpret_cast<mb_c32 *>(s->csi), s->y_lp, s->S_pad, cs,
+                    s->fft_ctas);
     if (r != MB_OK) return r;
     MARK(mk->fft_e[0]);
   }
@@ -663,6 +666,19 @@ extern "C" mb_status mb_cells_set_tuning(mb_cells *cs, const uint32_t *sym_batch
   return MB_OK;
 }
 
+extern "C" mb_status mb_cells_get_fft_ctas(const mb_cells *cs, uint32_t *fft_ctas) {
+  if (!cs || !fft_ctas) return MB_BAD_ARG;
+  for (size_t c = 0; c < cs->slots.size(); c++) fft_ctas[c] = cs->slots[c]->fft_ctas;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_cells_set_fft_ctas(mb_cells *cs, const uint32_t *fft_ctas) {
+  if (!cs || !fft_ctas) return MB_BAD_ARG;
+  for (size_t c = 0; c < cs->slots.size(); c++) cs->slots[c]->fft_ctas = fft_ctas[c];
+  cells_drop_graphs(cs);  // the captured launches change
+  return MB_OK;
+}
+
 // microseconds per slot of the current tuning: warm-up, then reps graph
 // launches timed with CUDA events on st
 static mb_status cells_time(mb_cells *cs, const void *const *iq, uint16_t *const *llr,
@@ -695,13 +711,18 @@ static mb_status cells_time(mb_cells *cs, const void *const *iq, uint16_t *const
 }
 
 // Autotuner: the knobs are, per cell, the uplink symbols per FFT/equalize
-// batch (sym_batch) and the tensor-core equalizer's (symbol, subcarrier)
-// columns per CTA (its MMA tile).  Cells of one shape form a class and share
-// a choice; classes are visited by decreasing work, each trying its
-// candidates with the others fixed (coordinate descent on the measured time
-// of the whole batched slot) and keeping a candidate only if it is at least
-// 1% faster.  The tuning stays on the object (later mb_cells_uplink calls
-// use it) and is returned per cell.
+// batch (sym_batch), the tensor-core equalizer's (symbol, subcarrier)
+// columns per CTA (its MMA tile) and, for cells whose FFT runs on the tensor
+// cores (mixed, N = 4096), the CTAs of each FFT launch: one CTA holds a whole
+// SM, so a cell's FFT on every SM keeps the other cells' kernels waiting,
+// while fewer CTAs with more two-row units each let the cells' FFTs and
+// solves share the GPU.  Cells of one shape form a class and share a choice;
+// classes are visited by decreasing work, each trying its candidates with
+// the others fixed (coordinate descent on the measured time of the whole
+// batched slot, first over (sym_batch, eq_cols), then over the FFT's CTAs)
+// and keeping a candidate only if it is at least 1% faster.  The tuning
+// stays on the object (later mb_cells_uplink calls use it) and is returned
+// per cell.
 extern "C" mb_status mb_cells_autotune(mb_cells *cs, const void *const *iq, uint16_t *const *llr,
                                        uint8_t *const *hard, uint32_t reps, void *stream,
                                        uint32_t *sym_batch_out, uint32_t *eq_cols_out,
@@ -781,6 +802,28 @@ extern "C" mb_status mb_cells_autotune(mb_cells *cs, const void *const *iq, uint
     }
   }
   if (r == MB_OK) r = mb_cells_set_tuning(cs, sb.data(), cols.data());
+  // the tensor-core FFT's CTAs per launch
+  std::vector<uint32_t> fc(n, 0);
+  if (r == MB_OK) r = mb_cells_set_fft_ctas(cs, fc.data());
+  for (uint32_t k : order) {
+    if (r != MB_OK) break;
+    const mb_cell_desc &d = cs->slots[members[k][0]]->c;
+    if (d.zf_precision != MB_ZF_MIXED || d.N != 4096) continue;
+    uint32_t cur = 0;
+    for (uint32_t cand : {74u, 37u, 18u}) {
+      for (uint32_t c : members[k]) fc[c] = cand;
+      double t = 0.0;
+      r = mb_cells_set_fft_ctas(cs, fc.data());
+      if (r == MB_OK) r = cells_time(cs, iq, llr, hard, reps, st, &t);
+      if (r != MB_OK) break;
+      if (t < 0.99 * best) {
+        best = t;
+        cur = cand;
+      }
+    }
+    for (uint32_t c : members[k]) fc[c] = cur;
+  }
+  if (r == MB_OK) r = mb_cells_set_fft_ctas(cs, fc.data());
   if (r != MB_OK) return r;
   if (sym_batch_out) std::copy(sb.begin(), sb.end(), sym_batch_out);
   if (eq_cols_out) std::copy(cols.begin(), cols.end(), eq_cols_out);

@@ -61,9 +61,12 @@ def test_cells_autotune_keeps_results(cells_data):
     for c, cfg in enumerate(cfgs):
         assert 1 <= choice[c]["sym_batch"] <= max(cfg.U, 1)
         assert choice[c]["eq_cols"] in (64, 128)
+        assert choice[c]["fft_ctas"] in (0, 74, 37, 18)
         assert torch.equal(llr[c], ref[c][0]) and torch.equal(hard[c], ref[c][1]), c
-    # a hand-set tuning (smallest batches, narrow tiles) gives the same bits
-    cs.set_tuning([{"sym_batch": 1, "eq_cols": 64} for _ in cfgs])
+    # a hand-set tuning (smallest batches, narrow tiles, tensor-core FFTs on
+    # 18 CTAs) gives the same bits
+    cs.set_tuning([{"sym_batch": 1, "eq_cols": 64, "fft_ctas": 18} for _ in cfgs])
+    assert all(t["fft_ctas"] == 18 for t in cs.tuning())
     with torch.cuda.stream(s):
         llr, hard = cs(iqs, stream=s)
     s.synchronize()
