@@ -779,7 +779,12 @@ def run_learned(args, shape="128x16"):
             seq = np.broadcast_to(d["seq"], d["bits"].shape)[..., :n_valid]
             bits = (lr < 0).astype(np.uint8) ^ seq
             ber = float(np.mean(bits != d["bits"][..., :n_valid]))
-            quality.setdefault(name, {})[f"{int(ds)}ns"] = {"evm_db": float(evm), "ber": ber}
+            q = {"evm_db": float(evm), "ber": ber}
+            if name not in ("group_zf", "exact") and ns > 0:
+                # subcarriers whose start was too far off for Newton-Schulz
+                # (the exact inverse taken instead)
+                q["exact_fallback"] = float((lz.flags() == 2).float().mean())
+            quality.setdefault(name, {})[f"{int(ds)}ns"] = q
 
     # throughput of each detector path, graph-replayed on device-resident slots
     R = 2

@@ -537,6 +537,11 @@ mb_status mb_lzf_features(mb_lzf *lzf, const mb_c32 *csi, float *features, void 
 mb_status mb_lzf_targets(mb_lzf *lzf, const mb_c32 *csi, float *A, float *b, void *stream);
 mb_status mb_lzf_run(mb_lzf *lzf, const mb_c32 *csi, mb_mlp *mlp, int init, uint32_t ns_iters,
                      mb_c32 *W, void *stream);
+/* Per subcarrier of the last run, flags [S] (device): 0 = Newton-Schulz
+ * from the chosen start, 1 = the Gram was not positive definite, 2 = the
+ * start was too far off for Newton-Schulz to converge (||I - G_s X0||_F >= 1)
+ * and the exact inverse was taken instead. */
+mb_status mb_lzf_flags(mb_lzf *lzf, int32_t *flags, void *stream);
 /* ||I - G_s X_s||_F per subcarrier of the last run, res [S] (device) */
 mb_status mb_lzf_residual(mb_lzf *lzf, float *res, void *stream);
 

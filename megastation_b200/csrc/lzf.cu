@@ -390,15 +390,43 @@ __global__ void sub_detect_kernel(const float2 *csi, const int *ig, const float 
       x[e] = acc;
     }
   }
+  __shared__ float e0sq;  // ||I - G X0||_F^2 of the initial iterate
+  if (threadIdx.x == 0) {
+    e0sq = 0.f;
+    if (mode != 2 && flag) flag[s] = 0;
+  }
   __syncthreads();
   for (uint32_t it = 0; it < iters; it++) {
+    float part = 0.f;
     for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x) {
       const uint32_t r = e / K, q = e % K;
       float2 acc = make_float2(0.f, 0.f);
       for (uint32_t k = 0; k < K; k++) acc = cfma(g[r * K + k], x[k * K + q], acc);
       t[e] = make_float2((r == q ? 2.f : 0.f) - acc.x, -acc.y);
+      const float ex = (r == q ? 1.f : 0.f) - acc.x;
+      part += ex * ex + acc.y * acc.y;
+    }
+    if (it == 0 && mode != 2) {
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if ((threadIdx.x & 31) == 0) atomicAdd(&e0sq, part);
     }
     __syncthreads();
+    if (it == 0 && mode != 2 && !(e0sq < 1.f)) {
+      // Newton-Schulz converges only from ||I - G X0|| < 1: a start further
+      // off (the blend of neighbouring groups' inverses under a channel that
+      // changes too fast across the band) takes the exact inverse instead,
+      // flagged 2 (uniform: every thread read the same sum)
+      for (uint32_t e = threadIdx.x; e < 2 * KK; e += blockDim.x) {
+        const uint32_t r = e / (2 * K), q = e % (2 * K);
+        aug[e] = q < K ? g[r * K + q] : make_float2(q - K == r ? 1.f : 0.f, 0.f);
+      }
+      __syncthreads();
+      const bool ok = gj_smem<float2, float>(aug, K, &bad);
+      if (threadIdx.x == 0 && flag) flag[s] = ok ? 2 : 1;
+      for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x) x[e] = aug[(e / K) * 2 * K + K + e % K];
+      __syncthreads();
+      break;
+    }
     float2 nx[4];
     uint32_t n = 0;
     for (uint32_t e = threadIdx.x; e < KK; e += blockDim.x, n++) {
@@ -591,6 +619,12 @@ extern "C" mb_status mb_lzf_run(mb_lzf *z, const mb_c32 *csi, mb_mlp *mlp, int i
                                           init == MB_LZF_LEARNED ? z->alpha : nullptr, init, ns_iters, z->X,
                                           reinterpret_cast<float2 *>(W), M, K, z->sg, z->G, z->flag);
   MB_CUDA_TRY(cudaGetLastError());
+  return MB_OK;
+}
+
+extern "C" mb_status mb_lzf_flags(mb_lzf *z, int32_t *flags, void *stream) {
+  if (!z || !flags) return MB_BAD_ARG;
+  MB_CUDA_TRY(cudaMemcpyAsync(flags, z->flag, sizeof(int) * z->S, cudaMemcpyDeviceToDevice, as_stream(stream)));
   return MB_OK;
 }
 

@@ -127,6 +127,14 @@ class LearnedZF:
                              init, ns_iters, _dev(W, "W"), _stream(stream)), "mb_lzf_run")
         return W
 
+    def flags(self, out=None, stream=None):
+        """Per subcarrier of the last run: 0 Newton-Schulz from the chosen
+        start, 1 not positive definite, 2 start too far off (exact inverse
+        taken instead)."""
+        out = torch.empty(self.S, dtype=torch.int32, device="cuda") if out is None else out
+        check(LIB.mb_lzf_flags(self._h, _dev(out, "flags"), _stream(stream)), "mb_lzf_flags")
+        return out
+
     def residual(self, out=None, stream=None):
         out = torch.empty(self.S, dtype=torch.float32, device="cuda") if out is None else out
         check(LIB.mb_lzf_residual(self._h, _dev(out, "res"), _stream(stream)), "mb_lzf_residual")
