@@ -207,3 +207,26 @@ def test_lzf_exact_at_headline_shape(mb):
     pick = np.arange(0, cfg.S, 97)
     Wr = orc.zf(c[pick].astype(np.complex64), S=len(pick), sg=1)
     assert np.abs(W[pick] - Wr).max() <= 2e-3 * np.abs(Wr).max()
+
+
+def test_lzf_far_start_takes_exact_inverse(mb):
+    """On a channel that changes fast across the band (256 x 32, 300 ns), the
+    group-centre start of many subcarriers is too far off for Newton-Schulz
+    (||I - G X0||_F >= 1): those subcarriers are flagged 2 and take the exact
+    inverse, so the iteration never diverges; the others converge."""
+    from megastation_b200 import datagen, learned
+    cfg = datagen.CellConfig(M=256, K=32, N=4096, S=3276, sg=16, Qm=6, U=2, snr_db=25.0, channel="tdl_ds",
+                             delay_spread_ns=300.0, seed=23)
+    csi = learned.pilot_csi(cfg, 1, seed=24, delay_spread_ns=(300.0, 300.0))[0]
+    lz = learned.LearnedZF(cfg.M, cfg.K, cfg.S, cfg.sg)
+    W_ex = lz.run(csi, init=learned.EXACT, ns_iters=0).clone()
+    W = lz.run(csi, init=learned.COARSE, ns_iters=2)
+    fl = lz.flags().cpu().numpy()
+    res = lz.residual().cpu().numpy()
+    torch.cuda.synchronize()
+    assert np.isin(fl, (0, 2)).all()
+    assert (fl == 2).any()
+    assert np.isfinite(res).all() and res.max() < 1.0
+    far = np.nonzero(fl == 2)[0]
+    Wn, We = W.cpu().numpy(), W_ex.cpu().numpy()
+    assert np.abs(Wn[far] - We[far]).max() <= 1e-5 * np.abs(We).max()
