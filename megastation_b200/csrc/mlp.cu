@@ -1,8 +1,9 @@
-// mlp.cu -- the network of the learned ZF initialiser: a 3-layer MLP
+// mlp.cu -- the network of the learned ZF initialisers: a 3-layer MLP
 // (n_in -> width -> width -> n_out, ReLU after the first two layers) with
-// FP32 master weights, BF16 copies of the weights for every product and FP32
-// accumulation, trained by the project's own forward, backward and Adam
-// kernels.  No counterpart in the reference.
+// FP32 master weights; every product takes BF16 weights and BF16
+// activations (or upstream gradients) with FP32 accumulation, the training
+// products on the tensor cores (tcgen05.mma), trained by the project's own
+// forward, backward and Adam kernels.  No counterpart in the reference.
 //
 // The training loss is the quadratic form the initialiser needs: each sample
 // carries a symmetric O x O matrix A, a vector b and a scalar c, and for the
@@ -23,82 +24,204 @@
 namespace mb {
 namespace {
 
-constexpr int kTM = 64, kTN = 64, kTK = 16, kGT = 256;
+// the activations enter every product as BF16, like the weights
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 __device__ __forceinline__ float ldf(const float *p, size_t i) { return p[i]; }
 __device__ __forceinline__ float ldf(const __nv_bfloat16 *p, size_t i) { return __bfloat162float(p[i]); }
 
-// C(m, n) = sum_k A(m, k) B(k, n) with A(m, k) = TRA ? A[k lda + m] : A[m lda + k]
-// and B(k, n) = TRB ? B[n ldb + k] : B[k ldb + n]; epilogue: + bias[n], then
-// optionally times (mask(m, n) > 0) (the ReLU derivative), or ReLU with the
-// pre-activation kept in zout; accumulate adds to C.  64 x 64 tiles, each
-// thread 4 x 4 outputs.
-template <typename TA, typename TB, bool TRA, bool TRB>
-__global__ void __launch_bounds__(kGT) gemm_kernel(int M, int N, int K, const TA *A, int lda,
-                                                   const TB *B, int ldb, float *C, int ldc,
-                                                   const float *bias, const float *mask,
-                                                   float *zout, int relu, int accumulate) {
-  __shared__ float As[kTK][kTM + 4];
-  __shared__ float Bs[kTK][kTN + 4];
-  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
-  float acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += kTK) {
-    for (int e = tid; e < kTM * kTK; e += kGT) {
-      // consecutive threads read consecutive memory in either layout
-      const int mm = TRA ? e % kTM : e / kTK, kk = TRA ? e / kTM : e % kTK;
-      const int m = m0 + mm, k = k0 + kk;
-      As[kk][mm] = (m < M && k < K) ? ldf(A, TRA ? (size_t)k * lda + m : (size_t)m * lda + k) : 0.f;
-    }
-    for (int e = tid; e < kTK * kTN; e += kGT) {
-      const int nn = TRB ? e / kTK : e % kTN, kk = TRB ? e % kTK : e / kTN;
-      const int n = n0 + nn, k = k0 + kk;
-      Bs[kk][nn] = (n < N && k < K) ? ldf(B, TRB ? (size_t)n * ldb + k : (size_t)k * ldb + n) : 0.f;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kTK; kk++) {
-      float a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
-      if (m >= M || n >= N) continue;
-      const size_t o = (size_t)m * ldc + n;
-      float v = acc[i][j] + (bias ? bias[n] : 0.f);
-      if (mask && !(mask[o] > 0.f)) v = 0.f;
-      if (relu) {
-        if (zout) zout[o] = v;
-        v = fmaxf(v, 0.f);
-      }
-      C[o] = accumulate ? C[o] + v : v;
-    }
+// Every product of the network runs on the tensor cores (tcgen05.mma,
+// kind::f16): BF16 operands, FP32 accumulation in tensor memory.
+//   C(m, n) = sum_k A(m, k) B(k, n), A(m, k) = TRA ? A[k lda + m] : A[m lda + k],
+//   B(k, n) = TRB ? B[n ldb + k] : B[k ldb + n]
+// A CTA of 128 threads owns a 128 x NT tile of C (NT = 64, 128 or 256) over
+// the k range of its split; the threads convert 64-wide k chunks of A and B
+// to BF16 and store them in the K-major canonical layout (8-row groups 1024 B
+// apart, 8-element k chunks 128 B apart), two stages deep, and thread 0
+// issues the four K = 16 MMAs of each chunk.  Thread t then reads row t of
+// the tile from TMEM lane t.  Epilogue as the network needs it: + bias[n],
+// then times (mask(m, n) > 0) (the ReLU derivative), or ReLU with the
+// pre-activation kept in zout; accumulate adds to C.  With split-K the
+// splits write their partial sums to `partial` [split][M][N] and a second
+// kernel adds them in a fixed order and applies the epilogue
+// (deterministic).
+constexpr int kGM = 128, kGK = 64, kGThreads = 128;
+
+__device__ __forceinline__ uint32_t gkmaj(uint32_t row, uint32_t kk) {
+  return (row / 8) * 1024 + (kk / 8) * 128 + (row % 8) * 16 + (kk % 8) * 2;
 }
 
+// rows x 64 k chunk of a BF16 operand into shared memory: element (row, k)
+// of the source at trans ? src[k ld + row] : src[row ld + k], zero outside
+// [0, nrow) x [0, nk).  Consecutive threads take consecutive rows of one
+// 8-element k chunk: their 16-byte stores fill whole 128-byte core-matrix
+// rows (no bank conflicts), and their loads are coalesced across threads
+// (row-contiguous source) or a whole 32-byte sector each (k-contiguous).
+template <typename T>
+__device__ __forceinline__ void load_chunk(uint8_t *dst, const T *src, int ld, int trans, int row0, int nrow,
+                                           int k0, int nk, int rows) {
+  const int chunks = rows * (kGK / 8);
+  for (int e = threadIdx.x; e < chunks; e += kGThreads) {
+    const int r = e % rows, kc = e / rows;
+    const int gr = row0 + r, gk = k0 + kc * 8;
+    float v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const bool in = gr < nrow && gk + j < nk;
+      v[j] = in ? ldf(src, trans ? (size_t)(gk + j) * ld + gr : (size_t)gr * ld + gk + j) : 0.f;
+    }
+    uint32_t w[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+      w[j] = *reinterpret_cast<const uint32_t *>(&h);
+    }
+    *reinterpret_cast<uint4 *>(dst + gkmaj(r, kc * 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+__device__ __forceinline__ float epi(float v, int m, int n, int ldc, float *C, const float *bias, const float *mask,
+                                     float *zout, int relu, int accumulate) {
+  const size_t o = (size_t)m * ldc + n;
+  v += bias ? bias[n] : 0.f;
+  if (mask && !(mask[o] > 0.f)) v = 0.f;
+  if (relu) {
+    if (zout) zout[o] = v;
+    v = fmaxf(v, 0.f);
+  }
+  return accumulate ? C[o] + v : v;
+}
+
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kGThreads) gemm_tc_kernel(int M, int N, int K, const TA *A, int lda, int tra,
+                                                            const TB *B, int ldb, int trb, float *C, int ldc,
+                                                            const float *bias, const float *mask, float *zout,
+                                                            int relu, int accumulate, int NT, int k_split,
+                                                            float *partial, int *err) {
+  extern __shared__ __align__(1024) uint8_t gsm[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid / 32;
+  const int n0 = blockIdx.x * NT, m0 = blockIdx.y * kGM;
+  const int kb = blockIdx.z * k_split, ke = min(K, kb + k_split);
+  const uint32_t a_bytes = kGM * kGK * 2, b_bytes = (uint32_t)NT * kGK * 2;
+  uint8_t *stage[2] = {gsm, gsm + a_bytes + b_bytes};
+  if (tid == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_slot, (uint32_t)NT);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t idesc = tc::idesc_bf16(kGM, (uint32_t)NT, false, false);
+  const int nchunks = (ke - kb + kGK - 1) / kGK;
+  bool ok = true;
+  for (int c = 0; c < nchunks; c++) {
+    const int s = c & 1;
+    // the stage's previous chunk (c - 2) must have been multiplied
+    if (c >= 2 && !tc::mbar_wait(&bar[s], ((c - 2) >> 1) & 1)) ok = false;
+    if (__syncthreads_or(!ok)) break;
+    // A's rows are m: A(m, k) sits at A[k lda + m] exactly when TRA; B's
+    // rows are n: B(k, n) sits at B[k ldb + n] exactly when not TRB
+    load_chunk(stage[s], A, lda, tra, m0, M, kb + c * kGK, ke, kGM);
+    load_chunk(stage[s] + a_bytes, B, ldb, !trb, n0, N, kb + c * kGK, ke, NT);
+    tc::fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint32_t a0 = tc::smem_u32(stage[s]), b0 = a0 + a_bytes;
+#pragma unroll
+      for (int ks = 0; ks < kGK / 16; ks++)
+        tc::mma_f16(tmem, tc::smem_desc(a0 + ks * 256, 128, 1024), tc::smem_desc(b0 + ks * 256, 128, 1024), idesc,
+                    (c | ks) != 0);
+      tc::mma_commit(&bar[s]);
+    }
+  }
+  // the last chunk's commit covers every MMA issued before it
+  if (ok && nchunks > 0 && !tc::mbar_wait(&bar[(nchunks - 1) & 1], ((nchunks - 1) >> 1) & 1)) ok = false;
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0 && err) atomicOr(err, tc::kErrTimeout);
+  } else {
+    tc::fence_after_sync();
+    const int m = m0 + tid;
+    for (int c16 = 0; c16 < NT / 16; c16++) {
+      float v[16];
+      if (nchunks > 0) {
+        tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c16 * 16, v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] = 0.f;
+      }
+      if (m >= M) continue;
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int n = n0 + c16 * 16 + j;
+        if (n >= N) break;
+        if (partial)
+          partial[((size_t)blockIdx.z * M + m) * N + n] = v[j];
+        else
+          C[(size_t)m * ldc + n] = epi(v[j], m, n, ldc, C, bias, mask, zout, relu, accumulate);
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, (uint32_t)NT);
+}
+
+// C = epilogue(sum over the splits of partial[s][M][N]), in split order
+__global__ void splitk_reduce_kernel(int M, int N, int splits, const float *partial, float *C, int ldc,
+                                     const float *bias, const float *mask, float *zout, int relu, int accumulate) {
+  const size_t total = (size_t)M * N;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    float v = 0.f;
+    for (int s = 0; s < splits; s++) v += partial[(size_t)s * total + e];
+    const int m = (int)(e / N), n = (int)(e % N);
+    C[(size_t)m * ldc + n] = epi(v, m, n, ldc, C, bias, mask, zout, relu, accumulate);
+  }
+}
+
+constexpr int kMaxSplits = 16;
+
+// the host side of one product; partial: split-K scratch of kMaxSplits * M * N
+// floats (nullable: no split-K)
 template <typename TA, typename TB, bool TRA, bool TRB>
 cudaError_t gemm(int M, int N, int K, const TA *A, int lda, const TB *B, int ldb, float *C, int ldc,
-                 const float *bias, const float *mask, float *zout, int relu, int accumulate,
-                 cudaStream_t st) {
+                 const float *bias, const float *mask, float *zout, int relu, int accumulate, cudaStream_t st,
+                 float *partial = nullptr, int *err = nullptr) {
   if (M <= 0 || N <= 0) return cudaSuccess;
-  const dim3 grid((N + kTN - 1) / kTN, (M + kTM - 1) / kTM);
-  gemm_kernel<TA, TB, TRA, TRB><<<grid, kGT, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, mask,
-                                                     zout, relu, accumulate);
+  const int NT = N <= 64 ? 64 : N <= 128 ? 128 : 256;
+  const size_t smem = 2 * ((size_t)kGM * kGK * 2 + (size_t)NT * kGK * 2);
+  static std::atomic<uint64_t> configured{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(configured.load() & bit)) {
+    e = cudaFuncSetAttribute(gemm_tc_kernel<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(2 * ((size_t)kGM * kGK * 2 + 256 * kGK * 2)));
+    if (e != cudaSuccess) return e;
+    configured.fetch_or(bit);
+  }
+  const int gx = (N + NT - 1) / NT, gy = (M + kGM - 1) / kGM;
+  // few output tiles over a long reduction (the weight gradients: K is the
+  // batch): split K so that the launch fills the GPU
+  int splits = 1;
+  if (partial && gx * gy < 32 && K >= 4 * kGK)
+    splits = std::min(kMaxSplits, std::max(1, K / (4 * kGK)));
+  const int k_split = ((K + splits - 1) / splits + kGK - 1) / kGK * kGK;
+  splits = std::max(1, (K + k_split - 1) / k_split);
+  gemm_tc_kernel<TA, TB><<<dim3(gx, gy, splits), kGThreads, smem, st>>>(
+      M, N, K, A, lda, TRA ? 1 : 0, B, ldb, TRB ? 1 : 0, C, ldc, bias, mask, zout, relu, accumulate, NT, k_split,
+      splits > 1 ? partial : nullptr, err);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || splits == 1) return e;
+  const size_t total = (size_t)M * N;
+  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 8);
+  splitk_reduce_kernel<<<blocks, 256, 0, st>>>(M, N, splits, partial, C, ldc, bias, mask, zout, relu, accumulate);
   return cudaGetLastError();
 }
 
@@ -162,7 +285,7 @@ __global__ void __launch_bounds__(256) mlp_infer_kernel(const float *x, int B, i
   const int r0 = blockIdx.x * ROWS, nr = min(ROWS, B - r0);
   for (int e = threadIdx.x; e < ROWS * I; e += blockDim.x) {
     const int r = e / I;
-    a0[e] = r < nr ? x[(size_t)(r0 + r) * I + e % I] : 0.f;
+    a0[e] = r < nr ? bf16r(x[(size_t)(r0 + r) * I + e % I]) : 0.f;
   }
   __syncthreads();
   // hidden layers: relu(a W + b)
@@ -205,7 +328,7 @@ __global__ void __launch_bounds__(256) mlp_infer_kernel(const float *x, int B, i
         }
       }
 #pragma unroll
-      for (int r = 0; r < ROWS; r++) aout[r * W + n] = fmaxf(acc[r], 0.f);
+      for (int r = 0; r < ROWS; r++) aout[r * W + n] = bf16r(fmaxf(acc[r], 0.f));
     }
     __syncthreads();
   }
@@ -263,7 +386,7 @@ __global__ void __launch_bounds__(256) mlp_infer_smem_kernel(const float *x, int
     const int nr = min(ROWS, B - r0);
     for (int e = threadIdx.x; e < ROWS * I; e += blockDim.x) {
       const int r = e / I;
-      a0[e] = r < nr ? x[(size_t)(r0 + r) * I + e % I] : 0.f;
+      a0[e] = r < nr ? bf16r(x[(size_t)(r0 + r) * I + e % I]) : 0.f;
     }
     __syncthreads();
     for (int layer = 0; layer < 2; layer++) {
@@ -300,7 +423,7 @@ __global__ void __launch_bounds__(256) mlp_infer_smem_kernel(const float *x, int
           for (int r = 0; r < ROWS; r++) acc[r] = fmaf(ain[r * K + k], w, acc[r]);
         }
 #pragma unroll
-        for (int r = 0; r < ROWS; r++) aout[r * W + n] = fmaxf(acc[r], 0.f);
+        for (int r = 0; r < ROWS; r++) aout[r * W + n] = bf16r(fmaxf(acc[r], 0.f));
       }
       __syncthreads();
     }
@@ -332,6 +455,7 @@ struct mb_mlp {
   float *p, *g, *m, *v;        // params, grads, Adam moments
   __nv_bfloat16 *wb;           // BF16 copies of p (all entries; only W* are read)
   float *z1, *h1, *z2, *h2, *y, *dy, *d2, *d1;  // activations and their gradients
+  float *part;                 // split-K partial sums of the weight gradients
   uint32_t step;
 };
 
@@ -345,7 +469,7 @@ extern "C" mb_status mb_mlp_destroy(mb_mlp *n) {
   if (!n) return MB_BAD_ARG;
   for (void *q : {(void *)n->p, (void *)n->g, (void *)n->m, (void *)n->v, (void *)n->wb,
                   (void *)n->z1, (void *)n->h1, (void *)n->z2, (void *)n->h2, (void *)n->y,
-                  (void *)n->dy, (void *)n->d2, (void *)n->d1})
+                  (void *)n->dy, (void *)n->d2, (void *)n->d1, (void *)n->part})
     cudaFree(q);
   delete n;
   return MB_OK;
@@ -392,6 +516,7 @@ extern "C" mb_status mb_mlp_create(uint32_t n_in, uint32_t width, uint32_t n_out
   alloc((void **)&n->d1, BW);
   alloc((void **)&n->y, sizeof(float) * (size_t)max_batch * n_out);
   alloc((void **)&n->dy, sizeof(float) * (size_t)max_batch * n_out);
+  alloc((void **)&n->part, sizeof(float) * kMaxSplits * (size_t)std::max(n_in, width) * std::max(width, n_out));
   if (st == MB_OK) {
     // He-normal hidden layers; the output layer starts at zero weights so the
     // untrained network returns its bias (set by the caller)
@@ -451,14 +576,15 @@ extern "C" mb_status mb_mlp_set_params(mb_mlp *n, const float *host) {
 static cudaError_t mlp_fwd(mb_mlp *n, const float *x, uint32_t B, float *y, cudaStream_t st) {
   const int I = n->n_in, W = n->width, O = n->n_out;
   const __nv_bfloat16 *wb = n->wb;
+  int *err = device_tables() ? device_tables()->err : nullptr;
   cudaError_t e = gemm<float, __nv_bfloat16, false, false>(B, W, I, x, I, wb + n->off[0], W, n->h1, W,
-                                                          n->p + n->off[1], nullptr, n->z1, 1, 0, st);
+                                                          n->p + n->off[1], nullptr, n->z1, 1, 0, st, nullptr, err);
   if (e == cudaSuccess)
     e = gemm<float, __nv_bfloat16, false, false>(B, W, W, n->h1, W, wb + n->off[2], W, n->h2, W,
-                                                n->p + n->off[3], nullptr, n->z2, 1, 0, st);
+                                                n->p + n->off[3], nullptr, n->z2, 1, 0, st, nullptr, err);
   if (e == cudaSuccess)
     e = gemm<float, __nv_bfloat16, false, false>(B, O, W, n->h2, W, wb + n->off[4], O, y, O,
-                                                n->p + n->off[5], nullptr, nullptr, 0, 0, st);
+                                                n->p + n->off[5], nullptr, nullptr, 0, 0, st, nullptr, err);
   return e;
 }
 
@@ -520,21 +646,22 @@ extern "C" mb_status mb_mlp_loss_grad(mb_mlp *n, const float *x, const float *A,
   if (loss) MB_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(float), st));
   quad_loss_kernel<<<(B + 255) / 256, 256, 0, st>>>(n->y, A, b, c, B, O, n->dy, loss);
   MB_CUDA_TRY(cudaGetLastError());
+  int *err = device_tables() ? device_tables()->err : nullptr;
   // layer 3: dW3 = H2^T dY, db3 = colsum dY, dH2 = (dY W3^T) * relu'(Z2)
   MB_CUDA_TRY((gemm<float, float, true, false>(W, O, B, n->h2, W, n->dy, O, g + n->off[4], O, nullptr,
-                                               nullptr, nullptr, 0, 0, st)));
+                                               nullptr, nullptr, 0, 0, st, n->part, err)));
   colsum_kernel<<<(O + 255) / 256, 256, 0, st>>>(n->dy, B, O, g + n->off[5]);
   MB_CUDA_TRY((gemm<float, __nv_bfloat16, false, true>(B, W, O, n->dy, O, wb + n->off[4], O, n->d2, W,
-                                                       nullptr, n->z2, nullptr, 0, 0, st)));
+                                                       nullptr, n->z2, nullptr, 0, 0, st, nullptr, err)));
   // layer 2
   MB_CUDA_TRY((gemm<float, float, true, false>(W, W, B, n->h1, W, n->d2, W, g + n->off[2], W, nullptr,
-                                               nullptr, nullptr, 0, 0, st)));
+                                               nullptr, nullptr, 0, 0, st, n->part, err)));
   colsum_kernel<<<(W + 255) / 256, 256, 0, st>>>(n->d2, B, W, g + n->off[3]);
   MB_CUDA_TRY((gemm<float, __nv_bfloat16, false, true>(B, W, W, n->d2, W, wb + n->off[2], W, n->d1, W,
-                                                       nullptr, n->z1, nullptr, 0, 0, st)));
+                                                       nullptr, n->z1, nullptr, 0, 0, st, nullptr, err)));
   // layer 1
   MB_CUDA_TRY((gemm<float, float, true, false>(I, W, B, x, I, n->d1, W, g + n->off[0], W, nullptr,
-                                               nullptr, nullptr, 0, 0, st)));
+                                               nullptr, nullptr, 0, 0, st, n->part, err)));
   colsum_kernel<<<(W + 255) / 256, 256, 0, st>>>(n->d1, B, W, g + n->off[1]);
   MB_CUDA_TRY(cudaGetLastError());
   return MB_OK;

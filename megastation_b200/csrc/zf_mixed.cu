@@ -290,8 +290,9 @@ __device__ __forceinline__ void block_reduce5(float &a, float &b, float &c, floa
 // the iterate is accepted when the last one is at most kPolyAccept = 0.04
 // (the returned X then has ||I - G X||_F <= 1.6e-3, below the BF16 rounding
 // of the detector image), otherwise the caller falls back to the exact
-// inverse.  The network: BF16 weights, FP32 activations and accumulation,
-// ReLU hidden layers (the arithmetic of mb_mlp_forward).  Result in Xs.
+// inverse.  The network: BF16 weights and activations into every product,
+// FP32 accumulation, ReLU hidden layers (the arithmetic of mb_mlp_forward).
+// Result in Xs.
 template <int MM>
 __device__ bool poly_init(const float2 *Gs, uint32_t ld, float2 *Xs, float2 *P2, float2 *P3, float2 *Ts,
                           float2 *Xn, uint32_t K, uint32_t M, const ZfNetView &net, uint32_t ns_iters,
@@ -336,17 +337,20 @@ __device__ bool poly_init(const float2 *Gs, uint32_t ld, float2 *Xs, float2 *P2,
   }
   __syncthreads();
   const uint32_t W = net.width;
+  // features and hidden activations enter each product as BF16, like the
+  // weights (the network's arithmetic everywhere, mlp.cu)
+  auto bf = [](float x) { return __bfloat162float(__float2bfloat16_rn(x)); };
   if ((uint32_t)tid < W) {
     float h = net.b1[tid];
 #pragma unroll
-    for (uint32_t k = 0; k < kZfInitFeatures; k++) h = fmaf(coef[k], __bfloat162float(net.w1[k * W + tid]), h);
-    act[tid] = fmaxf(h, 0.f);
+    for (uint32_t k = 0; k < kZfInitFeatures; k++) h = fmaf(bf(coef[k]), __bfloat162float(net.w1[k * W + tid]), h);
+    act[tid] = bf(fmaxf(h, 0.f));
   }
   __syncthreads();
   if ((uint32_t)tid < W) {
     float h = net.b2[tid];
     for (uint32_t k = 0; k < W; k++) h = fmaf(act[k], __bfloat162float(net.w2[k * W + tid]), h);
-    act[kZfInitMaxWidth + tid] = fmaxf(h, 0.f);
+    act[kZfInitMaxWidth + tid] = bf(fmaxf(h, 0.f));
   }
   __syncthreads();
   if (warp < (int)kZfInitCoeffs) {

@@ -6,8 +6,10 @@ imports it.  The algorithms have no counterpart in the reference (the
 reference ZF is per subcarrier group, beamform/beamform.cu:74-122); they are
 restated here from their definitions:
 
-- mlp_forward / mlp_loss_grad: the 3-layer ReLU MLP with weights rounded to
-  BF16 (round to nearest even) in every product, biases in full precision,
+- mlp_forward / mlp_loss_grad: the 3-layer ReLU MLP with both operands of
+  every product rounded to BF16 (round to nearest even): the weights, the
+  inputs and hidden activations, and in the backward pass the upstream
+  gradients; biases and the bias gradients (column sums) in full precision,
   and the quadratic loss y^T A y - 2 b^T y + c averaged over the batch;
   gradients are taken with respect to the (FP32) master parameters through
   the rounding (straight-through), flat in the order W1, b1, W2, b2, W3, b3.
@@ -37,19 +39,28 @@ def unpack(params, n_in, width, n_out):
     return W1.reshape(n_in, width), b1, W2.reshape(width, width), b2, W3.reshape(width, n_out), b3
 
 
-def mlp_forward(params, x, n_in, width, n_out):
+def _round_act(act_bf16):
+    """The rounding of an activation or gradient entering a product: BF16, or
+    none (act_bf16 False, the smooth model a finite-difference check needs)."""
+    if act_bf16:
+        return lambda v: bf16(np.asarray(v).astype(np.float32))
+    return lambda v: np.asarray(v, np.float64)
+
+
+def mlp_forward(params, x, n_in, width, n_out, act_bf16=True):
     W1, b1, W2, b2, W3, b3 = unpack(params, n_in, width, n_out)
     W1, W2, W3 = bf16(W1), bf16(W2), bf16(W3)
-    x = np.asarray(x, np.float64)
+    r = _round_act(act_bf16)
+    x = r(np.asarray(x, np.float32) if act_bf16 else x)
     z1 = x @ W1 + b1
-    h1 = np.maximum(z1, 0)
+    h1 = r(np.maximum(z1, 0))
     z2 = h1 @ W2 + b2
-    h2 = np.maximum(z2, 0)
+    h2 = r(np.maximum(z2, 0))
     return h2 @ W3 + b3, (x, z1, h1, z2, h2, W1, W2, W3)
 
 
-def mlp_loss_grad(params, x, A, b, c, n_in, width, n_out):
-    y, (x, z1, h1, z2, h2, W1, W2, W3) = mlp_forward(params, x, n_in, width, n_out)
+def mlp_loss_grad(params, x, A, b, c, n_in, width, n_out, act_bf16=True):
+    y, (x, z1, h1, z2, h2, W1, W2, W3) = mlp_forward(params, x, n_in, width, n_out, act_bf16)
     B = x.shape[0]
     A = np.asarray(A, np.float64).reshape(B, n_out, n_out)
     b = np.asarray(b, np.float64).reshape(B, n_out)
@@ -57,13 +68,14 @@ def mlp_loss_grad(params, x, A, b, c, n_in, width, n_out):
     Ay = np.einsum("bij,bj->bi", A, y)
     loss = np.mean(np.einsum("bi,bi->b", y, Ay) - 2 * np.einsum("bi,bi->b", b, y) + c)
     dy = 2 * (Ay - b) / B
-    gW3 = h2.T @ dy
+    r = _round_act(act_bf16)  # an upstream gradient entering a product
+    gW3 = h2.T @ r(dy)
     gb3 = dy.sum(0)
-    d2 = (dy @ W3.T) * (z2 > 0)
-    gW2 = h1.T @ d2
+    d2 = (r(dy) @ W3.T) * (z2 > 0)
+    gW2 = h1.T @ r(d2)
     gb2 = d2.sum(0)
-    d1 = (d2 @ W2.T) * (z1 > 0)
-    gW1 = x.T @ d1
+    d1 = (r(d2) @ W2.T) * (z1 > 0)
+    gW1 = x.T @ r(d1)
     gb1 = d1.sum(0)
     g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel(), gb3])
     return loss, g

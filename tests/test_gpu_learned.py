@@ -34,8 +34,11 @@ def test_mlp_forward_matches_oracle(mb):
     x = np.random.default_rng(2).standard_normal((B, n_in)).astype(np.float32)
     y = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
     yr, _ = om.mlp_forward(p, x, n_in, width, n_out)
-    # BF16 weights on both sides; FP32 accumulation over 256 terms here
-    assert np.abs(y - yr).max() <= 1e-4 * np.abs(yr).max()
+    # BF16 weights and activations on both sides, FP32 accumulation over 256
+    # terms here; a hidden activation whose FP32 and FP64 pre-activations
+    # fall on either side of a BF16 rounding boundary moves by one BF16 ulp
+    # (2^-8), which bounds the band
+    assert np.abs(y - yr).max() <= 1e-3 * np.abs(yr).max()
 
 
 def test_mlp_gradients_match_oracle(mb):
@@ -58,7 +61,10 @@ def test_mlp_gradients_match_oracle(mb):
     o = 0
     for s in sizes:
         blk, ref = g[o:o + s], gr[o:o + s]
-        assert np.abs(blk - ref).max() <= 2e-4 * np.abs(ref).max() + 1e-7, (o, s)
+        # the backward products on the tensor cores take BF16 activations and
+        # upstream gradients, rounded at the same places in the restatement;
+        # the band covers the one-ulp rounding flips of the forward pass
+        assert np.abs(blk - ref).max() <= 1e-3 * np.abs(ref).max() + 1e-7, (o, s)
         o += s
 
 

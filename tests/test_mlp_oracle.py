@@ -25,10 +25,13 @@ def test_oracle_gradient_finite_difference():
     A = np.einsum("bij,bkj->bik", M, M) / n_out
     b = rng.standard_normal((B, n_out))
     c = rng.standard_normal(B)
-    loss, g = om.mlp_loss_grad(p, x, A, b, c, n_in, width, n_out)
+    # the smooth model (activations not rounded): its gradient is what the
+    # backward pass computes, with the roundings of the GPU's products
+    # applied at the same places in mlp_loss_grad's default mode
+    loss, g = om.mlp_loss_grad(p, x, A, b, c, n_in, width, n_out, act_bf16=False)
 
     def f(q):
-        y, _ = om.mlp_forward(q, x, n_in, width, n_out)
+        y, _ = om.mlp_forward(q, x, n_in, width, n_out, act_bf16=False)
         # same loss without the BF16 rounding of the perturbed weights
         return np.mean(np.einsum("bi,bij,bj->b", y, A, y) - 2 * np.einsum("bi,bi->b", b, y) + c)
 
