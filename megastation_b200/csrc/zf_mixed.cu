@@ -13,9 +13,15 @@
 //     accumulation, and a Gram accurate to ~2^-16 (a plain BF16 Gram costs
 //     ~0.25 dB of EVM at 256x32, which the split removes).  The same
 //     shared-memory tile is both MMA operands (A = T, B^T = T, both K-major).
-//  2. FP32 Gauss-Jordan inverse X of G (registers, one barrier per pivot),
-//     ns_iters Newton-Schulz steps X <- X (2I - G X), then the 1-norm
-//     condition estimate ||G||_1 ||X||_1.
+//  2. FP32 Gauss-Jordan inverse X of G (registers, one barrier per pivot)
+//     or the learned polynomial start, ns_iters Newton-Schulz steps
+//     X <- X (2I - G X), then the 1-norm condition estimate ||G||_1 ||X||_1.
+//     For K <= 32 every matrix product of this step (the powers of G of the
+//     learned start and both products of each Newton-Schulz step) runs on
+//     tcgen05 as 64 x 64 x 64 products of split-BF16 real embeddings, on
+//     the normalised Gn = G / tau and Y = tau X; W then reads Y's BF16
+//     image and scales by 1 / tau.  For 32 < K <= 64 they run on the CUDA
+//     cores.
 //  3. W = X C on tcgen05: D0 = R(X) T over the plane-0 tiles, which stay in
 //     shared memory from step 1 (re-built from the CSI when they do not
 //     fit), gives row for row the plane-0 half of the detector image the
@@ -38,6 +44,7 @@ namespace {
 constexpr int kKT = 64;        // reduction elements per k tile
 constexpr float kPolyAccept = 0.04f;  // ||I - G X||_F before the last step of an accepted learned iterate
 constexpr int kThreads = 256;  // 8 warps; warps w and w+4 share TMEM lane quadrant w
+constexpr uint32_t kZfStageWidth = 64;  // networks up to this width are staged in shared memory
 
 struct ZfmParams {
   ZfNetView net;      // network of the learned initial iterate (used when learned)
@@ -52,6 +59,8 @@ struct ZfmParams {
   uint32_t nh;        // plane-0 k tiles: Mp / 64
   uint32_t resident;  // 1: all nh hi tiles stay in shared memory for W = X C
   uint32_t write_w;   // 1: also store W (FP32, CSI layout); 0: the detector image only
+  uint32_t net_bulk;  // 1: the network's six arrays come into shared memory by bulk copies (MM == 64)
+  uint32_t csi_nst;   // MM == 64: CSI k tiles staged by bulk copies, csi_nst at a time (0: register loads)
   float cond_thr;
 };
 
@@ -274,6 +283,136 @@ __device__ __forceinline__ void block_reduce5(float &a, float &b, float &c, floa
   __syncthreads();
 }
 
+// The learned iterate's network on the CTA's threads: the six features in
+// coef[0..5] -> the four coefficients in coef[8..11].  BF16 weights, and
+// features and hidden activations rounded to BF16 into every product, FP32
+// accumulation, ReLU hidden layers (the arithmetic of mb_mlp_forward,
+// mlp.cu).  act holds 2 kZfInitMaxWidth floats.
+__device__ __forceinline__ void zf_net_eval(const ZfNetView &net, float *act, float *coef) {
+  const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
+  const uint32_t W = net.width;
+  auto bf = [](float x) { return __bfloat162float(__float2bfloat16_rn(x)); };
+  if ((uint32_t)tid < W) {
+    float h = net.b1[tid];
+#pragma unroll
+    for (uint32_t k = 0; k < kZfInitFeatures; k++) h = fmaf(bf(coef[k]), __bfloat162float(net.w1[k * W + tid]), h);
+    act[tid] = bf(fmaxf(h, 0.f));
+  }
+  __syncthreads();
+  if ((uint32_t)tid < W) {
+    float h = net.b2[tid];
+#pragma unroll 8
+    for (uint32_t k = 0; k < W; k++) h = fmaf(act[k], __bfloat162float(net.w2[k * W + tid]), h);
+    act[kZfInitMaxWidth + tid] = bf(fmaxf(h, 0.f));
+  }
+  __syncthreads();
+  if (warp < (int)kZfInitCoeffs) {
+    float y = 0.f;
+    for (uint32_t k = lane; k < W; k += 32)
+      y = fmaf(act[kZfInitMaxWidth + k], __bfloat162float(net.w3[k * kZfInitCoeffs + warp]), y);
+    for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+    if (lane == 0) coef[8 + warp] = y + net.b3[warp];
+  }
+  __syncthreads();
+}
+
+// ---- 64 x 64 real matrices on the tensor cores (K <= 32).  The real
+// embeddings R(Z) (row 2u: [Re Z_uv, -Im Z_uv], row 2u+1: [Im Z_uv, Re Z_uv]
+// over columns 2v, 2v+1; R(A B) = R(A) R(B)) of the K x K complex matrices
+// of the inverse, zero-padded to 64 x 64, are held in shared memory as
+// BF16 images in the canonical no-swizzle layout of img_off (8 KB each), a
+// matrix M as hi = bf16(M) and lo = bf16(M - hi).  A product A B is then
+// A_hi B_hi + A_hi B_lo + A_lo B_hi accumulated in FP32 in tensor memory:
+// BF16 operands, an error of ~2^-16 of the entries (the split-BF16 Gram's
+// accuracy) and one 64 x 64 x 64 MMA per term.  The left operand is read
+// K-major (its rows), the right one MN-major (its rows are the reduction
+// index), so every product is exact as written, symmetric or not.
+constexpr uint32_t kSqImg = 64 * 64 * 2;
+
+// one term: D (+)= A B, a0 / b0 the images' shared-memory addresses
+__device__ __forceinline__ void sq_mma(uint32_t tmem, uint32_t a0, uint32_t b0, bool acc, uint32_t idesc) {
+#pragma unroll
+  for (int ks = 0; ks < 4; ks++) {
+    // A: K core matrices 128 B apart, 8-row groups 1024 B apart; B: 8-row
+    // K groups 1024 B apart, 8-column MN chunks 128 B apart
+    const uint64_t ad = tc::smem_desc(a0 + ks * 256, 128, 1024);
+    const uint64_t bd = tc::smem_desc(b0 + ks * 2048, 1024, 128);
+    tc::mma_f16(tmem, ad, bd, idesc, (acc || ks) ? 1u : 0u);
+  }
+}
+
+// D = A B for split A (ah, al) and B (bh, bl)
+__device__ __forceinline__ void sq_mma3(uint32_t tmem, const uint8_t *ah, const uint8_t *al, const uint8_t *bh,
+                                        const uint8_t *bl, uint32_t idesc) {
+  sq_mma(tmem, tc::smem_u32(ah), tc::smem_u32(bh), false, idesc);
+  sq_mma(tmem, tc::smem_u32(ah), tc::smem_u32(bl), true, idesc);
+  sq_mma(tmem, tc::smem_u32(al), tc::smem_u32(bh), true, idesc);
+}
+
+// 8 values of one row (8 consecutive columns, one 16-byte core row) into
+// the split images (lo may be null)
+__device__ __forceinline__ void sq_put8(uint8_t *hi, uint8_t *lo, uint32_t off, const float *v) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const __nv_bfloat162 a = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+    const float2 f = __bfloat1622float2(a);
+    const __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * e] - f.x, v[2 * e + 1] - f.y);
+    h[e] = *reinterpret_cast<const uint32_t *>(&a);
+    l[e] = *reinterpret_cast<const uint32_t *>(&b);
+  }
+  *reinterpret_cast<uint4 *>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  if (lo) *reinterpret_cast<uint4 *>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// hi + lo of 8 values of one row
+__device__ __forceinline__ void sq_get8(const uint8_t *hi, const uint8_t *lo, uint32_t off, float *v) {
+  const uint4 a = *reinterpret_cast<const uint4 *>(hi + off), b = *reinterpret_cast<const uint4 *>(lo + off);
+  const uint32_t aw[4] = {a.x, a.y, a.z, a.w}, bw[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&aw[e]));
+    const float2 fb = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&bw[e]));
+    v[2 * e] = fa.x + fb.x;
+    v[2 * e + 1] = fa.y + fb.y;
+  }
+}
+
+// two neighbouring values (c even) of one row into the split images
+__device__ __forceinline__ void sq_put2(uint8_t *hi, uint8_t *lo, uint32_t r, uint32_t c, float x, float y) {
+  const __nv_bfloat162 a = __floats2bfloat162_rn(x, y);
+  const float2 f = __bfloat1622float2(a);
+  const uint32_t off = img_off(r, c, 64);
+  *reinterpret_cast<__nv_bfloat162 *>(hi + off) = a;
+  *reinterpret_cast<__nv_bfloat162 *>(lo + off) = __floats2bfloat162_rn(x - f.x, y - f.y);
+}
+
+__device__ __forceinline__ float2 sq_get2(const uint8_t *hi, const uint8_t *lo, uint32_t r, uint32_t c) {
+  const uint32_t off = img_off(r, c, 64);
+  const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(hi + off));
+  const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(lo + off));
+  return make_float2(a.x + b.x, a.y + b.y);
+}
+
+// this thread's part of a 64 x 64 FP32 accumulator at tmem: row r = 16
+// (warp % 4) + lane of the 16 lanes per quadrant an M = 64 MMA writes,
+// 16-column chunks warp / 4 and warp / 4 + 2; f(r, c0, v) gets the 16
+// values of columns c0 .. c0 + 15 (lanes 16..31 only take part in the
+// warp-collective loads).  Two 16-column loads measured faster here than
+// one 32-column load.
+template <typename F>
+__device__ __forceinline__ void sq_readout(uint32_t tmem, F f) {
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const uint32_t r = (warp % 4) * 16 + lane;
+#pragma unroll 1
+  for (uint32_t j = 0; j < 2; j++) {
+    const uint32_t ch = warp / 4 + 2 * j;
+    float v[16];
+    tc::tmem_ld16(tmem + ((uint32_t)((warp % 4) * 32) << 16) + ch * 16, v);
+    if (lane < 16) f(r, ch * 16, v);
+  }
+}
+
 // Learned polynomial initial iterate (no reference counterpart).  With
 // tau = tr(G) / K and Gn = G / tau, the initial iterate is
 // X0 = (a0 I + a1 Gn + a2 Gn^2 + a3 Gn^3) / tau, whose coefficients a come
@@ -292,12 +431,14 @@ __device__ __forceinline__ void block_reduce5(float &a, float &b, float &c, floa
 // of the detector image), otherwise the caller falls back to the exact
 // inverse.  The network: BF16 weights and activations into every product,
 // FP32 accumulation, ReLU hidden layers (the arithmetic of mb_mlp_forward).
-// Result in Xs.
+// Result in Xs.  This CUDA-core form serves 32 < K <= 64 (MM = 128); for
+// K <= 32 the kernel takes the same steps with its products on the tensor
+// cores (the sq_* helpers above).
 template <int MM>
 __device__ bool poly_init(const float2 *Gs, uint32_t ld, float2 *Xs, float2 *P2, float2 *P3, float2 *Ts,
                           float2 *Xn, uint32_t K, uint32_t M, const ZfNetView &net, uint32_t ns_iters,
                           float *sred, float *act, float *coef) {
-  const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
+  const int tid = threadIdx.x;
   // tau and the diagonal's range
   float d = 0.f, z1 = 0.f, z2 = 0.f, dmin = INFINITY, dmax = -INFINITY;
   for (uint32_t i = tid; i < K; i += kThreads) {
@@ -336,31 +477,7 @@ __device__ bool poly_init(const float2 *Gs, uint32_t ld, float2 *Xs, float2 *P2,
     coef[5] = (float)K / (float)M;
   }
   __syncthreads();
-  const uint32_t W = net.width;
-  // features and hidden activations enter each product as BF16, like the
-  // weights (the network's arithmetic everywhere, mlp.cu)
-  auto bf = [](float x) { return __bfloat162float(__float2bfloat16_rn(x)); };
-  if ((uint32_t)tid < W) {
-    float h = net.b1[tid];
-#pragma unroll
-    for (uint32_t k = 0; k < kZfInitFeatures; k++) h = fmaf(bf(coef[k]), __bfloat162float(net.w1[k * W + tid]), h);
-    act[tid] = bf(fmaxf(h, 0.f));
-  }
-  __syncthreads();
-  if ((uint32_t)tid < W) {
-    float h = net.b2[tid];
-    for (uint32_t k = 0; k < W; k++) h = fmaf(act[k], __bfloat162float(net.w2[k * W + tid]), h);
-    act[kZfInitMaxWidth + tid] = bf(fmaxf(h, 0.f));
-  }
-  __syncthreads();
-  if (warp < (int)kZfInitCoeffs) {
-    float y = 0.f;
-    for (uint32_t k = lane; k < W; k += 32)
-      y = fmaf(act[kZfInitMaxWidth + k], __bfloat162float(net.w3[k * kZfInitCoeffs + warp]), y);
-    for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
-    if (lane == 0) coef[8 + warp] = y + net.b3[warp];
-  }
-  __syncthreads();
+  zf_net_eval(net, act, coef);
   const float c0 = coef[8], c1 = coef[9], c2 = coef[10], c3 = coef[11];
   // Gn^3 = Gn Gn^2 (Hermitian)
   cmatmul_any<MM, true>(Gs, ld, P2, K, K,
@@ -409,10 +526,13 @@ __device__ bool poly_init(const float2 *Gs, uint32_t ld, float2 *Xs, float2 *P2,
 }  // namespace
 
 template <int MM>
-__global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q) {
+__global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1) zf_mixed_kernel(const ZfmParams q) {
   extern __shared__ __align__(1024) uint8_t zsm[];
   __shared__ __align__(8) uint64_t tile_bar[2];
   __shared__ __align__(8) uint64_t mma_bar;
+  __shared__ __align__(8) uint64_t stage_bar[4];  // CSI tiles staged by bulk copies
+  __shared__ __align__(8) uint64_t net_bar;       // the network's weights
+  __shared__ float ns_acc[2];                     // residual norms, alternating
   __shared__ uint32_t tmem_slot;
   __shared__ int flag, fail, piv_bad;
   __shared__ float red[kThreads], red2[kThreads];
@@ -431,27 +551,67 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   // shared memory carve-up
   uint8_t *hi_base = zsm;
   uint8_t *lo_t[2] = {zsm + HS * tile_bytes, zsm + (HS + 1) * tile_bytes};
-  uint8_t *ximg = zsm + (HS + 2) * tile_bytes;                  // R(X): MM x MM BF16
-  float2 *Gs = reinterpret_cast<float2 *>(ximg + MM * MM * 2);  // K x ld
-  float2 *Xs = Gs + K * ld;                                     // K x ld
+  // MM == 64 (K <= 32): the inverse on the tensor cores.  Behind the tiles
+  // the split images of Gn = G / tau and of the iterate Y = tau X, then G
+  // (K x ld), then K x ld float2 more (the FP64 fallback's Gram spans both)
+  // that hold the network's weights when the kernel runs learned.  X of the
+  // exact start and the residual's image go in the lo tiles; W = X C reads
+  // the iterate's hi image.
+  uint8_t *gn_img = zsm + (HS + 2) * tile_bytes;
+  uint8_t *y_img = gn_img + 2 * kSqImg;
+  // MM == 128: R(X) (MM x MM BF16), G, X, and the powers Gn^2, Gn^3 of the
+  // learned initial iterate (allotted only when the kernel runs learned);
   // Newton-Schulz temporaries (leading dim K): T in the lo tiles, the other
-  // iterate in the R(X) image; both are free between the Gram and W = X C
+  // iterate in the R(X) image (both free between the Gram and W = X C)
+  uint8_t *ximg = MM == 64 ? y_img : zsm + (HS + 2) * tile_bytes;
+  float2 *Gs = reinterpret_cast<float2 *>(MM == 64 ? y_img + 2 * kSqImg : ximg + MM * MM * 2);
+  float2 *Xs = MM == 64 ? reinterpret_cast<float2 *>(lo_t[0]) : Gs + K * ld;
   float2 *Ts = reinterpret_cast<float2 *>(lo_t[0]);
   float2 *Xn = reinterpret_cast<float2 *>(ximg);
-  // powers Gn^2, Gn^3 of the learned initial iterate (behind Xs; allotted
-  // only when the kernel runs learned)
   float2 *P2 = Xs + K * ld, *P3 = P2 + K * K;
+  uint8_t *wsm = reinterpret_cast<uint8_t *>(Gs + K * ld);
 
   float2 *cg = q.csi + (uint64_t)g * M * K;
   uint8_t *imgw = q.img_w + (uint64_t)g * q.nkt * tile_bytes;
+  // CSI k tile kt (64 antennas x K users, contiguous in [M][K]) staged in
+  // the image region, which is free during the Gram
+  const uint32_t nst = MM == 64 ? q.csi_nst : 0;
+  const uint32_t nstd = nst ? nst : 1;  // divisor of the stage arithmetic (used only when nst > 0)
+  const uint32_t ctile = kKT * K * (uint32_t)sizeof(float2);
+  auto csi_rows = [&](uint32_t kt) { return min((uint32_t)kKT, M - kt * kKT); };
+  auto stage_csi = [&](uint32_t kt) {
+    const uint32_t ss = kt % nstd, bytes = csi_rows(kt) * K * (uint32_t)sizeof(float2);
+    tc::mbar_arrive_expect_tx(&stage_bar[ss], bytes);
+    tc::bulk_g2s(gn_img + ss * ctile, cg + (uint64_t)kt * kKT * K, bytes, &stage_bar[ss]);
+  };
+  // the network's arrays in shared memory: w1, w2, w3 (BF16), b1, b2, b3
+  const uint32_t NW = q.net.width;
+  const uint32_t net_sz[6] = {kZfInitFeatures * NW * 2, NW * NW * 2, NW * kZfInitCoeffs * 2, NW * 4, NW * 4,
+                              kZfInitCoeffs * 4};
+  const void *net_src[6] = {q.net.w1, q.net.w2, q.net.w3, q.net.b1, q.net.b2, q.net.b3};
+  const bool net_bulk = MM == 64 && q.learned && q.net_bulk;
 
   if (tid == 0) {
     tc::mbar_init(&tile_bar[0], 1);
     tc::mbar_init(&tile_bar[1], 1);
     tc::mbar_init(&mma_bar, 1);
+    for (int i = 0; i < 4; i++) tc::mbar_init(&stage_bar[i], 1);
+    tc::mbar_init(&net_bar, 1);
     tc::fence_mbar_init();
     fail = 0;
     piv_bad = 0;
+    ns_acc[0] = ns_acc[1] = 0.f;
+    for (uint32_t kt = 0; kt < min(nst, nh); kt++) stage_csi(kt);
+    if (net_bulk) {
+      uint32_t tot = 0;
+      for (int i = 0; i < 6; i++) tot += net_sz[i];
+      tc::mbar_arrive_expect_tx(&net_bar, tot);
+      uint32_t o = 0;
+      for (int i = 0; i < 6; i++) {
+        tc::bulk_g2s(wsm + o, net_src[i], net_sz[i], &net_bar);
+        o += net_sz[i];
+      }
+    }
   }
   // rows 2K..MM-1 of the R(C) tiles are padding: zero them once
   for (uint32_t c = tid; c < (HS + 2) * tile_bytes / 16; c += kThreads)
@@ -464,6 +624,14 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   uint32_t tiles_used = 0;  // double-buffer uses issued so far
   uint32_t mma_phase = 0;
   bool ok = true;
+  // the network the learned start evaluates: its bulk-copied shared-memory
+  // copy (waited for after the Gram), else global memory
+  ZfNetView netv = q.net;
+  if (net_bulk) {
+    const __nv_bfloat16 *sw = reinterpret_cast<const __nv_bfloat16 *>(wsm);
+    const float *sb = reinterpret_cast<const float *>(wsm + net_sz[0] + net_sz[1] + net_sz[2]);
+    netv = ZfNetView{sw, sw + kZfInitFeatures * NW, sw + kZfInitFeatures * NW + NW * NW, sb, sb + NW, sb + 2 * NW, NW};
+  }
 
   // Tile item e < 8K: user u = e % K and antennas 8 (e / K) .. +7 of the
   // k tile, i.e. 16 bytes of rows 2u (Re C) and 2u+1 (Im C).
@@ -508,19 +676,42 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   // A = sum over the plane-0 tiles of T T^T (hi hi + hi lo + lo hi); the
   // next tile's CSI loads are in flight while the current one is multiplied
   const uint32_t idesc_g = tc::idesc_bf16(MM, MM, false, false);
+  uint32_t staged = min(nst, nh);  // CSI tiles whose bulk copies were issued
+  uint32_t consumed = 0;            // and waited for
   {
     float2 pf[kIpt][8];
-    load_items(0, pf);
+    if (!nst) load_items(0, pf);
     for (uint32_t kt = 0; kt < nh; kt++, tiles_used++) {
       const uint32_t s = tiles_used % 2, use = tiles_used / 2;
       if (use >= 1 && !tc::mbar_wait(&tile_bar[s], (use - 1) & 1)) ok = false;
+      if (nst) {
+        if (!tc::mbar_wait(&stage_bar[kt % nstd], (kt / nstd) & 1)) ok = false;
+        else consumed = kt + 1;
+      }
       if (__syncthreads_or(!ok)) break;
+      if (nst) {
+        // the staged tile, [antenna][user], rows beyond M read as zero
+        const float2 *st = reinterpret_cast<const float2 *>(gn_img + (kt % nstd) * ctile);
+        const uint32_t rows = csi_rows(kt);
+#pragma unroll
+        for (int j = 0; j < kIpt; j++) {
+          const uint32_t e = tid + j * kThreads, u = e % K, r0 = (e / K) * 8;
+#pragma unroll
+          for (int i = 0; i < 8; i++)
+            pf[j][i] = (e < 8 * K && r0 + i < rows) ? st[(r0 + i) * K + u] : make_float2(0.f, 0.f);
+        }
+      }
       uint8_t *hi = hi_base + (q.resident ? kt : s) * tile_bytes;
       store_items(pf, hi, lo_t[s]);
-      if (kt + 1 < nh) load_items(kt + 1, pf);
+      if (!nst && kt + 1 < nh) load_items(kt + 1, pf);
       tc::fence_proxy_async_smem();
       __syncthreads();
       if (tid == 0) {
+        // the stage just read takes the tile nst further on
+        if (nst && kt + nst < nh) {
+          stage_csi(kt + nst);
+          staged = kt + nst + 1;
+        }
         tc::fence_after_sync();
         const uint32_t h0 = tc::smem_u32(hi), l0 = tc::smem_u32(lo_t[s]);
 #pragma unroll
@@ -535,6 +726,12 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
       }
     }
   }
+  // bulk copies land before their shared memory is read or reused or the
+  // CTA exits: the network's (issued at the start, long done by now) and,
+  // after a wait that gave up, CSI tiles still in flight
+  if (net_bulk && !tc::mbar_wait(&net_bar, 0)) ok = false;
+  if (tid == 0)
+    for (uint32_t kt = consumed; kt < staged; kt++) tc::mbar_wait(&stage_bar[kt % nstd], (kt / nstd) & 1);
   if (ok) {
     if (tid == 0) tc::mma_commit(&mma_bar);
     if (!tc::mbar_wait(&mma_bar, mma_phase & 1)) ok = false;
@@ -548,6 +745,7 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   int st = 0;
   bool used_learned = false;  // the learned initial iterate was accepted
   float wmx = 0.f;  // this thread's max |W| over the values it stored
+  float wscale = 1.f;  // W = wscale * (the R(X) image times C)
   if (!fail) {
     // R(G) = A + P A P^T (plane 1 of R(C) is P times plane 0): rows 2u and
     // 2u+1 of A sit in neighbouring TMEM lanes
@@ -570,82 +768,306 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
     }
     tc::fence_before_sync();
     __syncthreads();
-    bool pd = false;
-    if (q.learned)
-      used_learned = poly_init<MM>(Gs, ld, Xs, P2, P3, Ts, Xn, K, M, q.net, q.ns_iters, zi_red, zi_act, zi_coef);
-    if (!used_learned) {
-      if (MM == 64)
-        pd = K <= 16 ? gj_inverse<16>(Gs, Xs, K, ld, prow, &piv_bad)
-                     : gj_inverse<32>(Gs, Xs, K, ld, prow, &piv_bad);
-      else
-        pd = gj_inverse<64>(Gs, Xs, K, ld, prow, &piv_bad);
-    }
-    if (pd) {
-      // Newton-Schulz: T = 2I - G X; X <- X T, ping-ponging Xs and Xn
-      float2 *xc = Xs, *xn = Xn;
-      uint32_t ldc = ld, ldn = K;
-      for (uint32_t it = 0; it < q.ns_iters; it++) {
-        cmatmul_any<MM>(Gs, ld, xc, ldc, K, [&](uint32_t i, uint32_t j, float2 s) {
-          Ts[i * K + j] = make_float2((i == j ? 2.f : 0.f) - s.x, -s.y);
-        });
-        __syncthreads();
-        // X T = 2X - X G X is Hermitian for Hermitian X: upper blocks only
-        cmatmul_any<MM, true>(xc, ldc, Ts, K, K,
-                              [&](uint32_t i, uint32_t j, float2 s) { xn[i * ldn + j] = s; });
-        __syncthreads();
-        float2 *t = xc;
-        xc = xn;
-        xn = t;
-        const uint32_t l = ldc;
-        ldc = ldn;
-        ldn = l;
+    if constexpr (MM == 64) {
+      // ---- the inverse on the tensor cores (K <= 32)
+      uint8_t *gh = gn_img, *gl = gn_img + kSqImg, *yh = y_img, *yl = y_img + kSqImg;
+      uint8_t *eimg = lo_t[0];  // E = I - Gn Y (hi only)
+      const uint32_t two_k = 2 * K;
+      const uint32_t idesc_s = tc::idesc_bf16(64, 64, false, true);
+      bool tc_ok = true;  // uniform: every MMA wait so far succeeded
+      auto issue = [&](auto f) {
+        if (tid == 0) {
+          tc::fence_after_sync();
+          f();
+          tc::mma_commit(&mma_bar);
+        }
+      };
+      auto mma_wait = [&]() {
+        const bool w = tc::mbar_wait(&mma_bar, mma_phase & 1);
+        mma_phase++;
+        if (__syncthreads_or(!w)) tc_ok = false;
+        tc::fence_after_sync();
+        return tc_ok;
+      };
+      // complex entries (u8, j8 + 8 m) of the 32 x 32 grid: eight threads a row
+      const uint32_t u8 = tid / 8, j8 = tid % 8;
+      // tau = tr(G) / K and the diagonal's range
+      float d = 0.f, z1 = 0.f, z2 = 0.f, dmin = INFINITY, dmax = -INFINITY;
+      for (uint32_t i = tid; i < K; i += kThreads) {
+        const float g = Gs[i * ld + i].x;
+        d += g;
+        dmin = fminf(dmin, g);
+        dmax = fmaxf(dmax, g);
       }
-      if (xc != Xs) {
-        for (uint32_t e = tid; e < K * K; e += kThreads) Xs[(e / K) * ld + e % K] = xc[e];
-        __syncthreads();
-      }
-    }
-    if (pd || used_learned) {
-      // 1-norm condition estimate ||G||_1 ||X||_1 (both Hermitian): thread
-      // t sums column j0 + t % 32 over rows t / 32, t / 32 + 8, ...; warp 0
-      // adds the eight partial sums and takes the maximum over columns
-      float gmax = 0.f, xmax = 0.f;
-      for (uint32_t j0 = 0; j0 < K; j0 += 32) {
-        const uint32_t j = j0 + lane;
-        float sg = 0.f, sx = 0.f;
-        if (j < K)
-          for (uint32_t i = warp; i < K; i += kThreads / 32) {
-            const float2 gv = Gs[i * ld + j], xv = Xs[i * ld + j];
-            sg += sqrtf(gv.x * gv.x + gv.y * gv.y);
-            sx += sqrtf(xv.x * xv.x + xv.y * xv.y);
+      block_reduce5(d, z1, z2, dmin, dmax, zi_red);
+      const float tau = d / (float)K;
+      bool pd = false;
+      if (tau > 0.f && dmin > 0.f) {  // uniform
+        const float it = 1.f / tau;
+        // Gn images; ||Gn||_F^2 and the 1-norm (largest row sum of |Gn_uv|)
+        float f2 = 0.f, rs = 0.f;
+#pragma unroll
+        for (uint32_t m = 0; m < 4; m++) {
+          const uint32_t v = j8 + 8 * m;
+          float2 g = make_float2(0.f, 0.f);
+          if (u8 < K && v < K) g = make_float2(Gs[u8 * ld + v].x * it, Gs[u8 * ld + v].y * it);
+          f2 += g.x * g.x + g.y * g.y;
+          rs += sqrtf(g.x * g.x + g.y * g.y);
+          sq_put2(gh, gl, 2 * u8, 2 * v, g.x, -g.y);
+          sq_put2(gh, gl, 2 * u8 + 1, 2 * v, g.y, g.x);
+        }
+        rs += __shfl_xor_sync(0xffffffffu, rs, 1);
+        rs += __shfl_xor_sync(0xffffffffu, rs, 2);
+        rs += __shfl_xor_sync(0xffffffffu, rs, 4);
+        tc::fence_proxy_async_smem();
+        float a0 = 0.f, a1 = 0.f, n0 = INFINITY, gn1 = rs;
+        block_reduce5(f2, a0, a1, n0, gn1, zi_red);
+        const float t2 = f2 / (float)K;
+        // E = I - Gn Y into its image; returns ||E||_F (complex).  The warps'
+        // sums meet in ns_acc[n_res % 2] (the other entry is cleared for the
+        // next call: every thread has read it before the barrier below)
+        uint32_t n_res = 0;
+        auto residual = [&]() {
+          issue([&] { sq_mma3(tmem, gh, gl, yh, yl, idesc_s); });
+          float en = 0.f;
+          if (mma_wait()) {
+            sq_readout(tmem, [&](uint32_t r, uint32_t c0, float *v) {
+#pragma unroll
+              for (int i = 0; i < 16; i++) {
+                const float e = ((r == c0 + i && r < two_k) ? 1.f : 0.f) - v[i];
+                en += e * e;
+                v[i] = e;
+              }
+              sq_put8(eimg, nullptr, img_off(r, c0, 64), v);
+              sq_put8(eimg, nullptr, img_off(r, c0 + 8, 64), v + 8);
+            });
           }
-        red[tid] = sg;
-        red2[tid] = sx;
-        __syncthreads();
-        if (warp == 0) {
-          float a = 0.f, c = 0.f;
-          for (uint32_t w = 0; w < kThreads / 32; w++) {
-            a += red[w * 32 + lane];
-            c += red2[w * 32 + lane];
+          for (int o = 16; o > 0; o >>= 1) en += __shfl_xor_sync(0xffffffffu, en, o);
+          if (lane == 0) atomicAdd(&ns_acc[n_res & 1], en);
+          if (tid == 0) ns_acc[(n_res + 1) & 1] = 0.f;
+          tc::fence_proxy_async_smem();
+          tc::fence_before_sync();
+          __syncthreads();
+          en = ns_acc[n_res & 1];
+          n_res++;
+          return sqrtf(0.5f * en);  // each complex entry is four real ones
+        };
+        // Y <- Y + Y E = Y (2I - Gn Y)
+        auto refine = [&]() {
+          issue([&] {
+            sq_mma(tmem, tc::smem_u32(yh), tc::smem_u32(eimg), false, idesc_s);
+            sq_mma(tmem, tc::smem_u32(yl), tc::smem_u32(eimg), true, idesc_s);
+          });
+          if (mma_wait()) {
+            sq_readout(tmem, [&](uint32_t r, uint32_t c0, float *v) {
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const uint32_t off = img_off(r, c0 + 8 * h, 64);
+                float y[8];
+                sq_get8(yh, yl, off, y);
+#pragma unroll
+                for (int i = 0; i < 8; i++) y[i] += v[8 * h + i];
+                sq_put8(yh, yl, off, y);
+              }
+            });
           }
-          for (int o = 16; o > 0; o >>= 1) {
-            a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
-            c = fmaxf(c, __shfl_xor_sync(0xffffffffu, c, o));
+          tc::fence_proxy_async_smem();
+          tc::fence_before_sync();
+          __syncthreads();
+        };
+        if (q.learned) {
+          // Gn^2 = Gn Gn into the iterate's images; t3 = <Gn, Gn^2> / K and
+          // t4 = ||Gn^2||_F^2 / K (each complex entry is four real ones)
+          issue([&] { sq_mma3(tmem, gh, gl, gh, gl, idesc_s); });
+          float a3 = 0.f, a4 = 0.f;
+          if (mma_wait()) {
+            sq_readout(tmem, [&](uint32_t r, uint32_t c0, float *v) {
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const uint32_t off = img_off(r, c0 + 8 * h, 64);
+                float g[8];
+                sq_get8(gh, gl, off, g);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                  a3 += g[i] * v[8 * h + i];
+                  a4 += v[8 * h + i] * v[8 * h + i];
+                }
+                sq_put8(yh, yl, off, v + 8 * h);
+              }
+            });
           }
-          if (lane == 0) {
-            red[0] = a;
-            red2[0] = c;
+          tc::fence_proxy_async_smem();
+          tc::fence_before_sync();
+          float b0 = 0.f, m0 = INFINITY, m1 = -INFINITY;
+          block_reduce5(a3, a4, b0, m0, m1, zi_red);
+          // Gn^3 = Gn Gn^2 on the tensor cores while the network runs
+          if (tc_ok) issue([&] { sq_mma3(tmem, gh, gl, yh, yl, idesc_s); });
+          const float t3 = a3 / (2.f * K), t4 = a4 / (2.f * K);
+          if (tid == 0) {
+            zi_coef[0] = t2 - 1.f;
+            zi_coef[1] = t3 - 3.f * t2 + 2.f;
+            zi_coef[2] = t4 - 4.f * t3 + 6.f * t2 - 3.f;
+            zi_coef[3] = dmin * it - 1.f;
+            zi_coef[4] = dmax * it - 1.f;
+            zi_coef[5] = (float)K / (float)M;
+          }
+          __syncthreads();
+          zf_net_eval(netv, zi_act, zi_coef);
+          const float c0 = zi_coef[8], c1 = zi_coef[9], c2 = zi_coef[10], c3 = zi_coef[11];
+          // Y0 = c0 I + c1 Gn + c2 Gn^2 + c3 Gn^3, in place of Gn^2
+          if (tc_ok && mma_wait()) {
+            sq_readout(tmem, [&](uint32_t r, uint32_t cb, float *v) {
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const uint32_t off = img_off(r, cb + 8 * h, 64);
+                float g[8], p[8];
+                sq_get8(gh, gl, off, g);
+                sq_get8(yh, yl, off, p);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                  const uint32_t c = cb + 8 * h + i;
+                  p[i] = ((r == c && r < two_k) ? c0 : 0.f) + c1 * g[i] + c2 * p[i] + c3 * v[8 * h + i];
+                }
+                sq_put8(yh, yl, off, p);
+              }
+            });
+          }
+          tc::fence_proxy_async_smem();
+          tc::fence_before_sync();
+          __syncthreads();
+          // ns_iters steps, then up to two more only to rescue a near miss
+          // (0.04 < ||E|| < 0.3); a start further off goes to the exact inverse
+          float e_last = INFINITY;
+          bool conv = tc_ok;
+          for (uint32_t s = 0; s < q.ns_iters + 2 && conv; s++) {
+            if (s >= q.ns_iters && (e_last <= kPolyAccept || e_last >= 0.3f)) break;  // uniform
+            e_last = residual();
+            if (!(e_last < 1.f) || !tc_ok) conv = false;  // uniform: the iteration would not converge
+            else refine();
+          }
+          used_learned = conv && tc_ok && e_last <= kPolyAccept;
+        }
+        if (!used_learned && tc_ok) {
+          // exact start: Gauss-Jordan X of G (into the lo tiles), Y = tau X
+          pd = K <= 16 ? gj_inverse<16>(Gs, Xs, K, ld, prow, &piv_bad) : gj_inverse<32>(Gs, Xs, K, ld, prow, &piv_bad);
+          if (pd) {
+#pragma unroll
+            for (uint32_t m = 0; m < 4; m++) {
+              const uint32_t v = j8 + 8 * m;
+              float2 x = make_float2(0.f, 0.f);
+              if (u8 < K && v < K) x = make_float2(Xs[u8 * ld + v].x * tau, Xs[u8 * ld + v].y * tau);
+              sq_put2(yh, yl, 2 * u8, 2 * v, x.x, -x.y);
+              sq_put2(yh, yl, 2 * u8 + 1, 2 * v, x.y, x.x);
+            }
+            tc::fence_proxy_async_smem();
+            __syncthreads();
+            for (uint32_t s = 0; s < q.ns_iters && tc_ok; s++) {
+              residual();
+              if (tc_ok) refine();
+            }
           }
         }
-        __syncthreads();
-        gmax = fmaxf(gmax, red[0]);
-        xmax = fmaxf(xmax, red2[0]);
-        __syncthreads();
+        if ((pd || used_learned) && tc_ok) {
+          // 1-norm condition estimate ||G||_1 ||X||_1 = ||Gn||_1 ||Y||_1
+          float ys = 0.f;
+#pragma unroll
+          for (uint32_t m = 0; m < 4; m++) {
+            const float2 y = sq_get2(yh, yl, 2 * u8, 2 * (j8 + 8 * m));
+            ys += sqrtf(y.x * y.x + y.y * y.y);
+          }
+          ys += __shfl_xor_sync(0xffffffffu, ys, 1);
+          ys += __shfl_xor_sync(0xffffffffu, ys, 2);
+          ys += __shfl_xor_sync(0xffffffffu, ys, 4);
+          float b0 = 0.f, b1 = 0.f, b2 = 0.f, m0 = INFINITY;
+          block_reduce5(b0, b1, b2, m0, ys, zi_red);
+          cond_est = gn1 * ys;
+          if (!(cond_est <= q.cond_thr)) st = 2;
+          wscale = it;  // W = X C = (Y C) / tau
+        } else {
+          st = 2;
+        }
+      } else {
+        st = 2;  // G is not positive definite in FP32
       }
-      cond_est = gmax * xmax;
-      if (!(cond_est <= q.cond_thr)) st = 2;
+      if (!tc_ok) fail = 1;
     } else {
-      st = 2;
+      bool pd = false;
+      if (q.learned)
+        used_learned = poly_init<MM>(Gs, ld, Xs, P2, P3, Ts, Xn, K, M, q.net, q.ns_iters, zi_red, zi_act, zi_coef);
+      if (!used_learned) {
+        if (MM == 64)
+          pd = K <= 16 ? gj_inverse<16>(Gs, Xs, K, ld, prow, &piv_bad)
+                       : gj_inverse<32>(Gs, Xs, K, ld, prow, &piv_bad);
+        else
+          pd = gj_inverse<64>(Gs, Xs, K, ld, prow, &piv_bad);
+      }
+      if (pd) {
+        // Newton-Schulz: T = 2I - G X; X <- X T, ping-ponging Xs and Xn
+        float2 *xc = Xs, *xn = Xn;
+        uint32_t ldc = ld, ldn = K;
+        for (uint32_t it = 0; it < q.ns_iters; it++) {
+          cmatmul_any<MM>(Gs, ld, xc, ldc, K, [&](uint32_t i, uint32_t j, float2 s) {
+            Ts[i * K + j] = make_float2((i == j ? 2.f : 0.f) - s.x, -s.y);
+          });
+          __syncthreads();
+          // X T = 2X - X G X is Hermitian for Hermitian X: upper blocks only
+          cmatmul_any<MM, true>(xc, ldc, Ts, K, K,
+                                [&](uint32_t i, uint32_t j, float2 s) { xn[i * ldn + j] = s; });
+          __syncthreads();
+          float2 *t = xc;
+          xc = xn;
+          xn = t;
+          const uint32_t l = ldc;
+          ldc = ldn;
+          ldn = l;
+        }
+        if (xc != Xs) {
+          for (uint32_t e = tid; e < K * K; e += kThreads) Xs[(e / K) * ld + e % K] = xc[e];
+          __syncthreads();
+        }
+      }
+      if (pd || used_learned) {
+        // 1-norm condition estimate ||G||_1 ||X||_1 (both Hermitian): thread
+        // t sums column j0 + t % 32 over rows t / 32, t / 32 + 8, ...; warp 0
+        // adds the eight partial sums and takes the maximum over columns
+        float gmax = 0.f, xmax = 0.f;
+        for (uint32_t j0 = 0; j0 < K; j0 += 32) {
+          const uint32_t j = j0 + lane;
+          float sg = 0.f, sx = 0.f;
+          if (j < K)
+            for (uint32_t i = warp; i < K; i += kThreads / 32) {
+              const float2 gv = Gs[i * ld + j], xv = Xs[i * ld + j];
+              sg += sqrtf(gv.x * gv.x + gv.y * gv.y);
+              sx += sqrtf(xv.x * xv.x + xv.y * xv.y);
+            }
+          red[tid] = sg;
+          red2[tid] = sx;
+          __syncthreads();
+          if (warp == 0) {
+            float a = 0.f, c = 0.f;
+            for (uint32_t w = 0; w < kThreads / 32; w++) {
+              a += red[w * 32 + lane];
+              c += red2[w * 32 + lane];
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+              a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+              c = fmaxf(c, __shfl_xor_sync(0xffffffffu, c, o));
+            }
+            if (lane == 0) {
+              red[0] = a;
+              red2[0] = c;
+            }
+          }
+          __syncthreads();
+          gmax = fmaxf(gmax, red[0]);
+          xmax = fmaxf(xmax, red2[0]);
+          __syncthreads();
+        }
+        cond_est = gmax * xmax;
+        if (!(cond_est <= q.cond_thr)) st = 2;
+      } else {
+        st = 2;
+      }
     }
   }
 
@@ -654,18 +1076,22 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   // P D0 (R(X) commutes with P), so it needs no multiply of its own
   if (!fail && st == 0) {
     // R(X) image, K-major over the reduction index 2v + rj; rows/columns
-    // beyond 2K are padding and stay zero
-    for (uint32_t c = tid; c < MM * MM * 2 / 16; c += kThreads)
-      reinterpret_cast<uint4 *>(ximg)[c] = make_uint4(0, 0, 0, 0);
-    __syncthreads();
-    for (uint32_t e = tid; e < K * K; e += kThreads) {
-      const uint32_t u = e / K, v = e % K;
-      const float2 x = Xs[u * ld + v];
-      *reinterpret_cast<__nv_bfloat162 *>(ximg + img_off(2 * u, 2 * v, MM)) = __floats2bfloat162_rn(x.x, -x.y);
-      *reinterpret_cast<__nv_bfloat162 *>(ximg + img_off(2 * u + 1, 2 * v, MM)) = __floats2bfloat162_rn(x.y, x.x);
+    // beyond 2K are padding and stay zero.  MM == 64: the iterate's hi image
+    // R(Y) = tau R(X) is already there (the epilogue scales by 1 / tau).
+    if constexpr (MM != 64) {
+      for (uint32_t c = tid; c < MM * MM * 2 / 16; c += kThreads)
+        reinterpret_cast<uint4 *>(ximg)[c] = make_uint4(0, 0, 0, 0);
+      __syncthreads();
+      for (uint32_t e = tid; e < K * K; e += kThreads) {
+        const uint32_t u = e / K, v = e % K;
+        const float2 x = Xs[u * ld + v];
+        *reinterpret_cast<__nv_bfloat162 *>(ximg + img_off(2 * u, 2 * v, MM)) = __floats2bfloat162_rn(x.x, -x.y);
+        *reinterpret_cast<__nv_bfloat162 *>(ximg + img_off(2 * u + 1, 2 * v, MM)) =
+            __floats2bfloat162_rn(x.y, x.x);
+      }
+      tc::fence_proxy_async_smem();
+      __syncthreads();
     }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
     const uint32_t idesc_w = tc::idesc_bf16(MM, kKT, false, true);
     for (uint32_t kt0 = 0; kt0 < nh && ok; kt0 += TCH) {
       const uint32_t nt = min(TCH, nh - kt0);
@@ -721,7 +1147,10 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
         float v[16], nb[16];
         tc::tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + ch * 16, v);
 #pragma unroll
-        for (int i = 0; i < 16; i++) nb[i] = __shfl_xor_sync(0xffffffffu, v[i], 1);
+        for (int i = 0; i < 16; i++) {
+          v[i] *= wscale;
+          nb[i] = __shfl_xor_sync(0xffffffffu, v[i], 1);
+        }
         if (lane >= rows_per_warp) continue;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
@@ -834,10 +1263,20 @@ __global__ void __launch_bounds__(kThreads, 1) zf_mixed_kernel(const ZfmParams q
   if (warp == 0) tc::tmem_dealloc(tmem, TC);
 }
 
-static size_t zfm_smem(uint32_t K, uint32_t MM, uint32_t hi_slots, bool learned) {
-  const size_t tile = (size_t)MM * kKT * 2;
-  return (hi_slots + 2) * tile + (size_t)MM * MM * 2 + 2 * (size_t)K * (K + 1) * sizeof(float2) +
-         (learned ? 2 * (size_t)K * K * sizeof(float2) : 0);
+// dynamic shared memory of the kernel (its carve-up at the top of the kernel)
+static size_t zfm_smem(uint32_t K, uint32_t MM, uint32_t hi_slots, bool learned, uint32_t width) {
+  const size_t tile = (size_t)MM * kKT * 2, gk = (size_t)K * (K + 1) * sizeof(float2);
+  if (MM == 64) {
+    // tiles, the Gn and iterate images, G, then the FP64 Gram's second half
+    // or the staged network (BF16 weights, FP32 biases)
+    size_t net = 0;
+    if (learned && width <= kZfStageWidth) {
+      const size_t nw = (size_t)width * (kZfInitFeatures + width + kZfInitCoeffs);
+      net = (nw + 1) / 2 * 2 * 2 + (2 * (size_t)width + kZfInitCoeffs) * 4;
+    }
+    return (hi_slots + 2) * tile + 4 * (size_t)kSqImg + gk + std::max(gk, net);
+  }
+  return (hi_slots + 2) * tile + (size_t)MM * MM * 2 + 2 * gk + (learned ? 2 * (size_t)K * K * sizeof(float2) : 0);
 }
 
 uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K) {
@@ -871,6 +1310,16 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
   q.nh = s.Mp / kKT;
   q.ns_iters = opts ? opts->ns_iters : 2;
   q.cond_thr = opts && opts->cond_threshold > 0 ? opts->cond_threshold : 1e4f;
+  // bulk copies want 16-byte aligned addresses and sizes: the network's six
+  // arrays (width a multiple of 4), and CSI k tiles (K even)
+  auto a16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  q.net_bulk = 0;
+  if (s.MM == 64 && learned && net->width <= kZfStageWidth && net->width % 4 == 0 && a16(net->w1) &&
+      a16(net->w2) && a16(net->w3) && a16(net->b1) && a16(net->b2) && a16(net->b3))
+    q.net_bulk = 1;
+  q.csi_nst = 0;
+  if (s.MM == 64 && K % 2 == 0 && a16(csi))
+    q.csi_nst = std::min<uint32_t>(4, 4 * kSqImg / (kKT * K * (uint32_t)sizeof(float2)));
   int dev = 0, maxs = 0;
   MB_CUDA_TRY(cudaGetDevice(&dev));
   MB_CUDA_TRY(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -894,9 +1343,10 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
   }
   const size_t avail = (size_t)maxs - (size_t)static_smem[which].load();
   // keep every hi tile in shared memory when it fits, else stream two
-  q.resident = zfm_smem(K, s.MM, q.nh, learned) <= avail ? 1 : 0;
+  const uint32_t width = learned ? net->width : 0;
+  q.resident = zfm_smem(K, s.MM, q.nh, learned, width) <= avail ? 1 : 0;
   q.write_w = write_w ? 1 : 0;
-  const size_t smem = zfm_smem(K, s.MM, q.resident ? q.nh : 2, learned);
+  const size_t smem = zfm_smem(K, s.MM, q.resident ? q.nh : 2, learned, width);
   if (smem > avail) return MB_UNSUPPORTED;
   if (groups == 0) return MB_OK;
   if (s.MM == 64)
