@@ -185,14 +185,27 @@ def profile_traffic(name, unit_name, units):
     return float(m.group(1)) * units if m else None
 
 
+def fused_equalize(cfg, sym_batch, mixed):
+    """Whether the mixed slot equalizes inside its ZF kernel (the library's
+    rule: the tensor-core FFT of pilots and every uplink symbol in one
+    launch, K <= 32, M <= 256, sc_group a multiple of 16, and all of a
+    group's (symbol, subcarrier) columns in one 128-column tile)."""
+    if not (mixed and cfg.N == 4096 and cfg.U >= 1 and sym_batch >= cfg.U):
+        return False
+    return cfg.K <= 32 and cfg.M <= 256 and cfg.sg % 16 == 0 and cfg.U * cfg.sg <= 128
+
+
 def slot_launches(cfg, sym_batch, mixed, downlink=False):
     """Kernels one uplink slot launches: the pilot FFT (inside the first
     uplink FFT launch in the mixed path at N = 4096), the ZF, one uplink FFT
-    and one equalize per symbol batch; with a downlink also the precode and
-    the IFFT, and in the mixed path the precoder scaling and its BF16
-    images (the FP32 path's Cholesky kernel writes the precoder itself)."""
+    and one equalize per symbol batch (none when the ZF kernel equalizes);
+    with a downlink also the precode and the IFFT, and in the mixed path the
+    precoder scaling and its BF16 images (the FP32 path's Cholesky kernel
+    writes the precoder itself)."""
     batches = max(1, -(-cfg.U // max(sym_batch, 1)))
     n = (0 if mixed and cfg.N == 4096 else 1) + 1 + 2 * batches
+    if fused_equalize(cfg, sym_batch, mixed):
+        n -= 1
     return n + ((4 if mixed else 2) if downlink else 0)
 
 
@@ -202,8 +215,9 @@ def roofline(cfg, args, st, n_valid, hrow):
     hbm_peak, tc_peak, peak_kind = measured_peaks()
     calls = max(st["calls"], 1)
     mixed = args.precision == "mixed"
+    fused = mixed and st["n_eq"] == 0                  # equalized inside the ZF kernel
     n_fft = max(st["n_fft"], 1)                        # launches over all recorded slots
-    n_eq = max(st["n_eq"], 1)
+    n_eq = calls if fused else max(st["n_eq"], 1)
     rows = cfg.U * cfg.M * calls / n_fft               # antenna rows per uplink FFT launch
     syms = cfg.U * calls / n_eq                        # symbols per equalize launch
     out_b = 4 if mixed else 8                          # BF16 planar or c32 per subcarrier
@@ -231,17 +245,25 @@ def roofline(cfg, args, st, n_valid, hrow):
     }
     if tc_fft:
         del k["fft_pilot"]  # the pilot rows go through the uplink FFT launch
+    if fused:
+        # one kernel: the ZF (latency-bound, its FLOPs stated) and the
+        # equalize's bytes (CSI in, samples in, LLRs and hard bits out; the
+        # detector image never leaves shared memory), held to HBM
+        eq = k.pop("equalize")
+        k["zf"].update({"bound": "hbm", "units": cfg.G,
+                        "bytes": cfg.G * cfg.M * cfg.K * 8 + eq["bytes"] - cfg.G * img_group})
     names = {"fft_uplink": ("fft_tc_kernel<pilot + uplink rows>" if tc_fft else "fft_kernel<12, uplink LP>") if mixed
              else "fft_kernel<12, uplink>",
              "fft_pilot": "fft_kernel<12, pilot>",
-             "zf": "zf_mixed_kernel<64>" if mixed else "zf_chol_kernel<float>",
-             "equalize": "equalize_tc_kernel<64, 6>" if mixed else "equalize_fp32_kernel"}
+             "zf": (f"zf_mixed_kernel<64, {cfg.Qm}> (ZF + equalize)" if fused else "zf_mixed_kernel<64, 0>")
+             if mixed else "zf_chol_kernel<float>",
+             "equalize": f"equalize_tc_kernel<64, {cfg.Qm}>" if mixed else "equalize_fp32_kernel"}
     # the tensor-core FFT's traffic depends on the sample format: int8
     # workloads read the int8 capture, the others the int16 one
     fft_tc_prof = "fft_tc_uplink_4096x256" + ("_int8" if cfg.iq_dtype == "int8" else "")
     profiles = {"fft_uplink": fft_tc_prof if tc_fft else "fft_uplink_lp_4096x256",
                 "equalize": "equalize_tc_256x32",
-                "zf": "zf_mixed_256x32", "fft_pilot": "fft_uplink_lp_4096x256"}
+                "zf": "zf_eq_fused_256x32" if fused else "zf_mixed_256x32", "fft_pilot": "fft_uplink_lp_4096x256"}
     for key, v in k.items():
         sec = v["ms"] / 1e3
         if v["bound"] == "hbm":
@@ -250,6 +272,8 @@ def roofline(cfg, args, st, n_valid, hrow):
         else:
             v["achieved"] = v["flops"] / sec / 1e12 if sec > 0 else 0.0
             v["frac"] = v["achieved"] / tc_peak
+        if "flops" in v and v["bound"] == "hbm":
+            v["tensor_frac"] = v["flops"] / sec / 1e12 / tc_peak if sec > 0 else 0.0
     dom = max(k, key=lambda x: k[x]["per_slot_ms"])
     v = k[dom]
     hbm = v["bound"] == "hbm"

@@ -435,7 +435,10 @@ mb_status mb_pipe_timer_ms(mb_pipe *pipe, double *ms);
  * recorded calls (while timing, every kernel runs alone on the launching
  * stream, the first FFT batch included): [0] pilot FFT, [1] ZF (+ tail
  * fill), [2] uplink FFT batches, [3] equalize, [4] whole slot,
- * [5] number of uplink FFT launches timed in [2], [6] equalize launches,
+ * [5] number of uplink FFT launches timed in [2], [6] equalize launches
+ * (0 when the mixed-precision slot equalized inside its ZF kernel: one
+ * batch of all uplink symbols, K <= 32, M <= 256, sc_group a multiple of
+ * 16 and U * sc_group <= 128; the ZF stage [1] then holds both),
  * [7] recorded calls; then clears the record. */
 mb_status mb_slot_timing(mb_slot *slot, uint32_t max_calls);
 mb_status mb_slot_stage_ms(mb_slot *slot, double *out8);

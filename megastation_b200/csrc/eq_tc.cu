@@ -33,6 +33,7 @@
 #include "common.cuh"
 #include "eq_common.cuh"
 #include "eq_tc.cuh"
+#include "eq_tc_epi.cuh"
 #include "sgemv.cuh"
 #include "tc.cuh"
 
@@ -137,122 +138,16 @@ __global__ void __launch_bounds__(kEqThreads, 1)
     else timed_out = 1;
   }
   __syncwarp();
-  // Everything the epilogue needs besides the accumulator is computed, and
-  // the descrambling bytes loaded, before the wait, so their latency hides
-  // under the load/MMA phase.
-  // thread = D row = TMEM lane 32 (warp % 4) + lane = column (symbol l,
-  // subcarrier sl); warps w and w + 4 take alternate chunks of 8 users
-  const uint32_t quad = warp % 4;
-  const uint32_t c = quad * 32 + lane;
-  const uint32_t l = c / p.sg, sl = c % p.sg;
-  const uint32_t s = s_base + sl;
-  const bool valid = c < ncols && s < p.S;
-  const uint32_t lg = q.l0 + l_off + l;
-  // LLR placement of subcarrier s (equalize_kernel.cuh:272-287), the same
-  // for every user: code block cb, offset base in the (symbol, user) row
-  const uint32_t t0 = s * QM;
-  const uint32_t cb = t0 / p.cb_size32;
-  const uint32_t base = cb * p.cb_stride32 + p.zeros32 + (t0 - cb * p.cb_size32);
-  const bool llr_on = valid && cb < p.cb_blocks;
-  const bool pair = base + QM <= p.row_len32 && ((p.row_len32 | base) & 1) == 0 &&
-                    (reinterpret_cast<uintptr_t>(p.llr) & 3) == 0;
-  // hard bits: stream positions < n_valid only, first bit most significant
-  uint32_t nvm = 0;
-#pragma unroll
-  for (int qb = 0; qb < QM; qb++)
-    if (t0 + qb < p.n_valid32) nvm |= 1u << (QM - 1 - qb);
-  if (!valid) nvm = 0;
-  // 8-lane groups hold 8 consecutive subcarriers of one symbol (sg % 8 ==
-  // 0), i.e. QM whole bytes of the hard-bit row.  Lane gl < QM writes byte
-  // gl; its 8 bits come from the NSUB subcarriers from sa on, fetched with
-  // independent shuffles (a group cut short by S pads with zeros).
-  constexpr uint32_t NSUB = QM == 6 ? 2 : 8 / QM;
-  const uint32_t gl = lane & 7;
-  const uint32_t sa = gl < (uint32_t)QM ? 8 * gl / QM : 0;
-  const uint32_t boff = 8 * gl - QM * sa;  // first bit of the byte within sa's bits
-  const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
-  const uint32_t nvalid = __popc((vmask >> (lane & ~7u)) & 0xFFu);
-  const uint32_t gb = (s - gl) * QM / 8 + gl;
-  const bool byte_on = p.hard && gl < (nvalid * QM + 7) / 8 && gb * 8 < p.n_valid32;
-  const uint32_t end = p.n_valid32 - gb * 8;
-  const uint32_t seq_mask = byte_on && end < 8 ? (0xFF00u >> end) & 0xFFu : 0xFFu;
-  const uint32_t nch = q.N / 16;
-  // descrambling bytes of this warp's chunks ch = warp / 4 + 2 cc, four to a
-  // word: byte j of chunk cc (user 8 ch + j) in sqw[cc][j / 4]
-  constexpr int kMaxCh = MM / 32;  // N <= MM columns: at most MM / 32 chunks per warp
-  uint32_t sqw[kMaxCh][2];
-#pragma unroll
-  for (int cc = 0; cc < kMaxCh; cc++) {
-    const uint32_t ch = warp / 4 + 2 * cc;
-    const uint8_t *spu = p.seqb ? p.seqb + (uint64_t)(ch * 8) * p.seq_row_bytes + gb : nullptr;
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      uint32_t w = 0;
-#pragma unroll
-      for (int b = 0; b < 4; b++) {
-        const uint32_t j = 4 * h + b;
-        if (spu && byte_on && ch < nch && ch * 8 + j < p.K)
-          w |= ((uint32_t)__ldg(spu + j * p.seq_row_bytes) & seq_mask) << (8 * b);
-      }
-      sqw[cc][h] = w;
-    }
-  }
+  // the epilogue's per-thread setup overlaps the load/MMA phase
+  EqTcEpilogue<MM, QM> epi;
+  epi.prepare(p, s_base, l_off, ncols, q.l0, q.N, warp, lane);
   // everyone: wait for the accumulator (bounded)
   bool ok = tc::mbar_wait(&done_bar, 0);
   if (__syncthreads_or(!ok || timed_out)) {
     if (tid == 0 && q.err) atomicOr(q.err, tc::kErrTimeout);
   } else {
     tc::fence_after_sync();
-    // chunk loop not unrolled: the chunk's bytes are always in sqw[0], the
-    // array rotating by one chunk per pass
-#pragma unroll 1
-    for (uint32_t ch = warp / 4; ch < nch; ch += kEqThreads / 128) {
-      float v[16];
-      tc::tmem_ld16(tmem + (quad * 32 << 16) + ch * 16, v);
-      const uint64_t row = (uint64_t)lg * p.K + ch * 8;  // (symbol, first user of the chunk)
-      __half *lpu = reinterpret_cast<__half *>(p.llr) + row * p.row_len + base;
-      uint8_t *hpu = p.hard ? p.hard + row * p.hrow + gb : nullptr;
-      float2 *xpu = p.x ? p.x + row * p.S + s : nullptr;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        if (ch * 8 + j >= p.K) break;
-        const float2 x = make_float2(v[2 * j], v[2 * j + 1]);
-        __half2 lv[QM / 2];  // (Re, Im) pairs, bit-identical to demod()
-        demod2<QM>(x, lv);
-        if (llr_on) {
-          if (pair) {
-#pragma unroll
-            for (int h = 0; h < QM / 2; h++) reinterpret_cast<__half2 *>(lpu)[h] = lv[h];
-          } else {
-#pragma unroll
-            for (int h = 0; h < QM / 2; h++) {
-              if (base + 2 * h < p.row_len32) lpu[2 * h] = __low2half(lv[h]);
-              if (base + 2 * h + 1 < p.row_len32) lpu[2 * h + 1] = __high2half(lv[h]);
-            }
-          }
-        }
-        if (hpu) {
-          const uint32_t hb = hard2<QM>(lv) & nvm;
-          uint32_t win = 0;
-#pragma unroll
-          for (uint32_t k = 0; k < NSUB; k++)
-            win = (win << QM) | __shfl_sync(0xffffffffu, hb, (lane & ~7) + sa + k);
-          const uint32_t sq = (sqw[0][j / 4] >> (8 * (j % 4))) & 0xFFu;
-          if (byte_on) *hpu = (uint8_t)((win >> (NSUB * QM - boff - 8)) ^ sq);
-          hpu += p.hrow;
-        }
-        if (xpu) {
-          if (valid) *xpu = x;
-          xpu += p.S;
-        }
-        lpu += p.row_len;
-      }
-#pragma unroll
-      for (int cc = 0; cc + 1 < kMaxCh; cc++) {
-        sqw[cc][0] = sqw[cc + 1][0];
-        sqw[cc][1] = sqw[cc + 1][1];
-      }
-    }
+    epi.run(p, tmem, warp, lane);
   }
   tc::fence_before_sync();
   __syncthreads();

@@ -37,6 +37,7 @@ struct mb_slot {
   uint32_t sb_cap;    // uplink symbols the y / y_lp buffers hold (>= sym_batch)
   uint32_t eq_cols;   // tensor-core equalizer columns per CTA (0: 128)
   uint32_t fft_ctas;  // CTAs of each tensor-core FFT launch (0: one per SM)
+  bool eq_fused = false;  // the last uplink equalized inside the ZF kernel
   float2 *precoded;   // [D][M][N]
   const mb_mlp *zf_net;  // learned initial iterate of the mixed ZF (not owned), or null
   // mixed-precision downlink on the tensor cores (N = 4096): the BF16
@@ -310,6 +311,7 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
   }
   MARK(mk->pilot);
   float2 *prec = c.D ? s->precoder : nullptr;
+  s->eq_fused = false;
   if (mixed) {
     mb_zf_opts o{c.zf_precision, c.ns_iters, c.cond_threshold, s->zf_net ? 1u : 0u};
     ZfNetView v{};
@@ -317,9 +319,25 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
       r = mlp_zf_init_view(s->zf_net, &v);
       if (r != MB_OK) return r;
     }
+    // every uplink symbol already planarised by the combined FFT: the ZF
+    // kernel equalizes each group's columns itself, from the detector image
+    // in shared memory (shapes it cannot take fall back to two launches)
+    if (combined && nb0 == c.U) {
+      EqParams p;
+      r = equalize_prepare(p, reinterpret_cast<const mb_c32 *>(s->csi), reinterpret_cast<const mb_c32 *>(s->y_lp),
+                           c.K, c.M, c.S, c.sg, c.U, c.Qm, c.cb_size, c.cb_stride, c.zeros, 1, llr, hard, s->scr);
+      if (r != MB_OK) return r;
+      r = zf_mixed_eq_run(s->csi, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr, s->wmax, &v, p,
+                          s->y_lp, s->S_pad, c.U);
+      if (r == MB_OK) s->eq_fused = true;
+      else if (r != MB_UNSUPPORTED) return r;
+    }
     // W in FP32 only feeds the downlink precoder; the equalizer reads the image
-    r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr,
-                     s->wmax, &v);
+    if (!s->eq_fused)
+      r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr, s->wmax,
+                       &v);
+    else
+      r = MB_OK;
     if (r == MB_OK && prec) r = precoder_scale(s->csi, prec, s->wmax, c.M, c.K, s->G, cs);
     // the tensor-core downlink's BF16 precoder images, from the same precoder
     if (r == MB_OK && prec && s->pc_img) r = precoder_image(prec, s->pc_img, s->G, c.M, c.K, cs);
@@ -337,6 +355,13 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
     return MB_OK;
   }
   if (!mk && !combined) MB_CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
+  if (s->eq_fused) {
+    // equalized in the ZF stage (timing: an empty equalize stage)
+    MARK(mk->eq_b[0]);
+    MARK(mk->eq_e[0]);
+    MARK(mk->end);
+    return MB_OK;
+  }
   const uint64_t llr_sym = (uint64_t)c.K * c.cb_stride;
   const uint64_t hard_sym = (uint64_t)c.K * s->hrow;
   uint32_t bi = 0;
@@ -474,7 +499,7 @@ extern "C" mb_status mb_slot_stage_ms(mb_slot *s, double *out) {
       out[2] += ms(m.fft_b[bi], m.fft_e[bi]);
       out[5] += 1;
       out[3] += ms(m.eq_b[bi], m.eq_e[bi]);
-      out[6] += 1;
+      out[6] += s->eq_fused ? 0 : 1;  // no equalize launch of its own when fused
     }
     out[7] += 1;
   }

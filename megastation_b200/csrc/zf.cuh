@@ -3,6 +3,7 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "sgemv.cuh"
 
 namespace mb {
 
@@ -36,6 +37,17 @@ mb_status mlp_zf_init_view(const mb_mlp *n, ZfNetView *v);
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
                        const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
                        bool write_w = true, float *wmax = nullptr, const ZfNetView *net = nullptr);
+// the same ZF fused with the tensor-core equalizer: each CTA keeps its
+// group's detector image in shared memory and equalizes the group's
+// columns of nb symbols of planar BF16 samples y_lp [nb][re|im][M][S_pad]
+// into p's outputs (symbols 0..nb-1); MB_UNSUPPORTED when the shapes do
+// not allow it (K > 32, M > 256, sg % 16, more than one 128-column tile
+// per group, i.e. nb sg > 128), the caller then runs zf_mixed_run and
+// equalize_tc
+mb_status zf_mixed_eq_run(float2 *csi, uint32_t groups, uint32_t M, uint32_t K, const mb_zf_opts *opts,
+                          int32_t *status, float *cond, cudaStream_t st, bool write_w, float *wmax,
+                          const ZfNetView *net, const EqParams &p, const void *y_lp, uint32_t S_pad,
+                          uint32_t nb);
 // precoder P[g][u][b] = W[g][b][u] / wmax[g] from a precomputed per-group max
 mb_status precoder_scale(const float2 *W, float2 *P, const float *wmax, uint32_t M, uint32_t K,
                          uint32_t groups, cudaStream_t st);

@@ -32,9 +32,11 @@
 //     solve) and reported with status 2 (1 if even FP64 fails).
 #include <algorithm>
 #include <atomic>
+#include <cstring>
 
 #include "common.cuh"
 #include "eq_tc.cuh"
+#include "eq_tc_epi.cuh"
 #include "tc.cuh"
 #include "zf.cuh"
 
@@ -62,6 +64,11 @@ struct ZfmParams {
   uint32_t net_bulk;  // 1: the network's six arrays come into shared memory by bulk copies (MM == 64)
   uint32_t csi_nst;   // MM == 64: CSI k tiles staged by bulk copies, csi_nst at a time (0: register loads)
   float cond_thr;
+  // fused equalize (kernels with QMF > 0): the LLR layout and outputs of
+  // the group's eq_nb symbols, eq_spc of them per 128-column tile, eq_nct
+  // tiles; eq_N = 2K padded to 16
+  EqParams ep;
+  uint32_t eq_nb, eq_spc, eq_nct, eq_N;
 };
 
 __device__ __forceinline__ uint32_t img_off(uint32_t r, uint32_t kk, uint32_t MM) {
@@ -525,14 +532,21 @@ __device__ bool poly_init(const float2 *Gs, uint32_t ld, float2 *Xs, float2 *P2,
 }
 }  // namespace
 
-template <int MM>
-__global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1) zf_mixed_kernel(const ZfmParams q) {
+// QMF > 0: the fused form (MM == 64), which keeps the detector image in
+// shared memory and equalizes the group's symbols (modulation order QMF)
+// from the planar BF16 samples that ymap describes
+template <int MM, int QMF>
+__global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1)
+    zf_mixed_kernel(const ZfmParams q, const __grid_constant__ CUtensorMap ymap) {
+  static_assert(QMF == 0 || MM == 64, "the fused equalize needs K <= 32");
   extern __shared__ __align__(1024) uint8_t zsm[];
   __shared__ __align__(8) uint64_t tile_bar[2];
   __shared__ __align__(8) uint64_t mma_bar;
   __shared__ __align__(8) uint64_t stage_bar[4];  // CSI tiles staged by bulk copies
   __shared__ __align__(8) uint64_t net_bar;       // the network's weights
   __shared__ float ns_acc[2];                     // residual norms, alternating
+  __shared__ __align__(8) uint64_t eq_full[2], eq_empty[2], eq_done;  // fused equalize pipeline
+  __shared__ int eq_to;
   __shared__ uint32_t tmem_slot;
   __shared__ int flag, fail, piv_bad;
   __shared__ float red[kThreads], red2[kThreads];
@@ -572,7 +586,9 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1) zf_mixed_kernel(co
   uint8_t *wsm = reinterpret_cast<uint8_t *>(Gs + K * ld);
 
   float2 *cg = q.csi + (uint64_t)g * M * K;
-  uint8_t *imgw = q.img_w + (uint64_t)g * q.nkt * tile_bytes;
+  // the detector image: global memory, or (fused) shared memory from 0,
+  // over the tiles and the Gn images, which are free once W = X C is done
+  uint8_t *imgw = QMF ? zsm : q.img_w + (uint64_t)g * q.nkt * tile_bytes;
   // CSI k tile kt (64 antennas x K users, contiguous in [M][K]) staged in
   // the image region, which is free during the Gram
   const uint32_t nst = MM == 64 ? q.csi_nst : 0;
@@ -597,6 +613,15 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1) zf_mixed_kernel(co
     tc::mbar_init(&mma_bar, 1);
     for (int i = 0; i < 4; i++) tc::mbar_init(&stage_bar[i], 1);
     tc::mbar_init(&net_bar, 1);
+    if (QMF) {
+      for (int i = 0; i < 2; i++) {
+        tc::mbar_init(&eq_full[i], 1);
+        tc::mbar_init(&eq_empty[i], 1);
+      }
+      tc::mbar_init(&eq_done, 1);
+      eq_to = 0;
+      tc::prefetch_tmap(&ymap);
+    }
     tc::fence_mbar_init();
     fail = 0;
     piv_bad = 0;
@@ -1258,6 +1283,93 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1) zf_mixed_kernel(co
     if (q.cond) q.cond[g] = cond_est;
     if (fail && q.err) atomicOr(q.err, tc::kErrTimeout);
   }
+
+  // ------------------------------------------------ fused equalize (QMF)
+  // The tensor-core equalizer of eq_tc.cu on this group's columns, with
+  // the detector image from shared memory: D (128 x N) = Y (128 x 2Mp) A^T
+  // per tile of up to 128 (symbol, subcarrier) columns, the samples in
+  // 16-subcarrier x 64-antenna TMA boxes (32-byte swizzle) through two
+  // 16 KB stages behind the iterate's images, tile ct accumulating in TMEM
+  // columns 64 ct.  One thread loads, one issues the MMAs; then every
+  // thread runs the shared epilogue (demap, LLRs, descrambled hard bits).
+  if constexpr (QMF > 0) {
+    tc::fence_proxy_async_smem();  // the image's generic writes before the MMAs read it
+    tc::fence_before_sync();
+    __syncthreads();
+    if (!fail) {
+      const EqParams &p = q.ep;
+      constexpr uint32_t kCols = 128, y_tile = kCols * kKT * 2;
+      uint8_t *ystage = y_img;
+      const uint32_t s_base = g * p.sg, nct = q.eq_nct, total = nct * q.nkt;
+      auto tile_cols = [&](uint32_t ct) { return min(q.eq_spc, q.eq_nb - ct * q.eq_spc) * p.sg; };
+      uint32_t issued = 0;  // stage loads the loading thread issued
+      if (warp == 0 && lane == 0) {
+        tc::fence_after_sync();
+        for (uint32_t i = 0; i < total; i++) {
+          const uint32_t ct = i / q.nkt, kt = i % q.nkt, sgi = i % 2, use = i / 2;
+          if (use >= 1 && !tc::mbar_wait(&eq_empty[sgi], (use - 1) & 1)) {
+            eq_to = 1;
+            break;
+          }
+          const uint32_t ncols = tile_cols(ct), l_off = ct * q.eq_spc;
+          uint8_t *sy = ystage + sgi * y_tile;
+          tc::mbar_arrive_expect_tx(&eq_full[sgi], ncols * kKT * 2);
+          const uint32_t kk0 = kt * kKT, plane = kk0 / Mp, b0 = kk0 % Mp;
+          for (uint32_t j = 0; j < ncols / 16; j++) {
+            const uint32_t col0 = j * 16, l = col0 / p.sg, sl = col0 % p.sg;
+            const int32_t row = (int32_t)(((l_off + l) * 2 + plane) * M + b0);
+            tc::tma_load_2d(sy + j * 16 * 128, &ymap, (int32_t)(s_base + sl), row, &eq_full[sgi]);
+          }
+          issued = i + 1;
+        }
+      } else if (warp == 1 && lane == 0) {
+        const uint32_t idesc = tc::idesc_bf16(kCols, q.eq_N, true, false);
+        bool good = true;
+        for (uint32_t i = 0; i < total; i++) {
+          const uint32_t ct = i / q.nkt, kt = i % q.nkt, sgi = i % 2, use = i / 2;
+          if (!tc::mbar_wait(&eq_full[sgi], use & 1)) {
+            good = false;
+            break;
+          }
+          tc::fence_after_sync();
+          const uint32_t y0 = tc::smem_u32(ystage + sgi * y_tile), a0 = tc::smem_u32(zsm + kt * tile_bytes);
+#pragma unroll
+          for (int ks = 0; ks < kKT / 16; ks++) {
+            // Y: 32-byte atoms of 16 columns 2048 B apart, 8-antenna K groups
+            // 256 B apart; image: K core matrices 128 B apart, row groups 1024 B
+            const uint64_t yd = tc::smem_desc_mn_sw32(y0 + ks * 512, 2048, 256);
+            const uint64_t ad = tc::smem_desc(a0 + ks * 256, 128, 1024);
+            tc::mma_f16(tmem + ct * 64, yd, ad, idesc, (kt | ks) != 0);
+          }
+          tc::mma_commit(&eq_empty[sgi]);
+        }
+        // eq_done also after a wait that gave up: it then marks the end of
+        // the MMAs that were issued
+        tc::mma_commit(&eq_done);
+        if (!good) eq_to = 1;
+      }
+      __syncwarp();
+      // everyone: wait for the accumulators (bounded), then the epilogues
+      const bool got = tc::mbar_wait(&eq_done, 0);
+      if (__syncthreads_or(!got || eq_to)) {
+        // give up: the loads still in flight land before the CTA exits.  A
+        // stage is reloaded only after its previous load was consumed, so
+        // those are among the last two issued, each the current phase of
+        // its stage.
+        if (warp == 0 && lane == 0)
+          for (uint32_t i = issued >= 2 ? issued - 2 : 0u; i < issued; i++)
+            tc::mbar_wait(&eq_full[i % 2], (i / 2) & 1);
+        if (tid == 0 && q.err) atomicOr(q.err, tc::kErrTimeout);
+      } else {
+        tc::fence_after_sync();
+        for (uint32_t ct = 0; ct < nct; ct++) {
+          EqTcEpilogue<64, QMF == 0 ? 2 : QMF> epi;
+          epi.prepare(p, s_base, ct * q.eq_spc, tile_cols(ct), 0, q.eq_N, warp, lane);
+          epi.run(p, tmem + ct * 64, warp, lane);
+        }
+      }
+    }
+  }
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, TC);
@@ -1284,9 +1396,30 @@ uint64_t zf_mixed_scratch_bytes(uint32_t groups, uint32_t M, uint32_t K) {
   return (uint64_t)groups * s.img_group_bytes;
 }
 
-mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
-                       const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
-                       bool write_w, float *wmax, const ZfNetView *net) {
+using ZfmKernel = void (*)(const ZfmParams, const CUtensorMap);
+
+static ZfmKernel zfm_kernel_of(uint32_t MM, uint32_t qmf, int *which) {
+  switch (MM == 64 ? qmf : 0) {
+    case 2: *which = 2; return zf_mixed_kernel<64, 2>;
+    case 4: *which = 3; return zf_mixed_kernel<64, 4>;
+    case 6: *which = 4; return zf_mixed_kernel<64, 6>;
+    case 8: *which = 5; return zf_mixed_kernel<64, 8>;
+    default: break;
+  }
+  *which = MM == 64 ? 0 : 1;
+  return MM == 64 ? zf_mixed_kernel<64, 0> : zf_mixed_kernel<128, 0>;
+}
+
+// the fused equalize of zf_mixed_eq_run
+struct ZfmFused {
+  const EqParams *p;
+  const void *y_lp;
+  uint32_t S_pad, nb;
+};
+
+static mb_status zf_mixed_launch(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
+                                 const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
+                                 bool write_w, float *wmax, const ZfNetView *net, const ZfmFused *fe) {
   if (K == 0 || K > 64) return MB_UNSUPPORTED;
   const bool learned = opts && opts->init == 1;
   if (opts && opts->init > 1) return MB_BAD_ARG;
@@ -1294,7 +1427,7 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
   const TcShape s = tc_shape(M, K);
   const DeviceTables *tab = device_tables();
   if (!tab) return MB_CUDA_ERROR;
-  ZfmParams q;
+  ZfmParams q{};
   q.net = learned ? *net : ZfNetView{};
   q.learned = learned ? 1 : 0;
   q.csi = csi;
@@ -1320,24 +1453,49 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
   q.csi_nst = 0;
   if (s.MM == 64 && K % 2 == 0 && a16(csi))
     q.csi_nst = std::min<uint32_t>(4, 4 * kSqImg / (kKT * K * (uint32_t)sizeof(float2)));
+  // the fused equalize: K <= 32, at most 256 antennas (the whole detector
+  // image, 2 Mp / 64 k tiles of 8 KB, in shared memory over the tiles),
+  // whole 16-subcarrier boxes per group, at most four 128-column tiles
+  uint32_t qmf = 0;
+  CUtensorMap ymap;
+  memset(&ymap, 0, sizeof(ymap));
+  if (fe) {
+    const EqParams &p = *fe->p;
+    if (s.MM != 64 || q.nh > 4 || p.sg == 0 || p.sg % 16 || p.sg > 128 || fe->nb == 0 ||
+        !(p.Qm == 2 || p.Qm == 4 || p.Qm == 6 || p.Qm == 8) || fe->S_pad % 8 || fe->S_pad < p.S ||
+        p.M != M || p.K != K)
+      return MB_UNSUPPORTED;
+    const uint32_t spc_max = 128 / p.sg, ny = (fe->nb + spc_max - 1) / spc_max;
+    q.eq_spc = (fe->nb + ny - 1) / ny;
+    q.eq_nct = (fe->nb + q.eq_spc - 1) / q.eq_spc;
+    // one 128-column tile per group: with two (or more) the CTA's two 16 KB
+    // sample stages leave the loads latency-bound and the separate
+    // equalizer (three CTAs of three stages per SM) is faster (measured at
+    // 256x32: fused -2.4 / -3.0 / -0.4 us per slot at 2 / 4 / 8 symbols,
+    // +13.5 us at 12)
+    if (q.eq_nct > 1) return MB_UNSUPPORTED;
+    q.eq_nb = fe->nb;
+    q.eq_N = (2 * K + 15) / 16 * 16;
+    q.ep = p;
+    qmf = p.Qm;
+    // rows [nb][re|im][M] of S_pad subcarriers; boxes of 16 x 64, 32-byte swizzle
+    mb_status tr = make_tmap_2d_bf16(&ymap, fe->y_lp, fe->S_pad, (uint64_t)fe->nb * 2 * M, fe->S_pad, 16, kKT,
+                                     true);
+    if (tr != MB_OK) return tr;
+  }
   int dev = 0, maxs = 0;
   MB_CUDA_TRY(cudaGetDevice(&dev));
   MB_CUDA_TRY(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  static std::atomic<uint64_t> configured[2] = {{0}, {0}};
-  static std::atomic<int> static_smem[2] = {{0}, {0}};
-  const int which = s.MM == 64 ? 0 : 1;
+  static std::atomic<uint64_t> configured[6] = {};
+  static std::atomic<int> static_smem[6] = {};
+  int which = 0;
+  const ZfmKernel kern = zfm_kernel_of(s.MM, qmf, &which);
   const uint64_t bit = 1ull << (dev & 63);
   if (!(configured[which].load() & bit)) {
     cudaFuncAttributes fa;
-    if (which == 0) {
-      MB_CUDA_TRY(cudaFuncGetAttributes(&fa, zf_mixed_kernel<64>));
-      MB_CUDA_TRY(cudaFuncSetAttribute(zf_mixed_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       maxs - (int)fa.sharedSizeBytes));
-    } else {
-      MB_CUDA_TRY(cudaFuncGetAttributes(&fa, zf_mixed_kernel<128>));
-      MB_CUDA_TRY(cudaFuncSetAttribute(zf_mixed_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       maxs - (int)fa.sharedSizeBytes));
-    }
+    MB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    MB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     maxs - (int)fa.sharedSizeBytes));
     static_smem[which] = (int)fa.sharedSizeBytes;
     configured[which].fetch_or(bit);
   }
@@ -1346,15 +1504,31 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
   const uint32_t width = learned ? net->width : 0;
   q.resident = zfm_smem(K, s.MM, q.nh, learned, width) <= avail ? 1 : 0;
   q.write_w = write_w ? 1 : 0;
-  const size_t smem = zfm_smem(K, s.MM, q.resident ? q.nh : 2, learned, width);
+  size_t smem = zfm_smem(K, s.MM, q.resident ? q.nh : 2, learned, width);
+  if (qmf) {
+    // the two 16 KB sample stages behind the Gn images
+    if (!q.resident) return MB_UNSUPPORTED;
+    smem = std::max(smem, (size_t)(q.nh + 2) * s.MM * kKT * 2 + 2 * kSqImg + 2 * 128 * kKT * 2);
+  }
   if (smem > avail) return MB_UNSUPPORTED;
   if (groups == 0) return MB_OK;
-  if (s.MM == 64)
-    zf_mixed_kernel<64><<<groups, kThreads, smem, st>>>(q);
-  else
-    zf_mixed_kernel<128><<<groups, kThreads, smem, st>>>(q);
+  kern<<<groups, kThreads, smem, st>>>(q, ymap);
   MB_LAUNCH_CHECK();
   return MB_OK;
+}
+
+mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
+                       const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
+                       bool write_w, float *wmax, const ZfNetView *net) {
+  return zf_mixed_launch(csi, img_w, groups, M, K, opts, status, cond, st, write_w, wmax, net, nullptr);
+}
+
+mb_status zf_mixed_eq_run(float2 *csi, uint32_t groups, uint32_t M, uint32_t K, const mb_zf_opts *opts,
+                          int32_t *status, float *cond, cudaStream_t st, bool write_w, float *wmax,
+                          const ZfNetView *net, const EqParams &p, const void *y_lp, uint32_t S_pad,
+                          uint32_t nb) {
+  const ZfmFused fe{&p, y_lp, S_pad, nb};
+  return zf_mixed_launch(csi, nullptr, groups, M, K, opts, status, cond, st, write_w, wmax, net, &fe);
 }
 
 }  // namespace mb

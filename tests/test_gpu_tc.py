@@ -217,6 +217,52 @@ def test_slot_uplink_mixed_vs_oracle(mb, case):
         assert np.abs(llr[l].astype(np.float32) - lr).max() <= 1.0 + 0.02 * np.abs(lr).max()
 
 
+def test_slot_fuses_zf_and_equalize(mb):
+    # with every uplink symbol in one batch (and the FFT of pilots and
+    # symbols in one launch) the ZF kernel equalizes itself: no equalize
+    # launch of its own in the stage record; split batches keep two kernels
+    from megastation_b200 import datagen, slot
+    cfg = datagen.CellConfig(M=64, K=16, N=4096, S=3276, sg=16, Qm=6, U=3, snr_db=25.0, seed=31)
+    iq = torch.from_numpy(datagen.make_slot(cfg)["iq"]).cuda()
+    for sym_batch, n_eq in ((3, 0), (2, 2)):
+        run = slot.UplinkSlot(cfg, precision="mixed", sym_batch=sym_batch)
+        run.timing(1)
+        run(iq)
+        st = run.stage_ms()
+        assert st["n_eq"] == n_eq, (sym_batch, st)
+    assert mb.ops.device_error() == 0
+
+
+def test_fused_slot_fp64_groups_vs_oracle(mb):
+    # a condition threshold below 1 sends every group down the FP64 path,
+    # whose detector image the fused equalize reads from shared memory
+    from megastation_b200 import datagen, slot
+    cfg = datagen.CellConfig(M=64, K=16, N=4096, S=3276, sg=16, Qm=4, U=3, snr_db=25.0, seed=32)
+    d = datagen.make_slot(cfg)
+    run = slot.UplinkSlot(cfg, precision="mixed", sym_batch=cfg.U, cond_threshold=0.5)
+    llr, hard = run(torch.from_numpy(d["iq"]).cuda())
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    assert (run.status.cpu().numpy() == 2).all()
+    llr, hard = llr.cpu().numpy(), hard.cpu().numpy()
+    cb, zeros, stride = cfg.ldpc()
+    n_valid = min(cb, cfg.S * cfg.Qm)
+    ps = orc.pilot_sign(cfg.S)
+    csi = np.zeros((cfg.G, cfg.M, cfg.K), np.complex64)
+    for p in range(cfg.P):
+        orc.pilot_fft(d["iq"][p], cfg.N, cfg.S, cfg.start, cfg.K, cfg.sg, p * cfg.sg, ps, csi)
+    W = orc.zf(csi, S=cfg.S, sg=cfg.sg)
+    for l in range(cfg.U):
+        y = orc.uplink_fft(d["iq"][cfg.P + l], cfg.N, cfg.S, cfg.start)
+        llr_r, _, hard_r = orc.equalize(W, y, cfg.sg, cfg.Qm, cb, stride, zeros, seq=d["seq"][0])
+        lr = llr_r.astype(np.float32)
+        sure = np.abs(lr[:, zeros:zeros + n_valid]) > 4.0
+        bg = np.unpackbits(hard[l], axis=1)[:, :n_valid]
+        br = np.unpackbits(hard_r, axis=1)[:, :n_valid]
+        assert (bg[sure] == br[sure]).all()
+        assert np.abs(llr[l].astype(np.float32) - lr).max() <= 1.0 + 0.02 * np.abs(lr).max()
+
+
 def test_zf_mixed_forced_fp64_path(mb):
     # a condition threshold below 1 sends every group down the FP64 path
     M, K, G = 96, 16, 4
