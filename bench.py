@@ -53,6 +53,10 @@ def parse():
                     help="cells32: 32 seeded uneven cells in one graph launch per slot (autotuned); "
                          "full256x64: uplink + downlink slot, 256-QAM, latency percentiles; "
                          "learned128x16: per-subcarrier ZF with the learned initialiser")
+    ap.add_argument("--uplink-symbols", type=int, default=None,
+                    help="data symbols per slot of the cell256x32 workload (default 12, the headline); "
+                         "with --sym-batch at least as large and U x 16 <= 128 the slot equalizes "
+                         "inside its ZF kernel")
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed"])
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 path")
     ap.add_argument("--no-evm", action="store_true")
@@ -338,7 +342,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     datagen = _standalone_datagen()
-    cfg = datagen.CellConfig(**{**WORKLOAD, "iq_dtype": args.iq})
+    cfg = datagen.CellConfig(**{**workload_dict(args), "iq_dtype": args.iq})
     from oracle import ref_ops
     cb, zeros, stride = cfg.ldpc()
     import torch
@@ -609,9 +613,15 @@ def rotation(cfg, args):
     return max(2, args.rotate, -(-int(1.25 * 126e6) // slot_bytes))
 
 
+def workload_dict(args):
+    """The cell256x32 workload, with --uplink-symbols data symbols when given."""
+    u = getattr(args, "uplink_symbols", None)
+    return {**WORKLOAD, "U": u} if u else dict(WORKLOAD)
+
+
 def workload_config(cfg, args, R=None):
     R = rotation(cfg, args) if R is None else R
-    return {"workload": "uplink slot 256x32, N=4096, S=3276, 2 pilot + 12 data symbols, 64-QAM, "
+    return {"workload": f"uplink slot 256x32, N=4096, S=3276, 2 pilot + {cfg.U} data symbols, 64-QAM, "
                         f"8-tap exp-PDP rho=0.5, 25 dB, {cfg.iq_dtype} samples",
             "M": cfg.M, "K": cfg.K, "N": cfg.N, "S": cfg.S, "sg": cfg.sg, "Qm": cfg.Qm, "P": cfg.P,
             "U": cfg.U, "iq_dtype": cfg.iq_dtype, "precision": args.precision, "sym_batch": args.sym_batch,
@@ -958,7 +968,7 @@ def main():
 
     import megastation_b200 as mb
     from megastation_b200 import datagen, slot
-    cfg = datagen.CellConfig(**{**WORKLOAD, "iq_dtype": args.iq})
+    cfg = datagen.CellConfig(**{**workload_dict(args), "iq_dtype": args.iq})
     d = datagen.make_slot(cfg)
     cb, zeros, stride = cfg.ldpc()
     n_valid = min(cfg.S * cfg.Qm, cb)
