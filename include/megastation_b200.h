@@ -399,6 +399,16 @@ mb_status mb_slot_uplink(mb_slot *slot, const void *iq, uint16_t *llr,
 mb_status mb_slot_downlink(mb_slot *slot, const mb_c32 *symbols, void *out,
                            void *stream);
 
+/* The downlink branch of BandProcess::process (baseband/process.cc:196-214)
+ * from encoded bits: Modulation::modulate of each downlink symbol's K user
+ * rows (bits [D][K][in_bytes], in_bytes >= ceil(S Qm / 8); stream bit t is
+ * bit t % 8 of byte t / 8, and the first of a subcarrier's Qm bits is the
+ * MSB of its QAM index, modulation.cu:115-128), then mb_slot_downlink.  The
+ * reference scrambles and LDPC-encodes the MAC bits before (process.cc:
+ * 198-201); those bits come from the caller's encoder. */
+mb_status mb_slot_downlink_bits(mb_slot *slot, const uint8_t *bits, uint64_t in_bytes, void *out,
+                                void *stream);
+
 /* Single-GPU slot pipeline over host buffers (scheduler/gpu_engine.cc:77-437
  * and cpu_buffer.cc:5-49 for one GPU): each submitted slot's samples are
  * copied to a ring of `depth` device buffers, the slot runs (an mb_slot

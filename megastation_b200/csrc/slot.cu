@@ -45,6 +45,7 @@ struct mb_slot {
   // the FP16 precoded spectra [D][M][N], whose guard bins stay zero
   void *pc_img;
   void *z16;
+  mb_c32 *dl_sym;  // [D][K][S] modulated symbols of mb_slot_downlink_bits
   cudaStream_t side;
   cudaStream_t crit;  // pilot FFT -> ZF: the critical path, at the highest stream priority
   cudaEvent_t ev_fork, ev_join, ev_crit;
@@ -135,6 +136,7 @@ extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   cudaFree(s->precoded);
   cudaFree(s->pc_img);
   cudaFree(s->z16);
+  cudaFree(s->dl_sym);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->crit) cudaStreamDestroy(s->crit);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
@@ -180,6 +182,7 @@ static mb_status slot_create(const mb_cell_desc *cell, bool sb_cap_all, mb_slot 
   alloc((void **)&s->precoder, sizeof(float2) * gmk);
   if (c.D) alloc((void **)&s->wmax, sizeof(float) * s->G);
   alloc((void **)&s->precoded, sizeof(float2) * (size_t)c.D * c.M * c.N);
+  alloc((void **)&s->dl_sym, sizeof(mb_c32) * (size_t)c.D * c.K * c.S);
   if (c.D && c.zf_precision == MB_ZF_MIXED && c.N == 4096 && precode_tc_supported(c.K, c.sg) &&
       (c.out_dtype == MB_IQ_I16 || c.out_dtype == MB_IQ_I8 || c.out_dtype == MB_IQ_F16)) {
     alloc(&s->pc_img, (size_t)s->G * precode_tc_shape(c.M, c.K).img_group_bytes);
@@ -468,6 +471,19 @@ extern "C" mb_status mb_slot_downlink(mb_slot *s, const mb_c32 *symbols,
   if (r != MB_OK) return r;
   return mb_ifft_downlink(s->fft, reinterpret_cast<const mb_c32 *>(s->precoded), c.D,
                           out, c.out_dtype, st);
+}
+
+extern "C" mb_status mb_slot_downlink_bits(mb_slot *s, const uint8_t *bits, uint64_t in_bytes, void *out,
+                                           void *stream) {
+  if (!s || !bits || !out) return MB_BAD_ARG;
+  const mb_cell_desc &c = s->c;
+  if (!c.D || !s->dl_sym) return MB_BAD_SHAPE;
+  // every user row holds at least the S Qm bits of its symbol
+  if (in_bytes < ((uint64_t)c.S * c.Qm + 7) / 8) return MB_BAD_SHAPE;
+  // the D symbols' K user rows are independent: one modulate launch
+  mb_status r = mb_modulate(bits, s->dl_sym, in_bytes, c.S, (uint64_t)c.D * c.K, c.Qm, 0, nullptr, stream);
+  if (r != MB_OK) return r;
+  return mb_slot_downlink(s, s->dl_sym, out, stream);
 }
 
 extern "C" mb_status mb_slot_timing(mb_slot *s, uint32_t max_calls) {

@@ -55,6 +55,13 @@ class UplinkSlot:
               "mb_slot_downlink")
         return out
 
+    def downlink_bits(self, bits, out, stream=None):
+        """The downlink from encoded bits [D][K][in_bytes] (uint8): modulate,
+        precode, inverse FFT (mb_slot_downlink_bits)."""
+        check(LIB.mb_slot_downlink_bits(self._h, _dev(bits, "bits"), bits.shape[-1], _dev(out, "out"),
+                                        _stream(stream)), "mb_slot_downlink_bits")
+        return out
+
     def set_zf_init(self, net):
         """Mixed ZF from the learned polynomial initial iterate of `net` (a
         learned.MLP with 6 inputs and 4 outputs); None: the exact inverse.

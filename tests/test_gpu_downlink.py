@@ -77,3 +77,37 @@ def test_slot_downlink_vs_oracle(case, precision, out_dtype):
     if out_dtype == "f16":
         spec = np.fft.fft(got[..., 0] + 1j * got[..., 1], axis=-1)
         assert np.abs(spec[..., guard]).max() <= 1e-2 * np.abs(spec[..., ~guard]).max()
+
+
+def test_slot_downlink_from_bits_vs_oracle():
+    # mb_slot_downlink_bits: encoded bits -> the oracle's modulation
+    # (modulation.cu:115-128), precoding and inverse FFT; row length padded
+    # past ceil(S Qm / 8) to check the stride
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import megastation_b200 as mb
+    from megastation_b200 import datagen, slot
+    cfg = datagen.CellConfig(**SMALL)
+    d = datagen.make_slot(cfg)
+    D = 2
+    in_bytes = (cfg.S * cfg.Qm + 7) // 8 + 5
+    rng = np.random.default_rng(cfg.seed + 2)
+    bits = rng.integers(0, 256, (D, cfg.K, in_bytes), dtype=np.uint8)
+    run = slot.UplinkSlot(cfg, precision="mixed", sym_batch=cfg.U, D=D, out_dtype="int16")
+    out = torch.zeros(D, cfg.M, cfg.N, 2, dtype=torch.int16, device="cuda")
+    run(torch.from_numpy(d["iq"]).cuda())
+    run.downlink_bits(torch.from_numpy(bits).cuda(), out)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    W, _ = oracle_uplink(cfg, d)
+    syms = np.stack([orc.modulate(bits[l], cfg.S, cfg.Qm) for l in range(D)])
+    ref = _downlink_ref(cfg, W, syms, np.int16).astype(np.float32)
+    got = out.cpu().numpy().astype(np.float32)
+    rms = np.sqrt(np.mean(ref ** 2))
+    assert rms > 1.0
+    # W from BF16 operands (about 2^-9 relative), one LSB of output rounding
+    assert np.sqrt(np.mean((got - ref) ** 2)) <= 1e-2 * rms + 1.0
+    # too short a row is refused
+    from megastation_b200._lib import MbError
+    with pytest.raises(MbError):
+        run.downlink_bits(torch.from_numpy(bits[..., :in_bytes - 6].copy()).cuda(), out)
