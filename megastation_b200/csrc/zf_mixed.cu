@@ -47,6 +47,7 @@ constexpr int kKT = 64;        // reduction elements per k tile
 constexpr float kPolyAccept = 0.04f;  // ||I - G X||_F before the last step of an accepted learned iterate
 constexpr int kThreads = 256;  // 8 warps; warps w and w+4 share TMEM lane quadrant w
 constexpr uint32_t kZfStageWidth = 64;  // networks up to this width are staged in shared memory
+constexpr uint32_t kTcMinK = 16;        // K above this (and <= 32): the inverse's products on the tensor cores
 
 struct ZfmParams {
   ZfNetView net;      // network of the learned initial iterate (used when learned)
@@ -565,12 +566,16 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1)
   // shared memory carve-up
   uint8_t *hi_base = zsm;
   uint8_t *lo_t[2] = {zsm + HS * tile_bytes, zsm + (HS + 1) * tile_bytes};
-  // MM == 64 (K <= 32): the inverse on the tensor cores.  Behind the tiles
-  // the split images of Gn = G / tau and of the iterate Y = tau X, then G
-  // (K x ld), then K x ld float2 more (the FP64 fallback's Gram spans both)
-  // that hold the network's weights when the kernel runs learned.  X of the
-  // exact start and the residual's image go in the lo tiles; W = X C reads
-  // the iterate's hi image.
+  // MM == 64 (K <= 32): behind the tiles the split images of Gn = G / tau
+  // and of the iterate Y = tau X, then G (K x ld), then K x ld float2 more
+  // (the FP64 fallback's Gram spans both) that hold the network's weights
+  // when the kernel runs learned.  With the inverse on the tensor cores
+  // (16 < K <= 32) X of the exact start and the residual's image go in the
+  // lo tiles and W = X C reads the iterate's hi image; with the CUDA-core
+  // products (K <= 16: a 16 x 16 product is a fraction of one tensor-core
+  // round trip) X and the powers Gn^2, Gn^3 take the Gn images' place and
+  // R(X) the iterate's.
+  const bool tcns = MM == 64 && K > kTcMinK;  // uniform
   uint8_t *gn_img = zsm + (HS + 2) * tile_bytes;
   uint8_t *y_img = gn_img + 2 * kSqImg;
   // MM == 128: R(X) (MM x MM BF16), G, X, and the powers Gn^2, Gn^3 of the
@@ -579,7 +584,7 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1)
   // iterate in the R(X) image (both free between the Gram and W = X C)
   uint8_t *ximg = MM == 64 ? y_img : zsm + (HS + 2) * tile_bytes;
   float2 *Gs = reinterpret_cast<float2 *>(MM == 64 ? y_img + 2 * kSqImg : ximg + MM * MM * 2);
-  float2 *Xs = MM == 64 ? reinterpret_cast<float2 *>(lo_t[0]) : Gs + K * ld;
+  float2 *Xs = MM == 64 ? reinterpret_cast<float2 *>(tcns ? lo_t[0] : gn_img) : Gs + K * ld;
   float2 *Ts = reinterpret_cast<float2 *>(lo_t[0]);
   float2 *Xn = reinterpret_cast<float2 *>(ximg);
   float2 *P2 = Xs + K * ld, *P3 = P2 + K * K;
@@ -793,8 +798,8 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1)
     }
     tc::fence_before_sync();
     __syncthreads();
-    if constexpr (MM == 64) {
-      // ---- the inverse on the tensor cores (K <= 32)
+    if (tcns) {
+      // ---- the inverse on the tensor cores (16 < K <= 32)
       uint8_t *gh = gn_img, *gl = gn_img + kSqImg, *yh = y_img, *yl = y_img + kSqImg;
       uint8_t *eimg = lo_t[0];  // E = I - Gn Y (hi only)
       const uint32_t two_k = 2 * K;
@@ -1018,7 +1023,7 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1)
     } else {
       bool pd = false;
       if (q.learned)
-        used_learned = poly_init<MM>(Gs, ld, Xs, P2, P3, Ts, Xn, K, M, q.net, q.ns_iters, zi_red, zi_act, zi_coef);
+        used_learned = poly_init<MM>(Gs, ld, Xs, P2, P3, Ts, Xn, K, M, netv, q.ns_iters, zi_red, zi_act, zi_coef);
       if (!used_learned) {
         if (MM == 64)
           pd = K <= 16 ? gj_inverse<16>(Gs, Xs, K, ld, prow, &piv_bad)
@@ -1103,7 +1108,7 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1)
     // R(X) image, K-major over the reduction index 2v + rj; rows/columns
     // beyond 2K are padding and stay zero.  MM == 64: the iterate's hi image
     // R(Y) = tau R(X) is already there (the epilogue scales by 1 / tau).
-    if constexpr (MM != 64) {
+    if (!tcns) {
       for (uint32_t c = tid; c < MM * MM * 2 / 16; c += kThreads)
         reinterpret_cast<uint4 *>(ximg)[c] = make_uint4(0, 0, 0, 0);
       __syncthreads();
