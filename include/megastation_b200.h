@@ -499,6 +499,14 @@ mb_status mb_cells_get_tuning(const mb_cells *cells, uint32_t *sym_batch, uint32
  * 74, 37 and 18 per class after the other knobs. */
 mb_status mb_cells_get_fft_ctas(const mb_cells *cells, uint32_t *fft_ctas);
 mb_status mb_cells_set_fft_ctas(mb_cells *cells, const uint32_t *fft_ctas);
+/* The fourth knob, per cell: where the mixed-precision ZF's inverse runs
+ * its matrix products when K <= 32 -- 0 by K (the tensor cores for
+ * 16 < K, the CUDA cores below; the default), 1 the CUDA cores, 2 the
+ * tensor cores (tcgen05, split-BF16 operands, FP32 accumulation; its
+ * round trips cost more than a small group's products).  mb_cells_autotune
+ * tries the choice the rule did not make per class, last. */
+mb_status mb_cells_get_zf_path(const mb_cells *cells, uint32_t *zf_path);
+mb_status mb_cells_set_zf_path(mb_cells *cells, const uint32_t *zf_path);
 mb_status mb_cells_set_tuning(mb_cells *cells, const uint32_t *sym_batch,
                               const uint32_t *eq_cols);
 

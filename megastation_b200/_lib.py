@@ -140,6 +140,8 @@ def _load():
         "mb_cells_get_tuning": (ST, [VP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
         "mb_cells_get_fft_ctas": (ST, [VP, ctypes.POINTER(U32)]),
         "mb_cells_set_fft_ctas": (ST, [VP, ctypes.POINTER(U32)]),
+        "mb_cells_get_zf_path": (ST, [VP, VP]),
+        "mb_cells_set_zf_path": (ST, [VP, VP]),
         "mb_cells_set_tuning": (ST, [VP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
     }
     for name, (res, args) in sigs.items():

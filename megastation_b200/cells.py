@@ -55,9 +55,9 @@ class Cells:
         return llr, hard
 
     def autotune(self, iqs, reps=20, stream=None):
-        """Picks sym_batch, equalizer columns per CTA and the tensor-core
-        FFT's CTAs per launch per cell class by timing the batched slot;
-        returns (per-cell choices, us per slot)."""
+        """Picks sym_batch, equalizer columns per CTA, the tensor-core FFT's
+        CTAs per launch and the mixed ZF's product path per cell class by
+        timing the batched slot; returns (per-cell choices, us per slot)."""
         n = len(self.cfgs)
         sb, cols = (ctypes.c_uint32 * n)(), (ctypes.c_uint32 * n)()
         us = ctypes.c_double()
@@ -67,10 +67,11 @@ class Cells:
 
     def tuning(self):
         n = len(self.cfgs)
-        sb, cols, fc = (ctypes.c_uint32 * n)(), (ctypes.c_uint32 * n)(), (ctypes.c_uint32 * n)()
+        sb, cols, fc, zp = [(ctypes.c_uint32 * n)() for _ in range(4)]
         check(LIB.mb_cells_get_tuning(self._h, sb, cols), "mb_cells_get_tuning")
         check(LIB.mb_cells_get_fft_ctas(self._h, fc), "mb_cells_get_fft_ctas")
-        return [{"sym_batch": sb[i], "eq_cols": cols[i], "fft_ctas": fc[i]} for i in range(n)]
+        check(LIB.mb_cells_get_zf_path(self._h, zp), "mb_cells_get_zf_path")
+        return [{"sym_batch": sb[i], "eq_cols": cols[i], "fft_ctas": fc[i], "zf_path": zp[i]} for i in range(n)]
 
     def set_tuning(self, choices):
         n = len(self.cfgs)
@@ -80,3 +81,6 @@ class Cells:
         if all("fft_ctas" in c for c in choices):
             fc = (ctypes.c_uint32 * n)(*[c["fft_ctas"] for c in choices])
             check(LIB.mb_cells_set_fft_ctas(self._h, fc), "mb_cells_set_fft_ctas")
+        if all("zf_path" in c for c in choices):
+            zp = (ctypes.c_uint32 * n)(*[c["zf_path"] for c in choices])
+            check(LIB.mb_cells_set_zf_path(self._h, zp), "mb_cells_set_zf_path")

@@ -37,6 +37,7 @@ struct mb_slot {
   uint32_t sb_cap;    // uplink symbols the y / y_lp buffers hold (>= sym_batch)
   uint32_t eq_cols;   // tensor-core equalizer columns per CTA (0: 128)
   uint32_t fft_ctas;  // CTAs of each tensor-core FFT launch (0: one per SM)
+  uint32_t zf_path;   // mixed ZF, K <= 32: 0 by K, 1 CUDA-core products, 2 tensor-core products
   bool eq_fused = false;  // the last uplink equalized inside the ZF kernel
   float2 *precoded;   // [D][M][N]
   const mb_mlp *zf_net;  // learned initial iterate of the mixed ZF (not owned), or null
@@ -165,6 +166,7 @@ static mb_status slot_create(const mb_cell_desc *cell, bool sb_cap_all, mb_slot 
   s->sb_cap = sb_cap_all ? std::max<uint32_t>(c.U, 1) : s->c.sym_batch;
   s->eq_cols = 0;
   s->fft_ctas = 0;
+  s->zf_path = 0;
   s->G = (c.S + c.sg - 1) / c.sg;
   s->n_valid = std::min<uint64_t>((uint64_t)c.S * c.Qm, c.cb_size);
   s->hrow = (s->n_valid + 7) / 8;
@@ -331,14 +333,14 @@ static mb_status issue_uplink(mb_slot *s, const void *iq, uint16_t *llr,
                            c.K, c.M, c.S, c.sg, c.U, c.Qm, c.cb_size, c.cb_stride, c.zeros, 1, llr, hard, s->scr);
       if (r != MB_OK) return r;
       r = zf_mixed_eq_run(s->csi, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr, s->wmax, &v, p,
-                          s->y_lp, s->S_pad, c.U);
+                          s->y_lp, s->S_pad, c.U, s->zf_path);
       if (r == MB_OK) s->eq_fused = true;
       else if (r != MB_UNSUPPORTED) return r;
     }
     // W in FP32 only feeds the downlink precoder; the equalizer reads the image
     if (!s->eq_fused)
       r = zf_mixed_run(s->csi, s->img_w, s->G, c.M, c.K, &o, status, nullptr, cs, prec != nullptr, s->wmax,
-                       &v);
+                       &v, s->zf_path);
     else
       r = MB_OK;
     if (r == MB_OK && prec) r = precoder_scale(s->csi, prec, s->wmax, c.M, c.K, s->G, cs);
@@ -720,6 +722,21 @@ extern "C" mb_status mb_cells_set_fft_ctas(mb_cells *cs, const uint32_t *fft_cta
   return MB_OK;
 }
 
+extern "C" mb_status mb_cells_get_zf_path(const mb_cells *cs, uint32_t *zf_path) {
+  if (!cs || !zf_path) return MB_BAD_ARG;
+  for (size_t c = 0; c < cs->slots.size(); c++) zf_path[c] = cs->slots[c]->zf_path;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_cells_set_zf_path(mb_cells *cs, const uint32_t *zf_path) {
+  if (!cs || !zf_path) return MB_BAD_ARG;
+  for (size_t c = 0; c < cs->slots.size(); c++)
+    if (zf_path[c] > 2) return MB_BAD_ARG;
+  for (size_t c = 0; c < cs->slots.size(); c++) cs->slots[c]->zf_path = zf_path[c];
+  cells_drop_graphs(cs);  // the captured launches change
+  return MB_OK;
+}
+
 // microseconds per slot of the current tuning: warm-up, then reps graph
 // launches timed with CUDA events on st
 static mb_status cells_time(mb_cells *cs, const void *const *iq, uint16_t *const *llr,
@@ -865,6 +882,30 @@ extern "C" mb_status mb_cells_autotune(mb_cells *cs, const void *const *iq, uint
     for (uint32_t c : members[k]) fc[c] = cur;
   }
   if (r == MB_OK) r = mb_cells_set_fft_ctas(cs, fc.data());
+  // where the mixed ZF's inverse runs its products (K <= 32): the CUDA or
+  // the tensor cores, from the rule by K
+  std::vector<uint32_t> zp(n, 0);
+  if (r == MB_OK) r = mb_cells_set_zf_path(cs, zp.data());
+  for (uint32_t k : order) {
+    if (r != MB_OK) break;
+    const mb_cell_desc &d = cs->slots[members[k][0]]->c;
+    if (d.zf_precision != MB_ZF_MIXED || d.K > 32) continue;
+    uint32_t cur = 0;
+    for (uint32_t cand : {1u, 2u}) {
+      if ((cand == 2) == (d.K > 16)) continue;  // the rule's choice is the current one
+      for (uint32_t c : members[k]) zp[c] = cand;
+      double t = 0.0;
+      r = mb_cells_set_zf_path(cs, zp.data());
+      if (r == MB_OK) r = cells_time(cs, iq, llr, hard, reps, st, &t);
+      if (r != MB_OK) break;
+      if (t < 0.99 * best) {
+        best = t;
+        cur = cand;
+      }
+    }
+    for (uint32_t c : members[k]) zp[c] = cur;
+  }
+  if (r == MB_OK) r = mb_cells_set_zf_path(cs, zp.data());
   if (r != MB_OK) return r;
   if (sym_batch_out) std::copy(sb.begin(), sb.end(), sym_batch_out);
   if (eq_cols_out) std::copy(cols.begin(), cols.end(), eq_cols_out);

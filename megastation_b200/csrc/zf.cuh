@@ -33,10 +33,13 @@ struct ZfNetView {
 // fills v from an mb_mlp of the right shape (MB_BAD_SHAPE otherwise)
 mb_status mlp_zf_init_view(const mb_mlp *n, ZfNetView *v);
 
-// net (nullable) is used when opts->init == 1
+// net (nullable) is used when opts->init == 1.  path: where the inverse's
+// matrix products run for K <= 32 -- 0 the tensor cores for 16 < K and the
+// CUDA cores below, 1 the CUDA cores, 2 the tensor cores
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
                        const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
-                       bool write_w = true, float *wmax = nullptr, const ZfNetView *net = nullptr);
+                       bool write_w = true, float *wmax = nullptr, const ZfNetView *net = nullptr,
+                       uint32_t path = 0);
 // the same ZF fused with the tensor-core equalizer: each CTA keeps its
 // group's detector image in shared memory and equalizes the group's
 // columns of nb symbols of planar BF16 samples y_lp [nb][re|im][M][S_pad]
@@ -47,7 +50,7 @@ mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, ui
 mb_status zf_mixed_eq_run(float2 *csi, uint32_t groups, uint32_t M, uint32_t K, const mb_zf_opts *opts,
                           int32_t *status, float *cond, cudaStream_t st, bool write_w, float *wmax,
                           const ZfNetView *net, const EqParams &p, const void *y_lp, uint32_t S_pad,
-                          uint32_t nb);
+                          uint32_t nb, uint32_t path = 0);
 // precoder P[g][u][b] = W[g][b][u] / wmax[g] from a precomputed per-group max
 mb_status precoder_scale(const float2 *W, float2 *P, const float *wmax, uint32_t M, uint32_t K,
                          uint32_t groups, cudaStream_t st);

@@ -64,6 +64,7 @@ struct ZfmParams {
   uint32_t write_w;   // 1: also store W (FP32, CSI layout); 0: the detector image only
   uint32_t net_bulk;  // 1: the network's six arrays come into shared memory by bulk copies (MM == 64)
   uint32_t csi_nst;   // MM == 64: CSI k tiles staged by bulk copies, csi_nst at a time (0: register loads)
+  uint32_t tcns;      // MM == 64: 1 the inverse's products on the tensor cores, 0 on the CUDA cores
   float cond_thr;
   // fused equalize (kernels with QMF > 0): the LLR layout and outputs of
   // the group's eq_nb symbols, eq_spc of them per 128-column tile, eq_nct
@@ -575,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, MM == 64 ? 2 : 1)
   // products (K <= 16: a 16 x 16 product is a fraction of one tensor-core
   // round trip) X and the powers Gn^2, Gn^3 take the Gn images' place and
   // R(X) the iterate's.
-  const bool tcns = MM == 64 && K > kTcMinK;  // uniform
+  const bool tcns = MM == 64 && q.tcns;  // uniform
   uint8_t *gn_img = zsm + (HS + 2) * tile_bytes;
   uint8_t *y_img = gn_img + 2 * kSqImg;
   // MM == 128: R(X) (MM x MM BF16), G, X, and the powers Gn^2, Gn^3 of the
@@ -1424,7 +1425,9 @@ struct ZfmFused {
 
 static mb_status zf_mixed_launch(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
                                  const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
-                                 bool write_w, float *wmax, const ZfNetView *net, const ZfmFused *fe) {
+                                 bool write_w, float *wmax, const ZfNetView *net, const ZfmFused *fe,
+                                 uint32_t path) {
+  if (path > 2) return MB_BAD_ARG;
   if (K == 0 || K > 64) return MB_UNSUPPORTED;
   const bool learned = opts && opts->init == 1;
   if (opts && opts->init > 1) return MB_BAD_ARG;
@@ -1455,6 +1458,9 @@ static mb_status zf_mixed_launch(float2 *csi, void *img_w, uint32_t groups, uint
   if (s.MM == 64 && learned && net->width <= kZfStageWidth && net->width % 4 == 0 && a16(net->w1) &&
       a16(net->w2) && a16(net->w3) && a16(net->b1) && a16(net->b2) && a16(net->b3))
     q.net_bulk = 1;
+  // the inverse's products: tensor cores for 16 < K <= 32 unless the caller
+  // picks (path 1: CUDA cores, 2: tensor cores for any K <= 32)
+  q.tcns = s.MM == 64 && (path == 2 || (path == 0 && K > kTcMinK)) ? 1 : 0;
   q.csi_nst = 0;
   if (s.MM == 64 && K % 2 == 0 && a16(csi))
     q.csi_nst = std::min<uint32_t>(4, 4 * kSqImg / (kKT * K * (uint32_t)sizeof(float2)));
@@ -1524,16 +1530,16 @@ static mb_status zf_mixed_launch(float2 *csi, void *img_w, uint32_t groups, uint
 
 mb_status zf_mixed_run(float2 *csi, void *img_w, uint32_t groups, uint32_t M, uint32_t K,
                        const mb_zf_opts *opts, int32_t *status, float *cond, cudaStream_t st,
-                       bool write_w, float *wmax, const ZfNetView *net) {
-  return zf_mixed_launch(csi, img_w, groups, M, K, opts, status, cond, st, write_w, wmax, net, nullptr);
+                       bool write_w, float *wmax, const ZfNetView *net, uint32_t path) {
+  return zf_mixed_launch(csi, img_w, groups, M, K, opts, status, cond, st, write_w, wmax, net, nullptr, path);
 }
 
 mb_status zf_mixed_eq_run(float2 *csi, uint32_t groups, uint32_t M, uint32_t K, const mb_zf_opts *opts,
                           int32_t *status, float *cond, cudaStream_t st, bool write_w, float *wmax,
                           const ZfNetView *net, const EqParams &p, const void *y_lp, uint32_t S_pad,
-                          uint32_t nb) {
+                          uint32_t nb, uint32_t path) {
   const ZfmFused fe{&p, y_lp, S_pad, nb};
-  return zf_mixed_launch(csi, nullptr, groups, M, K, opts, status, cond, st, write_w, wmax, net, &fe);
+  return zf_mixed_launch(csi, nullptr, groups, M, K, opts, status, cond, st, write_w, wmax, net, &fe, path);
 }
 
 }  // namespace mb

@@ -1,7 +1,9 @@
 """Batched uneven cells (one CUDA graph launch per slot) against the same
 cells run one at a time through the single-cell slot runner: the kernels and
 inputs are the same, so LLRs and hard bits must match bit for bit, before and
-after the autotuner changes the batching and the equalizer tiles."""
+after the autotuner changes the batching, the equalizer tiles and the FFT's
+CTAs; and every cell against the FP64 oracle, whichever product path the
+mixed ZF takes."""
 import numpy as np
 import pytest
 import torch
@@ -54,14 +56,20 @@ def test_cells_autotune_keeps_results(cells_data):
         ref_llr, ref_hard = cs(iqs, stream=s)
         ref = [(a.clone(), b.clone()) for a, b in zip(ref_llr, ref_hard)]
         choice, us = cs.autotune(iqs, reps=5, stream=s)
-        llr, hard = cs(iqs, stream=s)
     s.synchronize()
     assert us > 0
     assert cs.tuning() == choice
+    # the ZF's product path changes its arithmetic; with the rule's path the
+    # tuned batching, equalizer tiles and FFT CTAs give the same bits
+    cs.set_tuning([{**t, "zf_path": 0} for t in choice])
+    with torch.cuda.stream(s):
+        llr, hard = cs(iqs, stream=s)
+    s.synchronize()
     for c, cfg in enumerate(cfgs):
         assert 1 <= choice[c]["sym_batch"] <= max(cfg.U, 1)
         assert choice[c]["eq_cols"] in (64, 128)
         assert choice[c]["fft_ctas"] in (0, 74, 37, 18)
+        assert choice[c]["zf_path"] in (0, 1, 2)
         assert torch.equal(llr[c], ref[c][0]) and torch.equal(hard[c], ref[c][1]), c
     # a hand-set tuning (smallest batches, narrow tiles, tensor-core FFTs on
     # 18 CTAs) gives the same bits
@@ -74,12 +82,16 @@ def test_cells_autotune_keeps_results(cells_data):
         assert torch.equal(llr[c], ref[c][0]) and torch.equal(hard[c], ref[c][1]), c
 
 
-@pytest.mark.parametrize("n,seed,precision", [(32, 3, "mixed"), (6, 11, "fp32")],
-                         ids=["bench-32-cells-mixed", "6-cells-fp32"])
-def test_cells_vs_oracle(n, seed, precision):
+@pytest.mark.parametrize("n,seed,precision,zf_path", [(32, 3, "mixed", 0), (32, 3, "mixed", 1), (32, 3, "mixed", 2),
+                                                      (6, 11, "fp32", 0)],
+                         ids=["bench-32-cells-mixed", "bench-32-cells-mixed-cuda-core-zf",
+                              "bench-32-cells-mixed-tensor-core-zf", "6-cells-fp32"])
+def test_cells_vs_oracle(n, seed, precision, zf_path):
     """Every cell of a batched slot against the FP64 oracle run on that cell
     alone (pilot FFT, ZF, FFT, equalize, descrambled hard bits); the 32-cell
-    set is the batched-cells workload of the bench (seed 3)."""
+    set is the batched-cells workload of the bench (seed 3), also with the
+    mixed ZF's products forced onto the CUDA cores (1) or the tensor cores
+    (2) for every cell with K <= 32."""
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     import megastation_b200 as mb
@@ -90,6 +102,8 @@ def test_cells_vs_oracle(n, seed, precision):
     data = [datagen.make_slot(c) for c in cfgs]
     iqs = [torch.from_numpy(d["iq"]).cuda() for d in data]
     cs = cells.Cells(cfgs, precision=precision)
+    if zf_path:
+        cs.set_tuning([{**t, "zf_path": zf_path} for t in cs.tuning()])
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
         cs(iqs, stream=s)
