@@ -510,6 +510,48 @@ mb_status mb_cells_set_zf_path(mb_cells *cells, const uint32_t *zf_path);
 mb_status mb_cells_set_tuning(mb_cells *cells, const uint32_t *sym_batch,
                               const uint32_t *eq_cols);
 
+/* ----------------------------------------------------------------- LDPC --- */
+/* LDPCEncoder / LDPCDecoder (ldpc/encoder.h:48-75, decoder.h:28-87, sized by
+ * ldpc/config.h and config/config.cc:84-135), which the reference takes from
+ * cuPHY.  The base graph is the caller's: the library ships no graph
+ * tables.  It must have the block structure of both NR base graphs (TS
+ * 38.212 5.3.2): block rows 0..3 over the kb information and the four core
+ * parity columns kb..kb+3 (whose 4Z x 4Z block must be invertible), every
+ * later row r with one more column kb + r, an identity block.  Entry k is
+ * block (row[k], col[k]): the Z x Z identity with its columns cyclically
+ * shifted right by shift[k] mod Z (row i has its one in column
+ * (i + shift) mod Z), so the standard's V values can be passed as they are.
+ * Host arrays, read at create. */
+typedef struct {
+  uint32_t kb;                 /* information block columns (22: BG1, 10: BG2) */
+  uint32_t rows;               /* block rows given */
+  uint32_t nnz;                /* entries */
+  const uint16_t *row, *col, *shift;
+} mb_ldpc_graph;
+typedef struct mb_ldpc mb_ldpc;
+/* parity_nodes: block rows used (LDPCConfig::parity_nodes, 4 .. rows; the
+ * code rate); max_batch: code blocks a decode launch keeps state for (a
+ * larger batch is decoded in turns).  Z <= 384, at most 32 circulants per
+ * row.  Allocates the graph tables, the core block's inverse and the
+ * decoder's check-node state. */
+mb_status mb_ldpc_create(const mb_ldpc_graph *graph, uint32_t Z, uint32_t parity_nodes, uint32_t max_batch,
+                         mb_ldpc **out);
+mb_status mb_ldpc_destroy(mb_ldpc *ldpc);
+/* info [batch][info_stride] bytes, kb Z bits each, MSB first -> codewords
+ * [batch][cw_stride] bytes: the (kb - 2 + parity_nodes) Z encoded bits after
+ * the 2Z punctured systematic ones (cuPHY's puncture option, nrLDPCEncode),
+ * MSB first: LDPCEncoder's output and the uplink LLR rows' cb_size. */
+mb_status mb_ldpc_encode(mb_ldpc *ldpc, const uint8_t *info, uint64_t info_stride, uint8_t *codewords,
+                         uint64_t cw_stride, uint32_t batch, void *stream);
+/* llr [batch][llr_stride] FP16: the (kb + parity_nodes) Z LLRs of a code
+ * block with the 2Z punctured ones first (zero), i.e. the equalizer's LLR
+ * rows (zeros = 2Z, cb_size = (kb - 2 + parity_nodes) Z, cb_stride the
+ * stride), positive for bit 0 -> the kb Z information bits, MSB first,
+ * [batch][out_stride] bytes.  Layered normalized min-sum (the rows in order
+ * as layers, messages 0.75 min), max_iter passes, no early stop. */
+mb_status mb_ldpc_decode(mb_ldpc *ldpc, const uint16_t *llr, uint64_t llr_stride, uint8_t *out,
+                         uint64_t out_stride, uint32_t batch, uint32_t max_iter, void *stream);
+
 /* ------------------------------------------------ learned ZF initialiser --- */
 /* No counterpart in the reference.  A 3-layer MLP (n_in -> width -> width
  * -> n_out, ReLU) with FP32 master weights, BF16 weights in every product

@@ -56,6 +56,10 @@ class MbZfOpts(ctypes.Structure):
                 ("init", U32)]
 
 
+class MbLdpcGraph(ctypes.Structure):
+    _fields_ = [("kb", U32), ("rows", U32), ("nnz", U32), ("row", VP), ("col", VP), ("shift", VP)]
+
+
 class MbCellDesc(ctypes.Structure):
     _fields_ = [("M", U32), ("K", U32), ("N", U32), ("S", U32), ("sg", U32), ("Qm", U32),
                 ("P", U32), ("U", U32), ("D", U32), ("iq_dtype", ctypes.c_int32),
@@ -141,6 +145,10 @@ def _load():
         "mb_cells_get_fft_ctas": (ST, [VP, ctypes.POINTER(U32)]),
         "mb_cells_set_fft_ctas": (ST, [VP, ctypes.POINTER(U32)]),
         "mb_cells_get_zf_path": (ST, [VP, VP]),
+        "mb_ldpc_create": (ST, [VP, U32, U32, U32, VP]),
+        "mb_ldpc_destroy": (ST, [VP]),
+        "mb_ldpc_encode": (ST, [VP, VP, U64, VP, U64, U32, VP]),
+        "mb_ldpc_decode": (ST, [VP, VP, U64, VP, U64, U32, U32, VP]),
         "mb_cells_set_zf_path": (ST, [VP, VP]),
         "mb_cells_set_tuning": (ST, [VP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
     }

@@ -245,6 +245,51 @@ class Scrambler:
               "Scrambler.scrambler")
 
 
+class Ldpc:
+    """ldpc/encoder.h:48-75 and decoder.h:28-87 (the reference's cuPHY
+    LDPCEncoder / LDPCDecoder) over a caller-supplied base graph: entries
+    [n][3] of (row, col, shift) with the NR block structure, kb information
+    columns, lifting size Z, parity_nodes block rows used.  Bits are packed
+    MSB first; LLRs are FP16 rows that start with the 2Z punctured ones."""
+
+    def __init__(self, entries, kb, Z, parity_nodes, max_batch=64):
+        import numpy as np
+        e = np.asarray(entries).reshape(-1, 3)
+        cols = [np.ascontiguousarray(e[:, i], dtype=np.uint16) for i in range(3)]
+        g = _lib.MbLdpcGraph(kb, int(e[:, 0].max()) + 1, len(e), *[c.ctypes.data for c in cols])
+        h = ctypes.c_void_p()
+        check(LIB.mb_ldpc_create(ctypes.byref(g), Z, parity_nodes, max_batch, ctypes.byref(h)), "Ldpc")
+        self._h = h
+        self.kb, self.Z, self.mb = kb, Z, parity_nodes
+        self.info_bytes = (kb * Z + 7) // 8
+        self.cw_bits = (kb - 2 + parity_nodes) * Z
+        self.n_llr = (kb + parity_nodes) * Z
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and LIB is not None:  # LIB is None once the interpreter is shutting down
+            LIB.mb_ldpc_destroy(h)
+            self._h = None
+
+    def encode(self, info, out=None, stream=None):
+        """info [B][>= kb Z / 8] uint8 -> codewords [B][>= cw_bits / 8] uint8."""
+        if out is None:
+            out = torch.zeros(info.shape[0], (self.cw_bits + 7) // 8, dtype=torch.uint8, device=info.device)
+        check(LIB.mb_ldpc_encode(self._h, _dev(info, "info", torch.uint8), info.stride(0),
+                                 _dev(out, "codewords", torch.uint8), out.stride(0), info.shape[0],
+                                 _stream(stream)), "Ldpc.encode")
+        return out
+
+    def decode(self, llr, max_iter=8, out=None, stream=None):
+        """llr [B][>= (kb + mb) Z] float16 -> information bits [B][kb Z / 8] uint8."""
+        if out is None:
+            out = torch.zeros(llr.shape[0], self.info_bytes, dtype=torch.uint8, device=llr.device)
+        check(LIB.mb_ldpc_decode(self._h, _dev(llr, "llr", torch.float16), llr.stride(0),
+                                 _dev(out, "out", torch.uint8), out.stride(0), llr.shape[0], max_iter,
+                                 _stream(stream)), "Ldpc.decode")
+        return out
+
+
 class Equalize:
     """sgemv/equalize.h:25-74: equalize + demodulate (+ descrambled hard bits)."""
 

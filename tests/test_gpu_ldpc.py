@@ -1,0 +1,132 @@
+"""The LDPC kernels (csrc/ldpc.cu through the C ABI) against the reference's
+encoder and the float32 restatement of the decoder (oracle/ldpc.py).
+
+The encoder must give the reference's nrLDPCEncode codewords bit for bit
+(tests/golden/ldpc/, base graphs 1 and 2 at Z = 16) and the restated encoder's
+on fewer parity rows and on a Z = 384 graph of base graph 1's shape; the
+decoder must give the restatement's information bits bit for bit on noisy
+FP16 LLRs, including where it fails to correct, and recover the information
+of moderately noisy codewords."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ldpc
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "ldpc")
+
+
+def _fixture(bg):
+    f = np.load(os.path.join(GOLD, f"bg{bg}_z16.npz"))
+    return f["entries"], f["info"], f["codewords"], int(f["Z"])
+
+
+def _big_graph(Z=384, seed=0):
+    """Base graph 1's circulant pattern with seeded shifts at Z = 384 (an
+    invertible core block), for production-size kernels."""
+    entries, _, _, _ = _fixture(1)
+    rng = np.random.default_rng(seed)
+    while True:
+        e = entries.copy()
+        kb = ldpc.KB[1]
+        for k, (r, c, s) in enumerate(e):
+            e[k, 2] = 0 if c >= kb + 4 else rng.integers(0, Z)
+        try:
+            ldpc.Graph(e, kb, Z, 4).core_inverse()
+            return e
+        except ValueError:
+            continue
+
+
+def _mb():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import megastation_b200 as mb
+    return mb
+
+
+def _pack(bits):
+    return torch.from_numpy(np.packbits(bits, axis=-1)).cuda()
+
+
+@pytest.mark.parametrize("bg", [1, 2])
+def test_encoder_matches_reference_codewords(bg):
+    mb = _mb()
+    entries, info, cw, Z = _fixture(bg)
+    code = mb.Ldpc(entries, ldpc.KB[bg], Z, ldpc.ROWS[bg])
+    out = code.encode(_pack(info))
+    torch.cuda.synchronize()
+    got = np.unpackbits(out.cpu().numpy(), axis=1)[:, :cw.shape[1]]
+    np.testing.assert_array_equal(got, cw)
+
+
+@pytest.mark.parametrize("case", ["bg1-z16-mb25", "bg2-z16-mb14", "bg1-z384-mb46", "bg1-z384-mb12"])
+def test_encoder_matches_restatement(case):
+    mb = _mb()
+    bg = 2 if case.startswith("bg2") else 1
+    Z = int(case.split("-")[1][1:])
+    m = int(case.split("-")[2][2:])
+    entries = _fixture(bg)[0] if Z == 16 else _big_graph(Z)
+    kb = ldpc.KB[bg]
+    g = ldpc.Graph(entries, kb, Z, m)
+    rng = np.random.default_rng(Z + m)
+    info = rng.integers(0, 2, (5, kb * Z), dtype=np.uint8)
+    code = mb.Ldpc(entries, kb, Z, m)
+    # a padded output row: the stride is the caller's
+    out = torch.zeros(5, (code.cw_bits + 7) // 8 + 3, dtype=torch.uint8, device="cuda")
+    code.encode(_pack(info), out=out)
+    torch.cuda.synchronize()
+    got = np.unpackbits(out.cpu().numpy(), axis=1)[:, :code.cw_bits]
+    for k in range(5):
+        np.testing.assert_array_equal(got[k], ldpc.encode(g, info[k])[2 * Z:])
+
+
+@pytest.mark.parametrize("case", ["bg1-z16-mb46", "bg2-z16-mb42", "bg2-z16-mb14", "bg1-z384-mb46"])
+@pytest.mark.parametrize("sigma,iters", [(0.5, 8), (0.9, 3), (1.3, 5)])
+def test_decoder_matches_restatement(case, sigma, iters):
+    mb = _mb()
+    bg = 2 if case.startswith("bg2") else 1
+    Z = int(case.split("-")[1][1:])
+    m = int(case.split("-")[2][2:])
+    entries = _fixture(bg)[0] if Z == 16 else _big_graph(Z)
+    kb = ldpc.KB[bg]
+    g = ldpc.Graph(entries, kb, Z, m)
+    B = 6 if Z == 16 else 2
+    rng = np.random.default_rng(int(sigma * 100) + Z + m)
+    info = rng.integers(0, 2, (B, kb * Z), dtype=np.uint8)
+    # equalizer-style rows: the code block's LLRs, punctured ones zero, then
+    # unused tail up to the row stride
+    stride = g.N + 24
+    llr = np.zeros((B, stride), np.float16)
+    for k in range(B):
+        x = ldpc.encode(g, info[k])
+        y = (1.0 - 2.0 * x) + sigma * rng.standard_normal(len(x))
+        llr[k, :g.N] = (2.0 * y / sigma ** 2).astype(np.float16)
+        llr[k, :2 * Z] = 0
+    code = mb.Ldpc(entries, kb, Z, m, max_batch=4)  # B = 6 decodes in two turns
+    out = code.decode(torch.from_numpy(llr).cuda(), max_iter=iters)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    got = np.unpackbits(out.cpu().numpy(), axis=1)[:, :kb * Z]
+    decoded = 0
+    for k in range(B):
+        bits, _ = ldpc.decode(g, llr[k, :g.N], iters)
+        np.testing.assert_array_equal(got[k], bits, err_msg=f"block {k}")
+        decoded += int((bits == info[k]).all())
+    if sigma <= 0.5:
+        assert decoded == B
+
+
+def test_graph_errors():
+    mb = _mb()
+    from megastation_b200._lib import MbError
+    entries, _, _, Z = _fixture(2)
+    bad = entries.copy()
+    bad[-1, 1] = 200  # a column past the graph
+    with pytest.raises(MbError):
+        mb.Ldpc(bad, 10, Z, 42)
+    with pytest.raises(MbError):
+        mb.Ldpc(entries, 10, Z, 3)  # fewer than the four core rows
