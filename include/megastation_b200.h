@@ -61,6 +61,7 @@ typedef struct {
 } mb_c32;
 
 typedef struct mb_mlp mb_mlp; /* the learned initialiser's network (below) */
+typedef struct mb_ldpc mb_ldpc; /* an LDPC code over a caller-supplied base graph (below) */
 
 const char *mb_status_str(mb_status s);
 /* Version string of this library build. */
@@ -409,6 +410,16 @@ mb_status mb_slot_downlink(mb_slot *slot, const mb_c32 *symbols, void *out,
 mb_status mb_slot_downlink_bits(mb_slot *slot, const uint8_t *bits, uint64_t in_bytes, void *out,
                                 void *stream);
 
+/* The rest of the uplink branch of BandProcess::process (process.cc:
+ * 186-189): LDPC-decode every (symbol, user) LLR row of the last uplink
+ * (one code block per row, llr as mb_slot_uplink wrote it) and descramble
+ * the decoded bits (Scrambler::scrambler, the LFSR mode).  mb_slot_set_ldpc
+ * attaches the code (not owned; NULL detaches), which must fit the cell's
+ * layout: zeros = 2Z, cb_size = (kb - 2 + parity_nodes) Z, cb_stride >=
+ * (kb + parity_nodes) Z.  decoded: [U][K][ceil(kb Z / 8)] bytes, MSB first. */
+mb_status mb_slot_set_ldpc(mb_slot *slot, mb_ldpc *code, uint32_t max_iter);
+mb_status mb_slot_decode(mb_slot *slot, const uint16_t *llr, uint8_t *decoded, void *stream);
+
 /* Single-GPU slot pipeline over host buffers (scheduler/gpu_engine.cc:77-437
  * and cpu_buffer.cc:5-49 for one GPU): each submitted slot's samples are
  * copied to a ring of `depth` device buffers, the slot runs (an mb_slot
@@ -528,7 +539,6 @@ typedef struct {
   uint32_t nnz;                /* entries */
   const uint16_t *row, *col, *shift;
 } mb_ldpc_graph;
-typedef struct mb_ldpc mb_ldpc;
 /* parity_nodes: block rows used (LDPCConfig::parity_nodes, 4 .. rows; the
  * code rate); max_batch: code blocks a decode launch keeps state for (a
  * larger batch is decoded in turns).  Z <= 384, at most 32 circulants per

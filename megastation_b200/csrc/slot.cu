@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "ldpc.cuh"
 #include "slot.cuh"
 #include "sgemv.cuh"
 #include "eq_tc.cuh"
@@ -38,6 +39,8 @@ struct mb_slot {
   uint32_t eq_cols;   // tensor-core equalizer columns per CTA (0: 128)
   uint32_t fft_ctas;  // CTAs of each tensor-core FFT launch (0: one per SM)
   uint32_t zf_path;   // mixed ZF, K <= 32: 0 by K, 1 CUDA-core products, 2 tensor-core products
+  mb_ldpc *ldpc = nullptr;  // decode stage's code (not owned), or null
+  uint32_t ldpc_iters = 0;
   bool eq_fused = false;  // the last uplink equalized inside the ZF kernel
   float2 *precoded;   // [D][M][N]
   const mb_mlp *zf_net;  // learned initial iterate of the mixed ZF (not owned), or null
@@ -486,6 +489,35 @@ extern "C" mb_status mb_slot_downlink_bits(mb_slot *s, const uint8_t *bits, uint
   mb_status r = mb_modulate(bits, s->dl_sym, in_bytes, c.S, (uint64_t)c.D * c.K, c.Qm, 0, nullptr, stream);
   if (r != MB_OK) return r;
   return mb_slot_downlink(s, s->dl_sym, out, stream);
+}
+
+extern "C" mb_status mb_slot_set_ldpc(mb_slot *s, mb_ldpc *code, uint32_t max_iter) {
+  if (!s) return MB_BAD_ARG;
+  if (code) {
+    // the code block must be the cell's: zeros = 2Z punctured LLRs, then
+    // cb_size = (kb - 2 + mb) Z, within the row stride
+    const mb_cell_desc &c = s->c;
+    if (c.zeros != 2ull * code->Z || c.cb_size != (uint64_t)(code->kb - 2 + code->mb) * code->Z ||
+        c.cb_stride < (uint64_t)(code->kb + code->mb) * code->Z || max_iter == 0)
+      return MB_BAD_SHAPE;
+  }
+  s->ldpc = code;
+  s->ldpc_iters = max_iter;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_slot_decode(mb_slot *s, const uint16_t *llr, uint8_t *decoded, void *stream) {
+  if (!s || !llr || !decoded) return MB_BAD_ARG;
+  if (!s->ldpc) return MB_BAD_SHAPE;
+  const mb_cell_desc &c = s->c;
+  if (c.scrambler_mode != MB_SCR_LFSR127) return MB_UNSUPPORTED;
+  const uint64_t bytes = ((uint64_t)s->ldpc->kb * s->ldpc->Z + 7) / 8;
+  const uint32_t blocks = c.U * c.K;  // one code block per (symbol, user) row
+  mb_status r = mb_ldpc_decode(s->ldpc, llr, c.cb_stride, decoded, bytes, blocks, s->ldpc_iters, stream);
+  if (r != MB_OK) return r;
+  // the decoded bits are descrambled (process.cc:188, Scrambler::scrambler
+  // on every row)
+  return mb_scramble(decoded, decoded, bytes, blocks, stream);
 }
 
 extern "C" mb_status mb_slot_timing(mb_slot *s, uint32_t max_calls) {

@@ -248,10 +248,13 @@ def _to_time(cfg, Y, gain):
     return q.astype(np.int16 if cfg.iq_dtype == "int16" else np.int8)
 
 
-def make_slot(cfg):
+def make_slot(cfg, coded=None):
     """Returns a dict: iq [P+U][M][N](...), H [S][M][K], bits [U][K][S*Qm]
     (transmitted coded bits, before scrambling), x [U][K][S] (transmitted
-    QAM symbols), noise_var, pilot_raw [S], seq [K][S*Qm]."""
+    QAM symbols), noise_var, pilot_raw [S], seq [K][S*Qm].  With coded
+    ([U][K][S*Qm] 0/1, e.g. LDPC codewords of scrambled information bits,
+    the reference's order, process.cc:196-214) those bits are sent as they
+    are: no scrambling of the coded bits."""
     rng = np.random.default_rng(np.random.Philox(cfg.seed))
     M, K, S, sg, Qm, U, P = cfg.M, cfg.K, cfg.S, cfg.sg, cfg.Qm, cfg.U, cfg.P
     H = _channel(cfg, rng)
@@ -260,6 +263,8 @@ def make_slot(cfg):
     bits = rng.integers(0, 2, (U, K, nbits), dtype=np.uint8)
     seq = scrambling_bits(cfg, nbits)
     tx = bits ^ seq[None]
+    if coded is not None:
+        bits = tx = np.asarray(coded, np.uint8).reshape(U, K, nbits)
     weights = 1 << np.arange(Qm - 1, -1, -1)
     idx = (tx.reshape(U, K, S, Qm) * weights).sum(-1)
     if Qm == 8:

@@ -62,6 +62,22 @@ class UplinkSlot:
                                         _stream(stream)), "mb_slot_downlink_bits")
         return out
 
+    def set_ldpc(self, code, max_iter=8):
+        """Attach an ops.Ldpc whose code block is the cell's (None detaches)."""
+        check(LIB.mb_slot_set_ldpc(self._h, code._h if code is not None else None, max_iter), "mb_slot_set_ldpc")
+        self._ldpc = code  # not owned by the library: keep it alive
+
+    def decode(self, llr=None, out=None, stream=None):
+        """LDPC decode + descramble of the last uplink's LLR rows:
+        [U][K][kb Z / 8] uint8 (mb_slot_decode)."""
+        llr = self.llr if llr is None else llr
+        code = self._ldpc
+        if out is None:
+            out = torch.zeros(self.cfg.U, self.cfg.K, code.info_bytes, dtype=torch.uint8, device="cuda")
+        check(LIB.mb_slot_decode(self._h, _dev(llr, "llr"), _dev(out, "decoded"), _stream(stream)),
+              "mb_slot_decode")
+        return out
+
     def set_zf_init(self, net):
         """Mixed ZF from the learned polynomial initial iterate of `net` (a
         learned.MLP with 6 inputs and 4 outputs); None: the exact inverse.

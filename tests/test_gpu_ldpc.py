@@ -130,3 +130,43 @@ def test_graph_errors():
         mb.Ldpc(bad, 10, Z, 42)
     with pytest.raises(MbError):
         mb.Ldpc(entries, 10, Z, 3)  # fewer than the four core rows
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp32"])
+def test_slot_uplink_decodes_the_reference_code(precision):
+    """The reference's uplink order end to end (process.cc:161-189): a cell
+    whose code block is base graph 1 at Z = 16 (S Qm = 1056 coded bits per
+    (symbol, user), the config.cc sizing at rate 1/3); information bits
+    scrambled by the LFSR sequence and encoded as the reference's encoder
+    does, sent over the channel; the slot's LLRs through mb_slot_decode
+    (LDPC decode, then descramble) give the information bits back."""
+    mb = _mb()
+    from oracle import oracle as orc
+
+    from megastation_b200 import datagen, slot
+    cfg = datagen.CellConfig(M=16, K=4, N=512, S=264, sg=8, Qm=4, U=2, snr_db=20.0, seed=71)
+    cb, zeros, stride = cfg.ldpc()
+    entries, _, _, Z = _fixture(1)
+    kb, m = ldpc.KB[1], ldpc.ROWS[1]
+    assert (cb, zeros) == ((kb - 2 + m) * Z, 2 * Z)
+    g = ldpc.Graph(entries, kb, Z, m)
+    rng = np.random.default_rng(72)
+    info = rng.integers(0, 2, (cfg.U, cfg.K, kb * Z), dtype=np.uint8)
+    seq = orc.scrambler_seq127()
+    scrambled = info ^ seq[np.arange(kb * Z) % 127]
+    coded = np.stack([np.stack([ldpc.encode(g, scrambled[l, u])[2 * Z:] for u in range(cfg.K)])
+                      for l in range(cfg.U)])
+    d = datagen.make_slot(cfg, coded=coded)
+    run = slot.UplinkSlot(cfg, precision=precision, sym_batch=cfg.U)
+    code = mb.Ldpc(entries, kb, Z, m)
+    run.set_ldpc(code, max_iter=8)
+    llr, _ = run(torch.from_numpy(d["iq"]).cuda())
+    out = run.decode(llr)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    got = np.unpackbits(out.cpu().numpy(), axis=-1)[..., :kb * Z]
+    np.testing.assert_array_equal(got, info)
+    # a code that does not fit the cell's LLR layout is refused
+    from megastation_b200._lib import MbError
+    with pytest.raises(MbError):
+        run.set_ldpc(mb.Ldpc(entries, kb, Z, 20))
