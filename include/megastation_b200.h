@@ -416,9 +416,17 @@ mb_status mb_slot_downlink_bits(mb_slot *slot, const uint8_t *bits, uint64_t in_
  * the decoded bits (Scrambler::scrambler, the LFSR mode).  mb_slot_set_ldpc
  * attaches the code (not owned; NULL detaches), which must fit the cell's
  * layout: zeros = 2Z, cb_size = (kb - 2 + parity_nodes) Z, cb_stride >=
- * (kb + parity_nodes) Z.  decoded: [U][K][ceil(kb Z / 8)] bytes, MSB first. */
+ * (kb + parity_nodes) Z; with downlink symbols it also allocates the
+ * buffers of mb_slot_downlink_info.  decoded: [U][K][ceil(kb Z / 8)] bytes,
+ * MSB first. */
 mb_status mb_slot_set_ldpc(mb_slot *slot, mb_ldpc *code, uint32_t max_iter);
 mb_status mb_slot_decode(mb_slot *slot, const uint16_t *llr, uint8_t *decoded, void *stream);
+/* The whole downlink branch of BandProcess::process (process.cc:196-214)
+ * from information bits [D][K][ceil(kb Z / 8)] (MSB first): scramble (the
+ * LFSR mode), LDPC-encode with the attached code, modulate, precode,
+ * inverse FFT into out as mb_slot_downlink.  Codeword bits past the code
+ * block up to S Qm are zero.  mb_slot_set_ldpc allocates its buffers. */
+mb_status mb_slot_downlink_info(mb_slot *slot, const uint8_t *info, void *out, void *stream);
 
 /* Single-GPU slot pipeline over host buffers (scheduler/gpu_engine.cc:77-437
  * and cpu_buffer.cc:5-49 for one GPU): each submitted slot's samples are

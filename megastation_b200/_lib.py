@@ -135,6 +135,7 @@ def _load():
         "mb_slot_downlink_bits": (ST, [VP, VP, U64, VP, VP]),
         "mb_slot_set_ldpc": (ST, [VP, VP, U32]),
         "mb_slot_decode": (ST, [VP, VP, VP, VP]),
+        "mb_slot_downlink_info": (ST, [VP, VP, VP, VP]),
         "mb_slot_buffers": (ST, [VP, ctypes.POINTER(VP), ctypes.POINTER(VP)]),
         "mb_slot_timing": (ST, [VP, U32]),
         "mb_slot_stage_ms": (ST, [VP, ctypes.POINTER(ctypes.c_double)]),

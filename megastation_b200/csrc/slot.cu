@@ -41,6 +41,10 @@ struct mb_slot {
   uint32_t zf_path;   // mixed ZF, K <= 32: 0 by K, 1 CUDA-core products, 2 tensor-core products
   mb_ldpc *ldpc = nullptr;  // decode stage's code (not owned), or null
   uint32_t ldpc_iters = 0;
+  // downlink from information bits: the scrambled bits [D][K][info bytes]
+  // and the codewords [D][K][dl_row] (their tail past the code block zero)
+  uint8_t *dl_info = nullptr, *dl_cw = nullptr;
+  uint64_t dl_row = 0;
   bool eq_fused = false;  // the last uplink equalized inside the ZF kernel
   float2 *precoded;   // [D][M][N]
   const mb_mlp *zf_net;  // learned initial iterate of the mixed ZF (not owned), or null
@@ -141,6 +145,8 @@ extern "C" mb_status mb_slot_destroy(mb_slot *s) {
   cudaFree(s->pc_img);
   cudaFree(s->z16);
   cudaFree(s->dl_sym);
+  cudaFree(s->dl_info);
+  cudaFree(s->dl_cw);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->crit) cudaStreamDestroy(s->crit);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
@@ -503,7 +509,36 @@ extern "C" mb_status mb_slot_set_ldpc(mb_slot *s, mb_ldpc *code, uint32_t max_it
   }
   s->ldpc = code;
   s->ldpc_iters = max_iter;
+  cudaFree(s->dl_info);
+  cudaFree(s->dl_cw);
+  s->dl_info = s->dl_cw = nullptr;
+  s->dl_row = 0;
+  if (code && s->c.D) {
+    // the downlink's buffers: a codeword row holds at least the S Qm bits
+    // the modulator reads
+    const mb_cell_desc &c = s->c;
+    const uint64_t info_bytes = ((uint64_t)code->kb * code->Z + 7) / 8;
+    s->dl_row = std::max((c.cb_size + 7) / 8, ((uint64_t)c.S * c.Qm + 7) / 8);
+    const uint64_t rows = (uint64_t)c.D * c.K;
+    MB_CUDA_TRY(cudaMalloc((void **)&s->dl_info, rows * info_bytes));
+    MB_CUDA_TRY(cudaMalloc((void **)&s->dl_cw, rows * s->dl_row));
+    MB_CUDA_TRY(cudaMemset(s->dl_cw, 0, rows * s->dl_row));
+  }
   return MB_OK;
+}
+
+extern "C" mb_status mb_slot_downlink_info(mb_slot *s, const uint8_t *info, void *out, void *stream) {
+  if (!s || !info || !out) return MB_BAD_ARG;
+  const mb_cell_desc &c = s->c;
+  if (!c.D || !s->ldpc || !s->dl_cw) return MB_BAD_SHAPE;
+  if (c.scrambler_mode != MB_SCR_LFSR127) return MB_UNSUPPORTED;
+  const uint64_t info_bytes = ((uint64_t)s->ldpc->kb * s->ldpc->Z + 7) / 8;
+  const uint32_t rows = c.D * c.K;
+  // process.cc:198-208: scramble, LDPC-encode, modulate, precode, IFFT
+  mb_status r = mb_scramble(s->dl_info, info, info_bytes, rows, stream);
+  if (r == MB_OK) r = mb_ldpc_encode(s->ldpc, s->dl_info, info_bytes, s->dl_cw, s->dl_row, rows, stream);
+  if (r == MB_OK) r = mb_slot_downlink_bits(s, s->dl_cw, s->dl_row, out, stream);
+  return r;
 }
 
 extern "C" mb_status mb_slot_decode(mb_slot *s, const uint16_t *llr, uint8_t *decoded, void *stream) {

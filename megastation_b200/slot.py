@@ -78,6 +78,14 @@ class UplinkSlot:
               "mb_slot_decode")
         return out
 
+    def downlink_info(self, info, out, stream=None):
+        """The downlink from information bits [D][K][kb Z / 8] (uint8):
+        scramble, LDPC-encode, modulate, precode, inverse FFT
+        (mb_slot_downlink_info; needs set_ldpc)."""
+        check(LIB.mb_slot_downlink_info(self._h, _dev(info, "info"), _dev(out, "out"), _stream(stream)),
+              "mb_slot_downlink_info")
+        return out
+
     def set_zf_init(self, net):
         """Mixed ZF from the learned polynomial initial iterate of `net` (a
         learned.MLP with 6 inputs and 4 outputs); None: the exact inverse.

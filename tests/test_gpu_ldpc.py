@@ -170,3 +170,36 @@ def test_slot_uplink_decodes_the_reference_code(precision):
     from megastation_b200._lib import MbError
     with pytest.raises(MbError):
         run.set_ldpc(mb.Ldpc(entries, kb, Z, 20))
+
+
+def test_slot_downlink_from_information_bits():
+    """process.cc:196-214 from information bits (mb_slot_downlink_info):
+    the same antenna samples as the downlink of the LFSR-scrambled bits
+    encoded by the reference's encoder (the restatement, pinned to it above)
+    through mb_slot_downlink_bits."""
+    mb = _mb()
+    from oracle import oracle as orc
+
+    from megastation_b200 import datagen, slot
+    cfg = datagen.CellConfig(M=16, K=4, N=512, S=264, sg=8, Qm=4, U=2, snr_db=20.0, seed=73)
+    entries, _, _, Z = _fixture(1)
+    kb, m = ldpc.KB[1], ldpc.ROWS[1]
+    g = ldpc.Graph(entries, kb, Z, m)
+    D = 2
+    rng = np.random.default_rng(74)
+    info = rng.integers(0, 2, (D, cfg.K, kb * Z), dtype=np.uint8)
+    seq = orc.scrambler_seq127()
+    coded = np.stack([np.stack([ldpc.encode(g, info[l, u] ^ seq[np.arange(kb * Z) % 127])[2 * Z:]
+                                for u in range(cfg.K)]) for l in range(D)])
+    d = datagen.make_slot(cfg)
+    run = slot.UplinkSlot(cfg, precision="mixed", sym_batch=cfg.U, D=D, out_dtype="int16")
+    run.set_ldpc(mb.Ldpc(entries, kb, Z, m))
+    run(torch.from_numpy(d["iq"]).cuda())
+    a = torch.zeros(D, cfg.M, cfg.N, 2, dtype=torch.int16, device="cuda")
+    b = torch.zeros_like(a)
+    run.downlink_info(_pack(info), a)
+    run.downlink_bits(_pack(coded), b)
+    torch.cuda.synchronize()
+    assert mb.ops.device_error() == 0
+    assert a.abs().max().item() > 0
+    assert torch.equal(a, b)
