@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cell256x32",
-                    choices=["cell256x32", "cells32", "full256x64", "learned128x16", "learned256x32"],
+                    choices=["cell256x32", "cells32", "full256x64", "learned128x16", "learned256x32", "ldpc256x32"],
                     help="cells32: 32 seeded uneven cells in one graph launch per slot (autotuned); "
                          "full256x64: uplink + downlink slot, 256-QAM, latency percentiles; "
                          "learned128x16: per-subcarrier ZF with the learned initialiser")
@@ -943,6 +943,70 @@ def run_cells(args):
     print(json.dumps(measure_cells(args)), flush=True)
 
 
+def measure_ldpc(args, steps=20):
+    """LDPC decode and encode of one slot's code blocks at the headline
+    cell's sizing (config.cc:84-135: BG1, rate 1/3, S = 3276, 64-QAM -> Z =
+    288, 46 parity rows; one block per (symbol, user): 12 x 32 = 384).  The
+    library ships no TS 38.212 tables, so the graph is base graph 1's
+    circulant pattern (the committed fixture recovered from the reference's
+    encoder) with seeded shifts mod 288; the cost depends on the pattern
+    and Z, not on the shift values.  LLRs: BPSK codewords through AWGN
+    (sigma 0.6), 8 min-sum passes."""
+    import numpy as np
+    import torch
+
+    import megastation_b200 as mb
+    from megastation_b200 import datagen
+    cfg = datagen.CellConfig(**{**workload_dict(args), "iq_dtype": args.iq})
+    cb, zeros, stride = cfg.ldpc()
+    Z, kb = zeros // 2, 22
+    m = cb // Z - (kb - 2)
+    pat = np.load(os.path.join(ROOT, "tests", "golden", "ldpc", "bg1_z16.npz"))["entries"]
+    rng = np.random.default_rng(5)
+    code = None
+    while code is None:
+        e = pat.copy()
+        e[:, 2] = np.where(e[:, 1] >= kb + 4, 0, rng.integers(0, Z, len(e)))
+        try:
+            code = mb.Ldpc(e, kb, Z, m, max_batch=cfg.U * cfg.K)
+        except mb._lib.MbError:
+            code = None  # a singular core block: other shifts
+    B = cfg.U * cfg.K
+    info = torch.randint(0, 256, (B, code.info_bytes), dtype=torch.uint8, device="cuda")
+    cw = code.encode(info)
+    bits = np.unpackbits(cw.cpu().numpy(), axis=1)[:, :code.cw_bits].astype(np.float32)
+    llr = np.zeros((B, stride), np.float16)
+    y = (1.0 - 2.0 * bits) + 0.6 * rng.standard_normal(bits.shape).astype(np.float32)
+    llr[:, zeros:zeros + cb] = (2.0 * y / 0.36).astype(np.float16)
+    llr_d = torch.from_numpy(llr).cuda()
+    out = torch.zeros(B, code.info_bytes, dtype=torch.uint8, device="cuda")
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    dec_ms = timed(lambda: code.decode(llr_d, max_iter=8, out=out))
+    enc_ms = timed(lambda: code.encode(info, out=cw))
+    ok = int((out == info).all(dim=1).sum().item())
+    return {"metric": "LDPC code blocks/s (decode, 8 passes)", "value": B / (dec_ms / 1e3),
+            "unit": "code blocks/s", "ms_per_slot_decode": dec_ms, "ms_per_slot_encode": enc_ms,
+            "encode_blocks_per_s": B / (enc_ms / 1e3), "code_blocks_per_slot": B,
+            "decoded_correctly": ok, "steps": steps,
+            "workload": f"BG1 pattern, Z = {Z}, {m} parity rows, {B} code blocks per slot, AWGN sigma 0.6"}
+
+
+def run_ldpc(args):
+    print(json.dumps(measure_ldpc(args, steps=max(args.steps, 3))), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -954,7 +1018,7 @@ def main():
     if args.workload != "cell256x32":
         if rank == 0:
             {"cells32": run_cells, "full256x64": run_full, "learned128x16": run_learned,
-             "learned256x32": lambda a: run_learned(a, "256x32")}[args.workload](args)
+             "learned256x32": lambda a: run_learned(a, "256x32"), "ldpc256x32": run_ldpc}[args.workload](args)
         return
 
     import torch
@@ -1098,19 +1162,22 @@ def main():
 
     # short runs of the other measured workloads, so that their numbers come
     # with every default run: the full uplink + downlink slot (256 x 64,
-    # 200 consecutive slots, latency percentiles) and the 32 uneven cells
-    # (autotuned, 50 batched slots); their own --workload lines go further
+    # 200 consecutive slots, latency percentiles), the 32 uneven cells
+    # (autotuned, 50 batched slots) and the LDPC codec on one slot's code
+    # blocks; their own --workload lines go further
     configs = None
     if rank == 0 and world == 1 and not args.no_configs:
         f = measure_full(args, n_min=200)
         c = measure_cells(args, steps=50, reps=5)
+        lp = measure_ldpc(args)
         configs = {
             "full256x64": {**{k: f[k] for k in ("metric", "value", "unit", "ms_per_step", "latency_us",
                                                    "uplink_evm_db", "downlink", "gpu_launches")},
                            "workload": f["config"]["workload"], "slots": f["steps"]},
             "cells32": {**{k: c[k] for k in ("metric", "value", "unit", "ms_per_step", "autotune",
                                                 "one_handle_per_cell", "gpu_launches")},
-                        "workload": c["config"]["workload"], "steps": c["steps"]}}
+                        "workload": c["config"]["workload"], "steps": c["steps"]},
+            "ldpc256x32": lp}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(cfg, d, args.cpu_seconds)

@@ -17,14 +17,16 @@
 // the 2Z punctured systematic ones (cuPHY's puncture option, nrLDPCEncode).
 //
 // Decode (one CTA per code block, thread z = check node z of the current
-// layer): LLRs (FP16, positive = bit 0) into a float array in shared memory;
-// the rows in order as layers; per check node two passes over its entries:
-// q_e = app - r_e (r_e the node's previous message to entry e, rebuilt
-// from its compressed state), then min1 (first index), min2 and the sign
-// parity of q < 0; r'_e = +-(0.75 min) and app = q_e + r'_e.  Within a layer
+// layer): LLRs (FP16, positive = bit 0) into a float array in shared memory
+// with the graph's entries; the rows in order as layers; per check node one
+// pass over its entries: q_e = app - r_e (r_e the node's previous message to
+// entry e, rebuilt from its compressed state), stored in place of app, with
+// min1 (first index), min2 and the sign parity of q < 0; a second pass
+// writes app = q_e + r'_e, r'_e = +-(0.75 min).  Within a layer
 // the Z check nodes touch disjoint variables (a circulant is a permutation),
 // so a layer needs one barrier.  The compressed state (min1, min2, index,
-// sign bits) per (layer, check node) lives in global memory.  Every
+// sign bits) per (layer, check node) lives in global memory, loaded two
+// layers ahead.  Every
 // floating-point step is an explicitly rounded single operation, so the
 // results equal the float32 restatement bit for bit.
 #include <algorithm>
@@ -101,52 +103,75 @@ __global__ void ldpc_encode_kernel(mb_ldpc h, const uint8_t *info, uint64_t info
   }
 }
 
-// previous message of check node z to entry e of its row, rebuilt from the
-// node's state (the same single rounding as when it was made)
-__device__ __forceinline__ float ldpc_msg(const uint4 &st, uint32_t e) {
-  const float m = __fmul_rn(kAlpha, e == st.z ? __uint_as_float(st.y) : __uint_as_float(st.x));
-  const uint32_t par = __popc(st.w) & 1u;
-  return (par ^ ((st.w >> e) & 1u)) ? -m : m;
-}
-
-__global__ void ldpc_decode_kernel(mb_ldpc h, const __half *llr, uint64_t llr_stride, uint8_t *out,
-                                   uint64_t out_stride, uint32_t max_iter, uint32_t b0) {
-  extern __shared__ float app[];  // [(kb + mb) Z]
+__global__ void __launch_bounds__(kMaxZ) ldpc_decode_kernel(mb_ldpc h, const __half *llr, uint64_t llr_stride,
+                                                            uint8_t *out, uint64_t out_stride, uint32_t max_iter,
+                                                            uint32_t b0) {
+  extern __shared__ float app[];  // [(kb + mb) Z], then the entries {col * Z, shift} and the row pointers
   const uint32_t Z = h.Z, kb = h.kb, mb = h.mb, N = (kb + mb) * Z, tid = threadIdx.x, nt = blockDim.x;
+  uint2 *ent = reinterpret_cast<uint2 *>(app + (N + 1) / 2 * 2);  // [nnz]
+  uint32_t *r_ptr = reinterpret_cast<uint32_t *>(ent + h.nnz);    // [mb + 1]
   const uint32_t cb = b0 + blockIdx.x;
   const __half *in = llr + (uint64_t)cb * llr_stride;
   for (uint32_t v = tid; v < N; v += nt) app[v] = __half2float(in[v]);
-  uint4 *state = h.state + (uint64_t)blockIdx.x * mb * Z;
-  for (uint32_t t = tid; t < mb * Z; t += nt) state[t] = make_uint4(0u, 0u, 0u, 0u);  // every message 0
+  for (uint32_t e = tid; e < h.nnz; e += nt) ent[e] = make_uint2((uint32_t)h.col[e] * Z, h.sh[e]);
+  for (uint32_t i = tid; i <= mb; i += nt) r_ptr[i] = h.row_ptr[i];
   __syncthreads();
+  // Thread z only ever reads and writes check node z's state, so its loads
+  // run two layers ahead of their use (a row's state is rewritten mb >= 4
+  // layers before it is read again); the first pass starts from zero
+  // messages without reading.
+  uint4 *state = h.state + (uint64_t)blockIdx.x * mb * Z;
+  const uint32_t layers = max_iter * mb;
+  auto load_state = [&](uint32_t L) {
+    return (L < mb || L >= layers || tid >= Z) ? make_uint4(0u, 0u, 0u, 0u) : state[(L % mb) * Z + tid];
+  };
+  uint4 st_a = load_state(0), st_b = load_state(1);
   for (uint32_t it = 0; it < max_iter; it++) {
     for (uint32_t i = 0; i < mb; i++) {
+      const uint32_t L = it * mb + i;
+      const uint4 st = st_a;
+      st_a = st_b;
+      st_b = load_state(L + 2);
       if (tid < Z) {
-        const uint32_t e0 = h.row_ptr[i], deg = h.row_ptr[i + 1] - e0;
-        const uint4 st = state[i * Z + tid];
+        const uint32_t e0 = r_ptr[i], deg = r_ptr[i + 1] - e0;
+        // the node's previous messages: +-(0.75 min1), the entry at index
+        // pos +-(0.75 min2), the sign from the parity of the sign bits
+        const float m1o = __fmul_rn(kAlpha, __uint_as_float(st.x));
+        const float m2o = __fmul_rn(kAlpha, __uint_as_float(st.y));
+        const uint32_t sgn_o = st.w ^ ((__popc(st.w) & 1u) ? ~0u : 0u);
         float min1 = INFINITY, min2 = INFINITY;
         uint32_t pos = 0, neg = 0;
+        // q_e = app - r_e overwrites the entry's app slot: within a layer
+        // no other thread touches it
         for (uint32_t e = 0; e < deg; e++) {
-          const uint32_t idx = h.col[e0 + e] * Z + (tid + h.sh[e0 + e]) % Z;
-          const float q = __fsub_rn(app[idx], ldpc_msg(st, e));
-          const float a = fabsf(q);
-          if (q < 0.f) neg |= 1u << e;
-          if (a < min1) {
+          const uint2 en = ent[e0 + e];
+          uint32_t z = tid + en.y;
+          if (z >= Z) z -= Z;
+          float *a = app + en.x + z;
+          const float r = __uint_as_float(__float_as_uint(e == st.z ? m2o : m1o) ^ (((sgn_o >> e) & 1u) << 31));
+          const float qe = __fsub_rn(*a, r);
+          *a = qe;
+          const float aq = fabsf(qe);
+          neg |= (qe < 0.f ? 1u : 0u) << e;
+          if (aq < min1) {
             min2 = min1;
-            min1 = a;
+            min1 = aq;
             pos = e;
-          } else if (a < min2) {
-            min2 = a;
+          } else if (aq < min2) {
+            min2 = aq;
           }
         }
         if (deg == 1) min2 = min1;
-        const uint4 ns = make_uint4(__float_as_uint(min1), __float_as_uint(min2), pos, neg);
+        const float m1 = __fmul_rn(kAlpha, min1), m2 = __fmul_rn(kAlpha, min2);
+        const uint32_t sgn = neg ^ ((__popc(neg) & 1u) ? ~0u : 0u);
         for (uint32_t e = 0; e < deg; e++) {
-          const uint32_t idx = h.col[e0 + e] * Z + (tid + h.sh[e0 + e]) % Z;
-          const float q = __fsub_rn(app[idx], ldpc_msg(st, e));
-          app[idx] = __fadd_rn(q, ldpc_msg(ns, e));
+          const uint2 en = ent[e0 + e];
+          uint32_t z = tid + en.y;
+          if (z >= Z) z -= Z;
+          float *a = app + en.x + z;
+          *a = __fadd_rn(*a, __uint_as_float(__float_as_uint(e == pos ? m2 : m1) ^ (((sgn >> e) & 1u) << 31)));
         }
-        state[i * Z + tid] = ns;
+        state[i * Z + tid] = make_uint4(__float_as_uint(min1), __float_as_uint(min2), pos, neg);
       }
       __syncthreads();
     }
@@ -306,7 +331,7 @@ extern "C" mb_status mb_ldpc_decode(mb_ldpc *h, const uint16_t *llr, uint64_t ll
   if (llr_stride < (uint64_t)(h->kb + h->mb) * h->Z || out_stride < ((uint64_t)h->kb * h->Z + 7) / 8)
     return MB_BAD_SHAPE;
   if (batch == 0) return MB_OK;
-  const size_t smem = (size_t)(h->kb + h->mb) * h->Z * sizeof(float);
+  const size_t smem = ((size_t)(h->kb + h->mb) * h->Z + 1) / 2 * 8 + 8 * (size_t)h->nnz + 4 * ((size_t)h->mb + 1);
   static_assert(kMaxZ <= 1024, "one thread per check node");
   int maxs = 0;
   MB_CUDA_TRY(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->dev));
