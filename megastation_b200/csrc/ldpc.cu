@@ -18,11 +18,11 @@
 //
 // Decode (one CTA per code block, thread z = check node z of the current
 // layer): LLRs (FP16, positive = bit 0) into a float array in shared memory
-// with the graph's entries; the rows in order as layers; per check node one
-// pass over its entries: q_e = app - r_e (r_e the node's previous message to
-// entry e, rebuilt from its compressed state), stored in place of app, with
-// min1 (first index), min2 and the sign parity of q < 0; a second pass
-// writes app = q_e + r'_e, r'_e = +-(0.75 min).  Within a layer
+// with the graph's entries; the rows in order as layers; per check node:
+// q_e = app - r_e (r_e the node's previous message to entry e, rebuilt from
+// its compressed state), min1 (first index), min2 and the sign parity of
+// q < 0, then app = q_e + r'_e, r'_e = +-(0.75 min); rows of up to 20
+// entries keep q in registers (ldpc_node).  Within a layer
 // the Z check nodes touch disjoint variables (a circulant is a permutation),
 // so a layer needs one barrier.  The compressed state (min1, min2, index,
 // sign bits) per (layer, check node) lives in global memory, loaded two
@@ -103,7 +103,100 @@ __global__ void ldpc_encode_kernel(mb_ldpc h, const uint8_t *info, uint64_t info
   }
 }
 
-__global__ void __launch_bounds__(kMaxZ) ldpc_decode_kernel(mb_ldpc h, const __half *llr, uint64_t llr_stride,
+// One check node's update over a row of at most D entries, all in registers:
+// every app load issued before any store (a row holds one circulant per
+// column block, so the node's D slots are distinct), then q_e = app - r_e
+// (r_e rebuilt from the node's previous state st) with min1 (first index),
+// min2 and the signs of q, then app = q_e + r'_e.  Returns the new state.
+template <int D>
+__device__ __forceinline__ uint4 ldpc_node(float *app, const uint2 *ent, uint32_t deg, uint32_t tid, uint32_t Z,
+                                           const uint4 &st) {
+  uint32_t idx[D];
+  float q[D];
+#pragma unroll
+  for (int j = 0; j < D; j++) {
+    if (j < (int)deg) {
+      const uint2 en = ent[j];
+      uint32_t z = tid + en.y;
+      if (z >= Z) z -= Z;
+      idx[j] = en.x + z;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < D; j++)
+    if (j < (int)deg) q[j] = app[idx[j]];
+  const float m1o = __fmul_rn(kAlpha, __uint_as_float(st.x));
+  const float m2o = __fmul_rn(kAlpha, __uint_as_float(st.y));
+  const uint32_t sgn_o = st.w ^ ((__popc(st.w) & 1u) ? ~0u : 0u);
+  float min1 = INFINITY, min2 = INFINITY;
+  uint32_t pos = 0, neg = 0;
+#pragma unroll
+  for (int j = 0; j < D; j++) {
+    if (j < (int)deg) {
+      const float r = __uint_as_float(__float_as_uint((uint32_t)j == st.z ? m2o : m1o) ^ (((sgn_o >> j) & 1u) << 31));
+      q[j] = __fsub_rn(q[j], r);
+      const float aq = fabsf(q[j]);
+      neg |= (q[j] < 0.f ? 1u : 0u) << j;
+      if (aq < min1) {
+        min2 = min1;
+        min1 = aq;
+        pos = j;
+      } else if (aq < min2) {
+        min2 = aq;
+      }
+    }
+  }
+  if (deg == 1) min2 = min1;
+  const float m1 = __fmul_rn(kAlpha, min1), m2 = __fmul_rn(kAlpha, min2);
+  const uint32_t sgn = neg ^ ((__popc(neg) & 1u) ? ~0u : 0u);
+#pragma unroll
+  for (int j = 0; j < D; j++)
+    if (j < (int)deg)
+      app[idx[j]] = __fadd_rn(q[j], __uint_as_float(__float_as_uint((uint32_t)j == pos ? m2 : m1) ^ (((sgn >> j) & 1u) << 31)));
+  return make_uint4(__float_as_uint(min1), __float_as_uint(min2), pos, neg);
+}
+
+// The same update for rows of any degree (up to 32): q_e is stored in place
+// of app between the two passes.
+__device__ __forceinline__ uint4 ldpc_node_any(float *app, const uint2 *ent, uint32_t deg, uint32_t tid,
+                                               uint32_t Z, const uint4 &st) {
+  const float m1o = __fmul_rn(kAlpha, __uint_as_float(st.x));
+  const float m2o = __fmul_rn(kAlpha, __uint_as_float(st.y));
+  const uint32_t sgn_o = st.w ^ ((__popc(st.w) & 1u) ? ~0u : 0u);
+  float min1 = INFINITY, min2 = INFINITY;
+  uint32_t pos = 0, neg = 0;
+  for (uint32_t e = 0; e < deg; e++) {
+    const uint2 en = ent[e];
+    uint32_t z = tid + en.y;
+    if (z >= Z) z -= Z;
+    float *a = app + en.x + z;
+    const float r = __uint_as_float(__float_as_uint(e == st.z ? m2o : m1o) ^ (((sgn_o >> e) & 1u) << 31));
+    const float qe = __fsub_rn(*a, r);
+    *a = qe;
+    const float aq = fabsf(qe);
+    neg |= (qe < 0.f ? 1u : 0u) << e;
+    if (aq < min1) {
+      min2 = min1;
+      min1 = aq;
+      pos = e;
+    } else if (aq < min2) {
+      min2 = aq;
+    }
+  }
+  if (deg == 1) min2 = min1;
+  const float m1 = __fmul_rn(kAlpha, min1), m2 = __fmul_rn(kAlpha, min2);
+  const uint32_t sgn = neg ^ ((__popc(neg) & 1u) ? ~0u : 0u);
+  for (uint32_t e = 0; e < deg; e++) {
+    const uint2 en = ent[e];
+    uint32_t z = tid + en.y;
+    if (z >= Z) z -= Z;
+    float *a = app + en.x + z;
+    *a = __fadd_rn(*a, __uint_as_float(__float_as_uint(e == pos ? m2 : m1) ^ (((sgn >> e) & 1u) << 31)));
+  }
+  return make_uint4(__float_as_uint(min1), __float_as_uint(min2), pos, neg);
+}
+
+__global__ void __launch_bounds__(kMaxZ, 2) ldpc_decode_kernel(mb_ldpc h, const __half *llr, uint64_t llr_stride,
                                                             uint8_t *out, uint64_t out_stride, uint32_t max_iter,
                                                             uint32_t b0) {
   extern __shared__ float app[];  // [(kb + mb) Z], then the entries {col * Z, shift} and the row pointers
@@ -134,44 +227,19 @@ __global__ void __launch_bounds__(kMaxZ) ldpc_decode_kernel(mb_ldpc h, const __h
       st_b = load_state(L + 2);
       if (tid < Z) {
         const uint32_t e0 = r_ptr[i], deg = r_ptr[i + 1] - e0;
-        // the node's previous messages: +-(0.75 min1), the entry at index
-        // pos +-(0.75 min2), the sign from the parity of the sign bits
-        const float m1o = __fmul_rn(kAlpha, __uint_as_float(st.x));
-        const float m2o = __fmul_rn(kAlpha, __uint_as_float(st.y));
-        const uint32_t sgn_o = st.w ^ ((__popc(st.w) & 1u) ? ~0u : 0u);
-        float min1 = INFINITY, min2 = INFINITY;
-        uint32_t pos = 0, neg = 0;
-        // q_e = app - r_e overwrites the entry's app slot: within a layer
-        // no other thread touches it
-        for (uint32_t e = 0; e < deg; e++) {
-          const uint2 en = ent[e0 + e];
-          uint32_t z = tid + en.y;
-          if (z >= Z) z -= Z;
-          float *a = app + en.x + z;
-          const float r = __uint_as_float(__float_as_uint(e == st.z ? m2o : m1o) ^ (((sgn_o >> e) & 1u) << 31));
-          const float qe = __fsub_rn(*a, r);
-          *a = qe;
-          const float aq = fabsf(qe);
-          neg |= (qe < 0.f ? 1u : 0u) << e;
-          if (aq < min1) {
-            min2 = min1;
-            min1 = aq;
-            pos = e;
-          } else if (aq < min2) {
-            min2 = aq;
-          }
-        }
-        if (deg == 1) min2 = min1;
-        const float m1 = __fmul_rn(kAlpha, min1), m2 = __fmul_rn(kAlpha, min2);
-        const uint32_t sgn = neg ^ ((__popc(neg) & 1u) ? ~0u : 0u);
-        for (uint32_t e = 0; e < deg; e++) {
-          const uint2 en = ent[e0 + e];
-          uint32_t z = tid + en.y;
-          if (z >= Z) z -= Z;
-          float *a = app + en.x + z;
-          *a = __fadd_rn(*a, __uint_as_float(__float_as_uint(e == pos ? m2 : m1) ^ (((sgn >> e) & 1u) << 31)));
-        }
-        state[i * Z + tid] = make_uint4(__float_as_uint(min1), __float_as_uint(min2), pos, neg);
+        // every thread of the layer takes the same branch
+        uint4 ns;
+        if (deg <= 4)
+          ns = ldpc_node<4>(app, ent + e0, deg, tid, Z, st);
+        else if (deg <= 6)
+          ns = ldpc_node<6>(app, ent + e0, deg, tid, Z, st);
+        else if (deg <= 10)
+          ns = ldpc_node<10>(app, ent + e0, deg, tid, Z, st);
+        else if (deg <= 20)
+          ns = ldpc_node<20>(app, ent + e0, deg, tid, Z, st);
+        else
+          ns = ldpc_node_any(app, ent + e0, deg, tid, Z, st);
+        state[i * Z + tid] = ns;
       }
       __syncthreads();
     }
