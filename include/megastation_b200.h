@@ -416,9 +416,9 @@ mb_status mb_slot_downlink_bits(mb_slot *slot, const uint8_t *bits, uint64_t in_
  * the decoded bits (Scrambler::scrambler, the LFSR mode).  mb_slot_set_ldpc
  * attaches the code (not owned; NULL detaches), which must fit the cell's
  * layout: zeros = 2Z, cb_size = (kb - 2 + parity_nodes) Z, cb_stride >=
- * (kb + parity_nodes) Z; with downlink symbols it also allocates the
- * buffers of mb_slot_downlink_info.  decoded: [U][K][ceil(kb Z / 8)] bytes,
- * MSB first. */
+ * (kb + parity_nodes) Z; max_iter 1 .. 32; with downlink symbols it also
+ * allocates the buffers of mb_slot_downlink_info.  decoded: [U][K][ceil(kb
+ * Z / 8)] bytes, MSB first. */
 mb_status mb_slot_set_ldpc(mb_slot *slot, mb_ldpc *code, uint32_t max_iter);
 mb_status mb_slot_decode(mb_slot *slot, const uint16_t *llr, uint8_t *decoded, void *stream);
 /* The whole downlink branch of BandProcess::process (process.cc:196-214)
@@ -549,7 +549,7 @@ typedef struct {
 } mb_ldpc_graph;
 /* parity_nodes: block rows used (LDPCConfig::parity_nodes, 4 .. rows; the
  * code rate); max_batch: code blocks a decode launch keeps state for (a
- * larger batch is decoded in turns).  Z <= 384, at most 32 circulants per
+ * larger batch is decoded in turns).  Z <= 384, at most 27 circulants per
  * row.  Allocates the graph tables, the core block's inverse and the
  * decoder's check-node state. */
 mb_status mb_ldpc_create(const mb_ldpc_graph *graph, uint32_t Z, uint32_t parity_nodes, uint32_t max_batch,
@@ -566,7 +566,11 @@ mb_status mb_ldpc_encode(mb_ldpc *ldpc, const uint8_t *info, uint64_t info_strid
  * rows (zeros = 2Z, cb_size = (kb - 2 + parity_nodes) Z, cb_stride the
  * stride), positive for bit 0 -> the kb Z information bits, MSB first,
  * [batch][out_stride] bytes.  Layered normalized min-sum (the rows in order
- * as layers, messages 0.75 min), max_iter passes, no early stop. */
+ * as layers, messages 0.75 min), max_iter passes (at most 32), no early
+ * stop, in FP16 arithmetic (the precision of the reference's cuPHY decoder;
+ * two code blocks per CTA in the halves of FP16 pairs).  Channel LLRs are
+ * clamped to +-1024 and messages to +-256, which keeps every value finite;
+ * NaN inputs give undefined bits. */
 mb_status mb_ldpc_decode(mb_ldpc *ldpc, const uint16_t *llr, uint64_t llr_stride, uint8_t *out,
                          uint64_t out_stride, uint32_t batch, uint32_t max_iter, void *stream);
 

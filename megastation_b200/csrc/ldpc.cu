@@ -16,19 +16,22 @@
 // information and core parity columns.  Out: the (kb - 2 + mb) Z bits after
 // the 2Z punctured systematic ones (cuPHY's puncture option, nrLDPCEncode).
 //
-// Decode (one CTA per code block, thread z = check node z of the current
-// layer): LLRs (FP16, positive = bit 0) into a float array in shared memory
-// with the graph's entries; the rows in order as layers; per check node:
+// Decode (one CTA per pair of code blocks, thread z = check node z of the
+// current layer, both blocks in the two halves of FP16 pairs): LLRs (FP16,
+// positive = bit 0) into a __half2 array in shared memory with the graph's
+// entries; the rows in order as layers; per check node and block:
 // q_e = app - r_e (r_e the node's previous message to entry e, rebuilt from
-// its compressed state), min1 (first index), min2 and the sign parity of
-// q < 0, then app = q_e + r'_e, r'_e = +-(0.75 min); rows of up to 20
-// entries keep q in registers (ldpc_node).  Within a layer
-// the Z check nodes touch disjoint variables (a circulant is a permutation),
-// so a layer needs one barrier.  The compressed state (min1, min2, index,
-// sign bits) per (layer, check node) lives in global memory, loaded two
-// layers ahead.  Every
-// floating-point step is an explicitly rounded single operation, so the
-// results equal the float32 restatement bit for bit.
+// its compressed state), min1 (first index), min2 and the parity of the
+// sign bits of q, then app = q_e + r'_e, r'_e = +-min(0.75 min, 256); rows of up to
+// 20 entries keep q in registers (ldpc_node).  FP16 is the reference
+// decoder's precision (cuPHY), and the pairs halve the instructions per
+// block; channel LLRs clamped to +-1024 and messages to +-256 keep every
+// value finite for up to 32 passes.
+// Within a layer the Z check nodes touch disjoint variables (a circulant is
+// a permutation), so a layer needs one barrier.  The compressed state (min1,
+// min2, index, sign bits) per (layer, check node) lives in global memory,
+// loaded two layers ahead.  Every step is one IEEE FP16 operation, so the
+// results equal the float16 restatement bit for bit.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -40,8 +43,18 @@ namespace mb {
 namespace {
 
 constexpr uint32_t kMaxZ = 384;
-constexpr uint32_t kMaxDeg = 32;   // sign bits per check node state
+constexpr uint32_t kMaxDeg = 27;   // sign bits per check node and block in its state
 constexpr float kAlpha = 0.75f;    // min-sum normalisation
+// FP16 range: channel LLRs are clamped to +-kLlrMax once and every message
+// to +-kMsgMax; q and app stay exact sums (app = llr + the messages of the
+// variable's rows, up to rounding), below 1024 + 46 * 256 = 12800 with at
+// most 46 rows, and the rounding of two operations a row visit (at most 32
+// each below 65504) adds at most 46 * 32 * 32 in kMaxIter passes: nothing
+// overflows.  (Clamping q or app instead breaks that sum: a later row then
+// removes more of its old message than app still holds, and signs flip.)
+constexpr float kLlrMax = 1024.f;
+constexpr float kMsgMax = 256.f;
+constexpr uint32_t kMaxIter = 32;
 
 __global__ void ldpc_encode_kernel(mb_ldpc h, const uint8_t *info, uint64_t info_stride, uint8_t *cw,
                                    uint64_t cw_stride) {
@@ -103,109 +116,182 @@ __global__ void ldpc_encode_kernel(mb_ldpc h, const uint8_t *info, uint64_t info
   }
 }
 
-// One check node's update over a row of at most D entries, all in registers:
-// every app load issued before any store (a row holds one circulant per
-// column block, so the node's D slots are distinct), then q_e = app - r_e
-// (r_e rebuilt from the node's previous state st) with min1 (first index),
-// min2 and the signs of q, then app = q_e + r'_e.  Returns the new state.
+// Packed pairs: a CTA decodes two code blocks at once, lane 0 (the low half
+// of every __half2) the pair's first block and lane 1 its second.
+__device__ __forceinline__ uint32_t h2u(__half2 v) {
+  uint32_t u;
+  memcpy(&u, &v, 4);
+  return u;
+}
+__device__ __forceinline__ __half2 u2h(uint32_t u) {
+  __half2 v;
+  memcpy(&v, &u, 4);
+  return v;
+}
+__device__ __forceinline__ __half2 llr_clamp(__half2 v) {
+  return __hmax2(__hmin2(v, __float2half2_rn(kLlrMax)), __float2half2_rn(-kLlrMax));
+}
+
+// A check node's state for the pair (one uint4 per layer and node):
+//   x, y  min1, min2 (__half2: |q| of each block)
+//   z     signs of q for entries 0..15: bit e block 0, bit 16 + e block 1
+//   w     signs for entries 16..26 in bits 0..10 / 16..26, and the index of
+//         min1 of block 0 in bits 11..15, of block 1 in bits 27..31
+// The interleaving puts both blocks' bits for entry e at the same distance
+// from bits 15 and 31, so one shift lines them up with the FP16 sign bits.
+// The node's messages rebuilt from the state:
+struct PairMsg {
+  uint32_t m1, m2;    // min(0.75 min1, kMsgMax), min(0.75 min2, kMsgMax) (__half2 bits)
+  uint32_t sgl, sgh;  // z / w with each block's sign parity applied: the message signs
+  uint32_t ohl, ohh;  // min1's index one-hot in the same interleaved layout
+};
+__device__ __forceinline__ PairMsg pair_msg(const uint4 &st) {
+  PairMsg m;
+  const __half2 a = __float2half2_rn(kAlpha);  // 0.75, exact in FP16
+  const __half2 cap = __float2half2_rn(kMsgMax);
+  m.m1 = h2u(__hmin2(__hmul2(a, u2h(st.x)), cap));
+  m.m2 = h2u(__hmin2(__hmul2(a, u2h(st.y)), cap));
+  const uint32_t par0 = (__popc(st.z & 0xFFFFu) + __popc(st.w & 0x7FFu)) & 1u;
+  const uint32_t par1 = (__popc(st.z >> 16) + __popc(st.w & 0x07FF0000u)) & 1u;
+  const uint32_t flip = (par0 ? 0x0000FFFFu : 0u) | (par1 ? 0xFFFF0000u : 0u);
+  m.sgl = st.z ^ flip;
+  m.sgh = st.w ^ flip;  // only bits 0..10 and 16..26 are read
+  const uint32_t p0 = (st.w >> 11) & 31u, p1 = st.w >> 27;
+  m.ohl = (p0 < 16 ? 1u << p0 : 0u) | (p1 < 16 ? 1u << (16 + p1) : 0u);
+  m.ohh = (p0 >= 16 ? 1u << (p0 - 16) : 0u) | (p1 >= 16 ? 1u << p1 : 0u);
+  return m;
+}
+// the message to entry j: the (capped) 0.75 min2 at min1's index, 0.75
+// min1 elsewhere, with the sign of q_j times the parity of all signs
+__device__ __forceinline__ __half2 pair_r(const PairMsg &m, uint32_t j) {
+  const uint32_t sh = j < 16 ? 15 - j : 31 - j;
+  const uint32_t oh = (j < 16 ? m.ohl : m.ohh) << sh;
+  const uint32_t sg = (j < 16 ? m.sgl : m.sgh) << sh;
+  // bits 15 / 31 of oh spread over their halves (byte permute with the
+  // selector's sign-replicate bit: bytes 1 and 3's top bits)
+  uint32_t sel;
+  asm("prmt.b32 %0, %1, %2, 0xBB99;" : "=r"(sel) : "r"(oh), "r"(0u));
+  const uint32_t mag = (m.m1 & ~sel) | (m.m2 & sel);
+  return u2h(mag ^ (sg & 0x80008000u));
+}
+// min tracking of entry j's |q| (blocks apart): the first index of min1 and
+// the least of the others, as a sequential scan in entry order keeps them;
+// the signs of q go into nl / nh
+__device__ __forceinline__ void pair_track(__half2 q, uint32_t j, __half2 &min1, __half2 &min2, uint32_t &pos,
+                                           uint32_t &nl, uint32_t &nh) {
+  const uint32_t qb = h2u(q);
+  const __half2 mag = u2h(qb & 0x7FFF7FFFu);
+  const uint32_t lt = __hlt2_mask(mag, min1);
+  pos = (pos & ~lt) | ((j * 0x00010001u) & lt);
+  min2 = __hmin2(min2, __hmax2(min1, mag));
+  min1 = __hmin2(min1, mag);
+  if (j < 16)
+    nl |= (qb >> (15 - j)) & (0x00010001u << j);
+  else
+    nh |= (qb >> (31 - j)) & (0x00010001u << (j - 16));
+}
+__device__ __forceinline__ uint4 pair_state(__half2 min1, __half2 min2, uint32_t pos, uint32_t nl, uint32_t nh,
+                                            uint32_t deg) {
+  if (deg == 1) min2 = min1;
+  return make_uint4(h2u(min1), h2u(min2), nl, nh | ((pos & 31u) << 11) | ((pos >> 16) << 27));
+}
+
+// One check node's update for the pair over a row of at most D entries, all
+// in registers: every app load issued before any store (a row holds one
+// circulant per column block, so the node's D slots are distinct), then
+// q_e = app - r_e (r_e rebuilt from the node's previous state) with the min
+// tracking, then app = q_e + r'_e.  Returns the new state.
 template <int D>
-__device__ __forceinline__ uint4 ldpc_node(float *app, const uint2 *ent, uint32_t deg, uint32_t tid, uint32_t Z,
+__device__ __forceinline__ uint4 ldpc_node(__half2 *app, const uint2 *ent, uint32_t deg, uint32_t tid, uint32_t Z,
                                            const uint4 &st) {
-  uint32_t idx[D];
-  float q[D];
+  // rows of more than 10 entries recompute the slot indices for the stores
+  // rather than hold them (register pressure)
+  constexpr bool kKeepIdx = D <= 10;
+  auto slot = [&](int j) {
+    const uint2 en = ent[j];
+    uint32_t z = tid + en.y;
+    if (z >= Z) z -= Z;
+    return en.x + z;
+  };
+  const PairMsg mo = pair_msg(st);
+  uint32_t idx[kKeepIdx ? D : 1];
+  __half2 q[D];
 #pragma unroll
   for (int j = 0; j < D; j++) {
     if (j < (int)deg) {
-      const uint2 en = ent[j];
-      uint32_t z = tid + en.y;
-      if (z >= Z) z -= Z;
-      idx[j] = en.x + z;
+      const uint32_t ix = slot(j);
+      if constexpr (kKeepIdx) idx[j] = ix;
+      q[j] = app[ix];
     }
   }
-#pragma unroll
-  for (int j = 0; j < D; j++)
-    if (j < (int)deg) q[j] = app[idx[j]];
-  const float m1o = __fmul_rn(kAlpha, __uint_as_float(st.x));
-  const float m2o = __fmul_rn(kAlpha, __uint_as_float(st.y));
-  const uint32_t sgn_o = st.w ^ ((__popc(st.w) & 1u) ? ~0u : 0u);
-  float min1 = INFINITY, min2 = INFINITY;
-  uint32_t pos = 0, neg = 0;
+  __half2 min1 = __float2half2_rn(INFINITY), min2 = min1;
+  uint32_t pos = 0, nl = 0, nh = 0;
 #pragma unroll
   for (int j = 0; j < D; j++) {
     if (j < (int)deg) {
-      const float r = __uint_as_float(__float_as_uint((uint32_t)j == st.z ? m2o : m1o) ^ (((sgn_o >> j) & 1u) << 31));
-      q[j] = __fsub_rn(q[j], r);
-      const float aq = fabsf(q[j]);
-      neg |= (q[j] < 0.f ? 1u : 0u) << j;
-      if (aq < min1) {
-        min2 = min1;
-        min1 = aq;
-        pos = j;
-      } else if (aq < min2) {
-        min2 = aq;
-      }
+      q[j] = __hsub2(q[j], pair_r(mo, j));
+      pair_track(q[j], j, min1, min2, pos, nl, nh);
     }
   }
-  if (deg == 1) min2 = min1;
-  const float m1 = __fmul_rn(kAlpha, min1), m2 = __fmul_rn(kAlpha, min2);
-  const uint32_t sgn = neg ^ ((__popc(neg) & 1u) ? ~0u : 0u);
+  const uint4 ns = pair_state(min1, min2, pos, nl, nh, deg);
+  const PairMsg mn = pair_msg(ns);
 #pragma unroll
-  for (int j = 0; j < D; j++)
-    if (j < (int)deg)
-      app[idx[j]] = __fadd_rn(q[j], __uint_as_float(__float_as_uint((uint32_t)j == pos ? m2 : m1) ^ (((sgn >> j) & 1u) << 31)));
-  return make_uint4(__float_as_uint(min1), __float_as_uint(min2), pos, neg);
+  for (int j = 0; j < D; j++) {
+    if (j < (int)deg) {
+      uint32_t ix;
+      if constexpr (kKeepIdx) ix = idx[j];
+      else ix = slot(j);
+      app[ix] = __hadd2(q[j], pair_r(mn, j));
+    }
+  }
+  return ns;
 }
 
-// The same update for rows of any degree (up to 32): q_e is stored in place
-// of app between the two passes.
-__device__ __forceinline__ uint4 ldpc_node_any(float *app, const uint2 *ent, uint32_t deg, uint32_t tid,
+// The same update for rows of any degree (up to kMaxDeg): q_e is stored in
+// place of app between the two passes.
+__device__ __forceinline__ uint4 ldpc_node_any(__half2 *app, const uint2 *ent, uint32_t deg, uint32_t tid,
                                                uint32_t Z, const uint4 &st) {
-  const float m1o = __fmul_rn(kAlpha, __uint_as_float(st.x));
-  const float m2o = __fmul_rn(kAlpha, __uint_as_float(st.y));
-  const uint32_t sgn_o = st.w ^ ((__popc(st.w) & 1u) ? ~0u : 0u);
-  float min1 = INFINITY, min2 = INFINITY;
-  uint32_t pos = 0, neg = 0;
+  const PairMsg mo = pair_msg(st);
+  __half2 min1 = __float2half2_rn(INFINITY), min2 = min1;
+  uint32_t pos = 0, nl = 0, nh = 0;
   for (uint32_t e = 0; e < deg; e++) {
     const uint2 en = ent[e];
     uint32_t z = tid + en.y;
     if (z >= Z) z -= Z;
-    float *a = app + en.x + z;
-    const float r = __uint_as_float(__float_as_uint(e == st.z ? m2o : m1o) ^ (((sgn_o >> e) & 1u) << 31));
-    const float qe = __fsub_rn(*a, r);
+    __half2 *a = app + en.x + z;
+    const __half2 qe = __hsub2(*a, pair_r(mo, e));
     *a = qe;
-    const float aq = fabsf(qe);
-    neg |= (qe < 0.f ? 1u : 0u) << e;
-    if (aq < min1) {
-      min2 = min1;
-      min1 = aq;
-      pos = e;
-    } else if (aq < min2) {
-      min2 = aq;
-    }
+    pair_track(qe, e, min1, min2, pos, nl, nh);
   }
-  if (deg == 1) min2 = min1;
-  const float m1 = __fmul_rn(kAlpha, min1), m2 = __fmul_rn(kAlpha, min2);
-  const uint32_t sgn = neg ^ ((__popc(neg) & 1u) ? ~0u : 0u);
+  const uint4 ns = pair_state(min1, min2, pos, nl, nh, deg);
+  const PairMsg mn = pair_msg(ns);
   for (uint32_t e = 0; e < deg; e++) {
     const uint2 en = ent[e];
     uint32_t z = tid + en.y;
     if (z >= Z) z -= Z;
-    float *a = app + en.x + z;
-    *a = __fadd_rn(*a, __uint_as_float(__float_as_uint(e == pos ? m2 : m1) ^ (((sgn >> e) & 1u) << 31)));
+    __half2 *a = app + en.x + z;
+    *a = __hadd2(*a, pair_r(mn, e));
   }
-  return make_uint4(__float_as_uint(min1), __float_as_uint(min2), pos, neg);
+  return ns;
 }
 
+// CTA p decodes code blocks b0 + 2p and b0 + 2p + 1 (the second only when
+// 2p + 1 < nb; otherwise its lane repeats the first and is not written)
 __global__ void __launch_bounds__(kMaxZ, 2) ldpc_decode_kernel(mb_ldpc h, const __half *llr, uint64_t llr_stride,
-                                                            uint8_t *out, uint64_t out_stride, uint32_t max_iter,
-                                                            uint32_t b0) {
-  extern __shared__ float app[];  // [(kb + mb) Z], then the entries {col * Z, shift} and the row pointers
+                                                               uint8_t *out, uint64_t out_stride, uint32_t max_iter,
+                                                               uint32_t b0, uint32_t nb) {
+  // the pair's a-posteriori LLRs [(kb + mb) Z] (__half2), then the entries
+  // {col * Z, shift} and the row pointers
+  extern __shared__ uint32_t dec_smem[];
   const uint32_t Z = h.Z, kb = h.kb, mb = h.mb, N = (kb + mb) * Z, tid = threadIdx.x, nt = blockDim.x;
-  uint2 *ent = reinterpret_cast<uint2 *>(app + (N + 1) / 2 * 2);  // [nnz]
-  uint32_t *r_ptr = reinterpret_cast<uint32_t *>(ent + h.nnz);    // [mb + 1]
-  const uint32_t cb = b0 + blockIdx.x;
-  const __half *in = llr + (uint64_t)cb * llr_stride;
-  for (uint32_t v = tid; v < N; v += nt) app[v] = __half2float(in[v]);
+  __half2 *app = reinterpret_cast<__half2 *>(dec_smem);
+  uint2 *ent = reinterpret_cast<uint2 *>(dec_smem + (N + 1) / 2 * 2);  // [nnz]
+  uint32_t *r_ptr = reinterpret_cast<uint32_t *>(ent + h.nnz);         // [mb + 1]
+  const uint32_t cb = b0 + 2 * blockIdx.x;
+  const bool two = 2 * blockIdx.x + 1 < nb;
+  const __half *in0 = llr + (uint64_t)cb * llr_stride;
+  const __half *in1 = two ? in0 + llr_stride : in0;
+  for (uint32_t v = tid; v < N; v += nt) app[v] = llr_clamp(__halves2half2(in0[v], in1[v]));
   for (uint32_t e = tid; e < h.nnz; e += nt) ent[e] = make_uint2((uint32_t)h.col[e] * Z, h.sh[e]);
   for (uint32_t i = tid; i <= mb; i += nt) r_ptr[i] = h.row_ptr[i];
   __syncthreads();
@@ -244,15 +330,18 @@ __global__ void __launch_bounds__(kMaxZ, 2) ldpc_decode_kernel(mb_ldpc h, const 
       __syncthreads();
     }
   }
-  // hard decisions of the information bits, MSB first
-  uint8_t *o = out + (uint64_t)cb * out_stride;
+  // hard decisions of the information bits, MSB first, both blocks
+  uint8_t *o0 = out + (uint64_t)cb * out_stride, *o1 = o0 + out_stride;
   for (uint32_t b = tid; b < (kb * Z + 7) / 8; b += nt) {
-    uint32_t v = 0;
+    uint32_t v0 = 0, v1 = 0;
     for (uint32_t k = 0; k < 8; k++) {
       const uint32_t bit = 8 * b + k;
-      v = (v << 1) | (bit < kb * Z && app[bit] < 0.f ? 1u : 0u);
+      const uint32_t ng = bit < kb * Z ? __hlt2_mask(app[bit], __float2half2_rn(0.f)) : 0u;
+      v0 = (v0 << 1) | (ng & 1u);
+      v1 = (v1 << 1) | (ng >> 31);
     }
-    o[b] = (uint8_t)v;
+    o0[b] = (uint8_t)v0;
+    if (two) o1[b] = (uint8_t)v1;
   }
 }
 
@@ -371,7 +460,7 @@ extern "C" mb_status mb_ldpc_create(const mb_ldpc_graph *g, uint32_t Z, uint32_t
   alloc_copy((void **)&h->col, col.data(), col.size() * sizeof(uint16_t));
   alloc_copy((void **)&h->sh, sh.data(), sh.size() * sizeof(uint16_t));
   alloc_copy((void **)&h->binv, inv32.data(), inv32.size() * sizeof(uint32_t));
-  alloc_copy((void **)&h->state, nullptr, (size_t)max_batch * mbr * Z * sizeof(uint4));
+  alloc_copy((void **)&h->state, nullptr, (size_t)((max_batch + 1) / 2) * mbr * Z * sizeof(uint4));
   if (st != MB_OK) {
     mb_ldpc_destroy(h);
     return st;
@@ -398,6 +487,7 @@ extern "C" mb_status mb_ldpc_decode(mb_ldpc *h, const uint16_t *llr, uint64_t ll
   if (!h || !llr || !out) return MB_BAD_ARG;
   if (llr_stride < (uint64_t)(h->kb + h->mb) * h->Z || out_stride < ((uint64_t)h->kb * h->Z + 7) / 8)
     return MB_BAD_SHAPE;
+  if (max_iter > kMaxIter) return MB_BAD_ARG;  // the FP16 range argument above
   if (batch == 0) return MB_OK;
   const size_t smem = ((size_t)(h->kb + h->mb) * h->Z + 1) / 2 * 8 + 8 * (size_t)h->nnz + 4 * ((size_t)h->mb + 1);
   static_assert(kMaxZ <= 1024, "one thread per check node");
@@ -406,11 +496,12 @@ extern "C" mb_status mb_ldpc_decode(mb_ldpc *h, const uint16_t *llr, uint64_t ll
   if (smem > (size_t)maxs) return MB_UNSUPPORTED;
   MB_CUDA_TRY(cudaFuncSetAttribute(ldpc_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const uint32_t threads = (h->Z + 31) / 32 * 32;
-  // at most max_batch code blocks at a time: each keeps its check-node state
+  // at most max_batch code blocks at a time, in pairs: each pair keeps its
+  // check-node state
   for (uint32_t b0 = 0; b0 < batch; b0 += h->max_batch) {
     const uint32_t nb = std::min(h->max_batch, batch - b0);
-    ldpc_decode_kernel<<<nb, threads, smem, as_stream(stream)>>>(*h, reinterpret_cast<const __half *>(llr),
-                                                                 llr_stride, out, out_stride, max_iter, b0);
+    ldpc_decode_kernel<<<(nb + 1) / 2, threads, smem, as_stream(stream)>>>(
+        *h, reinterpret_cast<const __half *>(llr), llr_stride, out, out_stride, max_iter, b0, nb);
     MB_LAUNCH_CHECK();
   }
   return MB_OK;

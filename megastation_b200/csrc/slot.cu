@@ -504,8 +504,9 @@ extern "C" mb_status mb_slot_set_ldpc(mb_slot *s, mb_ldpc *code, uint32_t max_it
     // cb_size = (kb - 2 + mb) Z, within the row stride
     const mb_cell_desc &c = s->c;
     if (c.zeros != 2ull * code->Z || c.cb_size != (uint64_t)(code->kb - 2 + code->mb) * code->Z ||
-        c.cb_stride < (uint64_t)(code->kb + code->mb) * code->Z || max_iter == 0)
+        c.cb_stride < (uint64_t)(code->kb + code->mb) * code->Z)
       return MB_BAD_SHAPE;
+    if (max_iter == 0 || max_iter > 32) return MB_BAD_ARG;  // mb_ldpc_decode's range
   }
   s->ldpc = code;
   s->ldpc_iters = max_iter;

@@ -16,8 +16,9 @@ oracle/ref_ldpc.mk builds it here.  This module
   identity block);
 * restates the encoder for such a graph (`encode`: core parity from the
   inverse of the 4Z x 4Z core block, extension parity row by row) and a
-  layered normalized min-sum decoder (`decode`) in the float32 arithmetic of
-  the library's kernel, for bit-exact comparisons.
+  layered normalized min-sum decoder (`decode`) in the float16 arithmetic of
+  the library's kernel (the precision of the reference's cuPHY decoder), for
+  bit-exact comparisons.
 
 Block (i, j) of the graph with shift s is the Z x Z identity with its
 columns cyclically shifted right by s: row r has its one in column
@@ -257,33 +258,57 @@ def syndrome_ok(g, x):
     return True
 
 
+# FP16 range: the channel LLRs are clamped to +-LLR_MAX once and every
+# check-to-variable message to +-MSG_MAX, while q and app are exact sums
+# (app = llr + the sum of the messages of its rows, up to rounding); with
+# at most 46 rows a variable stays below 1024 + 46 * 256 = 12800, and the
+# rounding of two operations a row visit (at most 32 below 65504) adds at
+# most 46 * 32 * 32 over 32 passes: nothing overflows for max_iter <= 32
+LLR_MAX = np.float16(1024)
+MSG_MAX = np.float16(256)
+MAX_ITER = 32
+
+
 def decode(g, llr, max_iter, alpha=0.75):
     """Layered normalized min-sum over the first mb block rows, rows in
-    order, max_iter passes, float32 arithmetic in the library kernel's order:
-    q = app - c2v; per check node min1 (first index), min2, the sign parity
-    of q < 0; r = +-(alpha * min); app = q + r.  llr [(kb + mb) Z] (float16
-    or float32; positive means bit 0).  Returns (bits [kb Z], app)."""
+    order, max_iter passes, float16 arithmetic in the library kernel's order
+    (every step one IEEE float16 operation, round to nearest even):
+    app = clip(llr, +-LLR_MAX); per row, for each check node q = app - c2v,
+    min1 = min |q| (first index), min2 = the least of the others (min1 for a
+    single entry), the parity of the sign bits of q (-0 counts as negative);
+    r = +-min(alpha * min, MSG_MAX)
+    (alpha * min2 at min1's index); app = q + r.  llr [(kb + mb) Z]
+    (float16; positive means bit 0), or [B][(kb + mb) Z] for B independent
+    blocks.  Returns (bits [kb Z] or [B][kb Z], app)."""
     Z, kb = g.Z, g.kb
-    app = np.asarray(llr, np.float32).copy()
-    a = np.float32(alpha)
+    x = np.asarray(llr, np.float16)
+    one = x.ndim == 1
+    assert max_iter <= MAX_ITER
+    app = np.clip(np.atleast_2d(x), -LLR_MAX, LLR_MAX).T.copy()       # [N][B]
+    a = np.float16(alpha)
     z = np.arange(Z)
     idx = [np.stack([c * Z + (z + s) % Z for c, s in ents]) for ents in g.rows]
-    c2v = [np.zeros((len(ents), Z), np.float32) for ents in g.rows]
+    B = app.shape[1]
+    c2v = [np.zeros((len(ents), Z, B), np.float16) for ents in g.rows]
     for _ in range(max_iter):
         for i in range(g.mb):
-            q = (app[idx[i]] - c2v[i]).astype(np.float32)
+            q = app[idx[i]] - c2v[i]                                   # [deg][Z][B]
             mag = np.abs(q)
             deg = mag.shape[0]
-            pos = np.argmin(mag, axis=0)
-            min1 = mag[pos, z]
-            rest = mag.copy()
-            rest[pos, z] = np.inf
-            min2 = rest.min(axis=0) if deg > 1 else min1
-            neg = q < 0
+            pos = np.argmin(mag, axis=0)                               # [Z][B]
+            min1 = np.take_along_axis(mag, pos[None], axis=0)[0]
+            if deg > 1:
+                rest = mag.copy()
+                np.put_along_axis(rest, pos[None], np.float16(np.inf), axis=0)
+                min2 = rest.min(axis=0)
+            else:
+                min2 = min1
+            neg = np.signbit(q)
             par = np.logical_xor.reduce(neg, axis=0)
-            m1, m2 = (a * min1).astype(np.float32), (a * min2).astype(np.float32)
-            m = np.where(np.arange(deg)[:, None] == pos[None, :], m2[None, :], m1[None, :])
-            r = np.where(par[None, :] ^ neg, -m, m).astype(np.float32)
-            app[idx[i]] = (q + r).astype(np.float32)
+            m1, m2 = np.minimum(a * min1, MSG_MAX), np.minimum(a * min2, MSG_MAX)
+            m = np.where(np.arange(deg)[:, None, None] == pos[None], m2[None], m1[None])
+            r = np.where(par[None] ^ neg, -m, m)
+            app[idx[i]] = q + r
             c2v[i] = r
-    return (app[:kb * Z] < 0).astype(np.uint8), app
+    bits = (app[:kb * Z] < 0).astype(np.uint8).T
+    return (bits[0], app[:, 0]) if one else (bits, app.T)

@@ -1,12 +1,13 @@
 """The LDPC kernels (csrc/ldpc.cu through the C ABI) against the reference's
-encoder and the float32 restatement of the decoder (oracle/ldpc.py).
+encoder and the float16 restatement of the decoder (oracle/ldpc.py).
 
 The encoder must give the reference's nrLDPCEncode codewords bit for bit
 (tests/golden/ldpc/, base graphs 1 and 2 at Z = 16) and the restated encoder's
 on fewer parity rows and on a Z = 384 graph of base graph 1's shape; the
 decoder must give the restatement's information bits bit for bit on noisy
-FP16 LLRs, including where it fails to correct, and recover the information
-of moderately noisy codewords."""
+FP16 LLRs, including where it fails to correct, for odd batches (a pair's
+second block absent) and for LLRs at the FP16 limit (the a-posteriori clamp),
+and recover the information of moderately noisy codewords."""
 import os
 
 import numpy as np
@@ -94,7 +95,7 @@ def test_decoder_matches_restatement(case, sigma, iters):
     entries = _fixture(bg)[0] if Z == 16 else _big_graph(Z)
     kb = ldpc.KB[bg]
     g = ldpc.Graph(entries, kb, Z, m)
-    B = 6 if Z == 16 else 2
+    B = 7 if Z == 16 else 3  # odd: the last pair has one block
     rng = np.random.default_rng(int(sigma * 100) + Z + m)
     info = rng.integers(0, 2, (B, kb * Z), dtype=np.uint8)
     # equalizer-style rows: the code block's LLRs, punctured ones zero, then
@@ -106,7 +107,7 @@ def test_decoder_matches_restatement(case, sigma, iters):
         y = (1.0 - 2.0 * x) + sigma * rng.standard_normal(len(x))
         llr[k, :g.N] = (2.0 * y / sigma ** 2).astype(np.float16)
         llr[k, :2 * Z] = 0
-    code = mb.Ldpc(entries, kb, Z, m, max_batch=4)  # B = 6 decodes in two turns
+    code = mb.Ldpc(entries, kb, Z, m, max_batch=4)  # B = 7 decodes in two turns
     out = code.decode(torch.from_numpy(llr).cuda(), max_iter=iters)
     torch.cuda.synchronize()
     assert mb.ops.device_error() == 0
@@ -118,6 +119,41 @@ def test_decoder_matches_restatement(case, sigma, iters):
         decoded += int((bits == info[k]).all())
     if sigma <= 0.5:
         assert decoded == B
+
+
+@pytest.mark.parametrize("bg", [1, 2])
+def test_decoder_clamps_large_llrs(bg):
+    """LLRs up to the FP16 limit (and infinities), 32 passes: channel LLRs
+    clamped to +-1024 and messages to +-256 keep every value finite, the
+    kernel equals the restatement, bounds included, bit for bit, and the
+    confident codewords decode; more than 32 passes are refused."""
+    mb = _mb()
+    entries, info, _, Z = _fixture(bg)
+    kb = ldpc.KB[bg]
+    g = ldpc.Graph(entries, kb, Z, ldpc.ROWS[bg])
+    rng = np.random.default_rng(40 + bg)
+    B = 3
+    llr = np.zeros((B, g.N), np.float16)
+    for k in range(B):
+        x = ldpc.encode(g, info[k])
+        y = (1.0 - 2.0 * x) * rng.uniform(2e3, 7e4, len(x))
+        y[rng.integers(0, len(x), 8)] *= -1  # a few confident errors
+        llr[k] = np.clip(y, -65504, 65504).astype(np.float16)
+        llr[k, :2 * Z] = 0
+    llr[0, 2 * Z + 5] = np.inf
+    llr[1, 2 * Z + 9] = -np.inf
+    llr[2, 2 * Z + 3] = np.float16(-0.0)  # a negative zero counts as negative
+    code = mb.Ldpc(entries, kb, Z, ldpc.ROWS[bg], max_batch=B)
+    out = code.decode(torch.from_numpy(llr).cuda(), max_iter=32)
+    torch.cuda.synchronize()
+    got = np.unpackbits(out.cpu().numpy(), axis=1)[:, :kb * Z]
+    bits, app = ldpc.decode(g, llr, 32)
+    assert np.isfinite(app.astype(np.float32)).all()
+    np.testing.assert_array_equal(got, bits)
+    np.testing.assert_array_equal(bits, info[:B])
+    from megastation_b200._lib import MbError
+    with pytest.raises(MbError):
+        code.decode(torch.from_numpy(llr).cuda(), max_iter=33)
 
 
 def test_graph_errors():
