@@ -209,9 +209,7 @@ __device__ __forceinline__ uint4 ldpc_node(__half2 *app, const uint2 *ent, uint3
   constexpr bool kKeepIdx = D <= 10;
   auto slot = [&](int j) {
     const uint2 en = ent[j];
-    uint32_t z = tid + en.y;
-    if (z >= Z) z -= Z;
-    return en.x + z;
+    return en.x + tid - (tid >= en.y ? Z : 0u);
   };
   const PairMsg mo = pair_msg(st);
   uint32_t idx[kKeepIdx ? D : 1];
@@ -256,9 +254,7 @@ __device__ __forceinline__ uint4 ldpc_node_any(__half2 *app, const uint2 *ent, u
   uint32_t pos = 0, nl = 0, nh = 0;
   for (uint32_t e = 0; e < deg; e++) {
     const uint2 en = ent[e];
-    uint32_t z = tid + en.y;
-    if (z >= Z) z -= Z;
-    __half2 *a = app + en.x + z;
+    __half2 *a = app + en.x + tid - (tid >= en.y ? Z : 0u);
     const __half2 qe = __hsub2(*a, pair_r(mo, e));
     *a = qe;
     pair_track(qe, e, min1, min2, pos, nl, nh);
@@ -267,9 +263,7 @@ __device__ __forceinline__ uint4 ldpc_node_any(__half2 *app, const uint2 *ent, u
   const PairMsg mn = pair_msg(ns);
   for (uint32_t e = 0; e < deg; e++) {
     const uint2 en = ent[e];
-    uint32_t z = tid + en.y;
-    if (z >= Z) z -= Z;
-    __half2 *a = app + en.x + z;
+    __half2 *a = app + en.x + tid - (tid >= en.y ? Z : 0u);
     *a = __hadd2(*a, pair_r(mn, e));
   }
   return ns;
@@ -292,7 +286,9 @@ __global__ void __launch_bounds__(kMaxZ, 2) ldpc_decode_kernel(mb_ldpc h, const 
   const __half *in0 = llr + (uint64_t)cb * llr_stride;
   const __half *in1 = two ? in0 + llr_stride : in0;
   for (uint32_t v = tid; v < N; v += nt) app[v] = llr_clamp(__halves2half2(in0[v], in1[v]));
-  for (uint32_t e = tid; e < h.nnz; e += nt) ent[e] = make_uint2((uint32_t)h.col[e] * Z, h.sh[e]);
+  // entry e as {col * Z + shift, Z - shift}: check node z meets variable
+  // col * Z + (z + shift) mod Z, i.e. x + z, less Z once z >= y
+  for (uint32_t e = tid; e < h.nnz; e += nt) ent[e] = make_uint2((uint32_t)h.col[e] * Z + h.sh[e], Z - h.sh[e]);
   for (uint32_t i = tid; i <= mb; i += nt) r_ptr[i] = h.row_ptr[i];
   __syncthreads();
   // Thread z only ever reads and writes check node z's state, so its loads
@@ -300,17 +296,17 @@ __global__ void __launch_bounds__(kMaxZ, 2) ldpc_decode_kernel(mb_ldpc h, const 
   // layers before it is read again); the first pass starts from zero
   // messages without reading.
   uint4 *state = h.state + (uint64_t)blockIdx.x * mb * Z;
-  const uint32_t layers = max_iter * mb;
-  auto load_state = [&](uint32_t L) {
-    return (L < mb || L >= layers || tid >= Z) ? make_uint4(0u, 0u, 0u, 0u) : state[(L % mb) * Z + tid];
+  // the state of row r in pass it: none in the first pass nor past the last
+  auto load_state = [&](uint32_t it, uint32_t r) {
+    return (it == 0 || it >= max_iter || tid >= Z) ? make_uint4(0u, 0u, 0u, 0u) : state[r * Z + tid];
   };
-  uint4 st_a = load_state(0), st_b = load_state(1);
+  uint4 st_a = load_state(0, 0), st_b = load_state(0, 1);
   for (uint32_t it = 0; it < max_iter; it++) {
     for (uint32_t i = 0; i < mb; i++) {
-      const uint32_t L = it * mb + i;
       const uint4 st = st_a;
       st_a = st_b;
-      st_b = load_state(L + 2);
+      // row i + 2, in this pass or the next (mb >= 4)
+      st_b = i + 2 < mb ? load_state(it, i + 2) : load_state(it + 1, i + 2 - mb);
       if (tid < Z) {
         const uint32_t e0 = r_ptr[i], deg = r_ptr[i + 1] - e0;
         // every thread of the layer takes the same branch
