@@ -80,3 +80,23 @@ def test_singular_core_is_refused():
     g = ldpc.Graph(e, 10, Z, 42)
     with pytest.raises(ValueError):
         g.core_inverse()
+
+
+@pytest.mark.parametrize("bg", [1, 2])
+def test_restated_decoder_bounds(bg):
+    """The float16 decoder's bounds (channel LLRs clamped to +-1024, messages
+    to +-256, q and app unclamped sums) keep every value finite over the
+    32 passes allowed, from LLRs at the FP16 limit and infinities, and the
+    confident codewords decode; more passes are refused."""
+    entries, info, _, Z = _fixture(bg)
+    g = ldpc.Graph(entries, ldpc.KB[bg], Z, ldpc.ROWS[bg])
+    for k in range(2):
+        x = ldpc.encode(g, info[k])
+        llr = np.clip((1.0 - 2.0 * x) * 65504.0, -65504, 65504).astype(np.float16)
+        llr[2 * Z + k] = np.inf if llr[2 * Z + k] > 0 else -np.inf
+        bits, app = ldpc.decode(g, llr, ldpc.MAX_ITER)
+        assert np.isfinite(app.astype(np.float32)).all()
+        assert np.abs(app.astype(np.float32)).max() <= 1024 + ldpc.ROWS[bg] * 256 + 2048
+        np.testing.assert_array_equal(bits, info[k])
+    with pytest.raises(AssertionError):
+        ldpc.decode(g, llr, ldpc.MAX_ITER + 1)
