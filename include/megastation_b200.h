@@ -570,7 +570,9 @@ mb_status mb_ldpc_encode(mb_ldpc *ldpc, const uint8_t *info, uint64_t info_strid
  * stop, in FP16 arithmetic (the precision of the reference's cuPHY decoder;
  * two code blocks per CTA in the halves of FP16 pairs).  Channel LLRs are
  * clamped to +-1024 and messages to +-256, which keeps every value finite;
- * NaN inputs give undefined bits. */
+ * NaN inputs give undefined bits.  The check-node state lives in the handle:
+ * decodes on one handle that can overlap on the GPU (different streams)
+ * race, so serialise them or give each stream its own handle. */
 mb_status mb_ldpc_decode(mb_ldpc *ldpc, const uint16_t *llr, uint64_t llr_stride, uint8_t *out,
                          uint64_t out_stride, uint32_t batch, uint32_t max_iter, void *stream);
 
