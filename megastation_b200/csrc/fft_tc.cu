@@ -235,10 +235,16 @@ __global__ void __launch_bounds__(kFtThreads, 1)
 
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   // this CTA's units: blockIdx.x, blockIdx.x + gridDim.x, ... (strided, so
-  // the pilot rows at the front spread over all CTAs)
+  // the pilot rows at the front spread over all CTAs), taken in an order
+  // rotated by the CTA index, so that the CTAs reach their pilot units (CSI
+  // stores, pilot loads) at different times rather than all at the start
   if (blockIdx.x >= p.units) return;
   const uint32_t n_units = (p.units - blockIdx.x + gridDim.x - 1) / gridDim.x;
-  auto unit_of = [&](uint32_t i) { return blockIdx.x + i * gridDim.x; };
+  const uint32_t rot = blockIdx.x % n_units;
+  auto unit_of = [&](uint32_t i) {
+    const uint32_t k = i + rot < n_units ? i + rot : i + rot - n_units;
+    return blockIdx.x + k * gridDim.x;
+  };
 
   if (tid == kFtCompute) {
     tc::mbar_init(&bar_mats, 1);
