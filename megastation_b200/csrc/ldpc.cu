@@ -22,11 +22,11 @@
 // entries; the rows in order as layers; per check node and block:
 // q_e = app - r_e (r_e the node's previous message to entry e, rebuilt from
 // its compressed state), min1 (first index), min2 and the parity of the
-// sign bits of q, then app = q_e + r'_e, r'_e = +-min(0.75 min, 256); rows of up to
-// 20 entries keep q in registers (ldpc_node).  FP16 is the reference
-// decoder's precision (cuPHY), and the pairs halve the instructions per
-// block; channel LLRs clamped to +-1024 and messages to +-256 keep every
-// value finite for up to 32 passes.
+// sign bits of q, then app = q_e + r'_e, r'_e = +-min(0.75 min, 256).  Rows
+// of up to 20 entries keep q in registers (ldpc_node, variants for 4, 6, 10
+// and 20 entries).  FP16 is the reference decoder's precision (cuPHY), and
+// the pairs halve the instructions per block; channel LLRs clamped to
+// +-1024 and messages to +-256 keep every value finite for up to 32 passes.
 // Within a layer the Z check nodes touch disjoint variables (a circulant is
 // a permutation), so a layer needs one barrier.  The compressed state (min1,
 // min2, index, sign bits) per (layer, check node) lives in global memory,
